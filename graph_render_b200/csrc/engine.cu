@@ -1,0 +1,651 @@
+// ForceAtlas2 / Barnes-Hut engine for one graph on one B200, and its C ABI.
+//
+// One tick (crates/graph-core/src/layout/forceatlas2/state.rs:130-148):
+//   bounds+mean -> Morton keys -> radix sort -> sorted nodes + unique keys ->
+//   Karras tree -> FP64 cell sums -> cell preorder -> warp-cooperative walk
+//   (repulsion) -> attraction + gravity + FP64 swing/traction + speed ->
+//   update + FP64 step sum.
+// Every launch is sized from n alone and reads the per-tick counts (leaves,
+// cells, convergence) from device memory, so one tick is captured once into a
+// CUDA graph and replayed.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/graph_cuda.h"
+#include "common.cuh"
+#include "forces.cuh"
+#include "radix_sort.cuh"
+#include "scan.cuh"
+#include "simple_graph.cuh"
+#include "tree.cuh"
+#include "walk.cuh"
+
+using namespace gr;
+
+// ------------------------------------------------------------- errors ------
+
+static thread_local int g_err = 0;
+static thread_local int g_err_index = -1;
+static thread_local char g_msg[256] = "";
+
+static int set_err(int code, const char *msg, int index = -1) {
+    g_err = code;
+    g_err_index = index;
+    snprintf(g_msg, sizeof g_msg, "%s", msg ? msg : "");
+    return code;
+}
+static int ok() { return set_err(GR_OK, ""); }
+
+#define CU(call)                                                                  \
+    do {                                                                          \
+        cudaError_t e_ = (call);                                                  \
+        if (e_ != cudaSuccess) {                                                  \
+            char b_[200];                                                         \
+            snprintf(b_, sizeof b_, "%s: %s", #call, cudaGetErrorString(e_));     \
+            return set_err(e_ == cudaErrorMemoryAllocation ? GR_ALLOC_FAILED      \
+                                                           : GR_CUDA_ERROR, b_); \
+        }                                                                         \
+    } while (0)
+
+// ------------------------------------------------------------- params ------
+
+struct Spec {
+    const char *name;
+    int kind;
+    double min, max, def, step;
+    const char *doc;
+};
+
+// The first five are graph-core's Fa2Params schema (registry/tunable.rs:229-240);
+// the rest are the options the engine adds, appended.
+static const Spec kSpecs[] = {
+    {"max_iter", GR_KIND_INT, 1.0, 10000.0, 100.0, 1.0, "iteration ceiling (networkx default 100)"},
+    {"jitter_tolerance", GR_KIND_FLOAT, 0.0, 1e6, 1.0, 0.1, "jitter tolerance (networkx default 1.0)"},
+    {"scaling_ratio", GR_KIND_FLOAT, 0.0, 1e6, 2.0, 0.1, "repulsion scale (networkx default 2.0)"},
+    {"gravity", GR_KIND_FLOAT, 0.0, 1e6, 1.0, 0.1, "gravitational pull to the centroid (networkx default 1.0)"},
+    {"seed", GR_KIND_INT, 0.0, 4294967295.0, 0.0, 1.0, "seeds the initial positions and the coincidence jiggle"},
+    {"dim", GR_KIND_INT, 2.0, 3.0, 2.0, 1.0, "coordinates per node: 2, or 3 (octree)"},
+    {"theta", GR_KIND_FLOAT, 0.0, 10.0, 0.8, 0.1, "Barnes-Hut opening angle; 0 sums every pair exactly"},
+    {"lin_log", GR_KIND_BOOL, 0.0, 1.0, 0.0, 1.0, "logarithmic attraction (networkx linlog)"},
+    {"strong_gravity", GR_KIND_BOOL, 0.0, 1.0, 0.0, 1.0, "gravity proportional to distance (networkx strong_gravity)"},
+    {"dissuade_hubs", GR_KIND_BOOL, 0.0, 1.0, 0.0, 1.0, "attraction divided by mass (networkx distributed_action)"},
+    {"edge_weight_influence", GR_KIND_FLOAT, 0.0, 10.0, 0.0, 0.1, "attraction weight = edge weight ^ influence; 0 = unit weights"},
+};
+static const uint32_t kNParams = sizeof(kSpecs) / sizeof(kSpecs[0]);
+static const uint32_t kRefParams = 5;
+
+enum { P_MAX_ITER, P_JT, P_SCALING, P_GRAVITY, P_SEED, P_DIM, P_THETA, P_LINLOG, P_STRONG, P_DISSUADE, P_INFLUENCE };
+
+static int params_values(const uint8_t *bytes, size_t len, double *out) {
+    for (uint32_t i = 0; i < kNParams; i++) out[i] = kSpecs[i].def;
+    if (len == 0) return ok();
+    if (!bytes || (len != (size_t)kNParams * 8 && len != (size_t)kRefParams * 8))
+        return set_err(GR_PARAMS_MALFORMED, "params buffer is not 5 or 11 little-endian f64 values");
+    uint32_t cnt = (uint32_t)(len / 8);
+    for (uint32_t i = 0; i < cnt; i++) {
+        double v;
+        memcpy(&v, bytes + 8 * i, 8);
+        const Spec &s = kSpecs[i];
+        bool good = std::isfinite(v) && v >= s.min && v <= s.max;
+        if (good && s.kind == GR_KIND_INT) good = std::floor(v) == v;
+        if (good && s.kind == GR_KIND_BOOL) good = (v == 0.0 || v == 1.0);
+        if (!good) {
+            char b[160];
+            snprintf(b, sizeof b, "parameter %s is out of range (refused, never clamped)", s.name);
+            return set_err(GR_PARAM_OUT_OF_RANGE, b, (int)i);
+        }
+        out[i] = v;
+    }
+    return ok();
+}
+
+// ------------------------------------------------------------- engine ------
+
+struct gr_fa2 {
+    int dim = 2;
+    uint32_t n = 0;
+    uint64_t m = 0;
+    double prm[16];
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    // graph
+    uint32_t *rp = nullptr, *col = nullptr;
+    float *wt = nullptr;
+    float4 *pos = nullptr;
+
+    // per-tick buffers
+    uint64_t *keys = nullptr, *ukey = nullptr;
+    uint32_t *vals = nullptr, *sorig = nullptr, *flag = nullptr, *excl = nullptr, *uid = nullptr;
+    uint32_t *leaf_start = nullptr, *cells_at = nullptr, *P = nullptr, *leaf_pre = nullptr;
+    float4 *sp = nullptr;
+    BinTree bt{};
+    Body *leaf_body = nullptr, *int_body = nullptr;
+    uint8_t *leaf_coinc = nullptr;
+    Cells cells{};
+    float *rep = nullptr, *U = nullptr;
+    double *part = nullptr;
+    DevState *st = nullptr;
+    RadixSorter sorter;
+    Scanner scanner;
+
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+
+    std::vector<void *> allocs;
+
+    template <typename T>
+    cudaError_t alloc(T **p, size_t count) {
+        cudaError_t e = cudaMalloc((void **)p, (count ? count : 1) * sizeof(T));
+        if (e == cudaSuccess) allocs.push_back((void *)*p);
+        return e;
+    }
+    ~gr_fa2() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (void *p : allocs) cudaFree(p);
+        sorter.release();
+        scanner.release();
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+    uint32_t bnd_blocks() const { return std::max<uint32_t>(1, std::min<uint32_t>(div_up(n, BND_THREADS), 592)); }
+};
+
+static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
+    const uint32_t n = h->n;
+    const int D = h->dim;
+    cudaError_t e;
+#define A(p, c) if ((e = h->alloc(&(p), (c)))) return e
+    A(h->keys, n);
+    A(h->vals, n);
+    A(h->ukey, n);
+    A(h->sorig, n);
+    A(h->flag, n);
+    A(h->excl, n);
+    A(h->uid, n);
+    A(h->leaf_start, (size_t)n + 1);
+    A(h->cells_at, n);
+    A(h->P, (size_t)n + 1);
+    A(h->leaf_pre, n);
+    A(h->sp, n);
+    A(h->bt.first, n);
+    A(h->bt.last, n);
+    A(h->bt.left, n);
+    A(h->bt.right, n);
+    A(h->bt.delta, n);
+    A(h->bt.int_parent, n);
+    A(h->bt.leaf_parent, n);
+    A(h->bt.visit, n);
+    A(h->leaf_body, n);
+    A(h->int_body, n);
+    A(h->leaf_coinc, n);
+    A(h->cells.A, 2 * (size_t)n);
+    A(h->cells.B, 2 * (size_t)n);
+    if (D == 3) A(h->cells.C, 2 * (size_t)n);
+    A(h->rep, (size_t)n * D);
+    A(h->U, (size_t)n * D);
+    size_t np = std::max<size_t>((size_t)h->bnd_blocks() * 3 * D, 2 * (size_t)div_up(n, FRC_THREADS)) + 8;
+    A(h->part, np);
+#undef A
+    if ((e = h->sorter.init(n))) return e;
+    if ((e = h->scanner.init(n))) return e;
+    return cudaSuccess;
+}
+
+template <int D>
+static void enqueue_tick(gr_fa2 *h, bool forces_only) {
+    const uint32_t n = h->n;
+    cudaStream_t s = h->stream;
+    const uint32_t gn = div_up(n, 256);
+    DevState *st = h->st;
+    const uint32_t *conv = &st->converged;
+    k_bounds<D><<<h->bnd_blocks(), BND_THREADS, 0, s>>>(h->pos, n, st, h->part);
+    k_keys<D><<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals);
+    h->sorter.sort(h->keys, h->vals, n, 64, s, conv);
+    k_gather<<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals, h->sp, h->sorig, h->flag);
+    h->scanner.scan(h->flag, h->excl, n, nullptr, 0, &st->n_unique, nullptr, s, conv);
+    k_leaves<<<gn, 256, 0, s>>>(n, st, h->keys, h->flag, h->excl, h->leaf_start, h->ukey, h->uid);
+    k_karras<<<gn, 256, 0, s>>>(st, h->ukey, h->bt);
+    k_aggregate<D><<<gn, 256, 0, s>>>(st, h->sp, h->leaf_start, h->bt, h->leaf_body, h->int_body, h->leaf_coinc);
+    k_count<D><<<gn, 256, 0, s>>>(st, h->bt, h->cells_at);
+    h->scanner.scan(h->cells_at, h->P, n, &st->n_unique, 0, &st->n_cells, nullptr, s, conv);
+    k_assign<D><<<gn, 256, 0, s>>>(st, h->bt, h->P, h->cells_at, h->leaf_start, h->leaf_body, h->int_body,
+                                   h->leaf_coinc, h->cells, h->leaf_pre, st);
+    WalkParams wp;
+    wp.n = n;
+    wp.kr = (float)h->prm[P_SCALING];
+    wp.theta2 = (float)(h->prm[P_THETA] * h->prm[P_THETA]);
+    wp.seed = (uint32_t)h->prm[P_SEED];
+    k_walk<D><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig, h->uid,
+                                                                h->leaf_pre, h->rep, st);
+    ForceParams fp;
+    fp.n = n;
+    fp.gravity = (float)h->prm[P_GRAVITY];
+    fp.lin_log = (int)h->prm[P_LINLOG];
+    fp.strong_gravity = (int)h->prm[P_STRONG];
+    fp.dissuade_hubs = (int)h->prm[P_DISSUADE];
+    fp.jitter_tolerance = h->prm[P_JT];
+    k_forces<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(fp, st, h->pos, h->rp, h->col, h->wt, h->rep,
+                                                                h->U, h->part, forces_only ? 0 : 1);
+    if (!forces_only) k_update<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(n, st, h->pos, h->U, h->part);
+}
+
+static void enqueue(gr_fa2 *h, bool forces_only) {
+    if (h->dim == 3)
+        enqueue_tick<3>(h, forces_only);
+    else
+        enqueue_tick<2>(h, forces_only);
+}
+
+static int build_graph(gr_fa2 *h) {
+    if (h->exec) return GR_OK;
+    CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue(h, false);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &h->graph);
+    if (e != cudaSuccess) return set_err(GR_CUDA_ERROR, cudaGetErrorString(e));
+    CU(cudaGraphInstantiate(&h->exec, h->graph, 0));
+    return GR_OK;
+}
+
+static int read_state(gr_fa2 *h, DevState *out) {
+    CU(cudaMemcpyAsync(out, h->st, sizeof(DevState), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return GR_OK;
+}
+
+static int check_device(gr_fa2 *h, const DevState &s) {
+    if (s.error & ERR_NONFINITE) return set_err(GR_LAYOUT_FAILED, "non-finite position (StageError::NonFinite)");
+    if (s.error) {
+        char b[96];
+        snprintf(b, sizeof b, "device error bits 0x%x", s.error);
+        return set_err(GR_DEVICE_FAULT, b);
+    }
+    return GR_OK;
+}
+
+static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                       const double *weight, const uint8_t *params, size_t params_len, const float *pos0) {
+    if (!out) return set_err(GR_INVALID_ARGUMENT, "out is null");
+    *out = nullptr;
+    double prm[16];
+    if (int c = params_values(params, params_len, prm)) return c;
+    if (m && (!src || !dst)) return set_err(GR_INVALID_ARGUMENT, "edge arrays are null");
+    if (m > 0x7fffffffull) return set_err(GR_INVALID_ARGUMENT, "more than 2^31 edges");
+    const int D = (int)prm[P_DIM];
+    std::vector<float> xyz((size_t)n * D);
+    if (pos0) {
+        for (size_t i = 0; i < xyz.size(); i++) {
+            if (!std::isfinite(pos0[i])) return set_err(GR_INVALID_ARGUMENT, "non-finite start position");
+            xyz[i] = pos0[i];
+        }
+    } else {
+        // state.rs:272-283 / synthetic.rs:37-50: Mulberry32(seed), dim draws per node.
+        uint32_t s = (uint32_t)prm[P_SEED];
+        for (size_t i = 0; i < xyz.size(); i++) {
+            s += 0x6D2B79F5u;
+            uint32_t a = s;
+            uint32_t t = (a ^ (a >> 15)) * (1u | a);
+            t = (t + ((t ^ (t >> 7)) * (61u | t))) ^ t;
+            xyz[i] = (float)((double)(t ^ (t >> 14)) / 4294967296.0);
+        }
+    }
+    gr_fa2 *h = new (std::nothrow) gr_fa2();
+    if (!h) return set_err(GR_ALLOC_FAILED, "host allocation failed");
+    h->dim = D;
+    h->n = n;
+    memcpy(h->prm, prm, sizeof prm);
+    int rc = GR_OK;
+    do {
+        if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            rc = set_err(GR_CUDA_ERROR, "stream creation failed");
+            break;
+        }
+        h->own_stream = true;
+        cudaStream_t s = h->stream;
+        cudaError_t e = cudaSuccess;
+        // --- simple graph + CSR on the device
+        uint32_t *d_src = nullptr, *d_dst = nullptr, *d_err = nullptr;
+        double *d_w = nullptr;
+        uint64_t *ek = nullptr, *dk = nullptr;
+        uint32_t *ev = nullptr, *dv = nullptr, *eflag = nullptr, *eexcl = nullptr, *ms_d = nullptr;
+        RadixSorter esort;
+        Scanner escan;
+        uint32_t ms = 0;
+        auto cleanup = [&]() {
+            cudaFree(d_src);
+            cudaFree(d_dst);
+            cudaFree(d_w);
+            cudaFree(d_err);
+            cudaFree(ek);
+            cudaFree(ev);
+            cudaFree(dk);
+            cudaFree(dv);
+            cudaFree(eflag);
+            cudaFree(eexcl);
+            cudaFree(ms_d);
+            esort.release();
+            escan.release();
+        };
+        const uint64_t cap = std::max<uint64_t>(2 * m, 1);
+        if ((e = cudaMalloc(&d_err, 2 * sizeof(uint32_t))) || (e = cudaMalloc(&ms_d, 2 * sizeof(uint32_t))) ||
+            (e = cudaMalloc(&ek, cap * sizeof(uint64_t))) || (e = cudaMalloc(&ev, cap * sizeof(uint32_t))) ||
+            (e = cudaMalloc(&dk, cap * sizeof(uint64_t))) || (e = cudaMalloc(&dv, cap * sizeof(uint32_t))) ||
+            (e = cudaMalloc(&eflag, cap * sizeof(uint32_t))) || (e = cudaMalloc(&eexcl, cap * sizeof(uint32_t))) ||
+            (e = esort.init((uint32_t)cap)) || (e = escan.init((uint32_t)cap))) {
+            cleanup();
+            rc = set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+            break;
+        }
+        cudaMemsetAsync(d_err, 0, 2 * sizeof(uint32_t), s);
+        cudaMemsetAsync(ms_d, 0, 2 * sizeof(uint32_t), s);
+        if (m) {
+            if ((e = cudaMalloc(&d_src, m * 4)) || (e = cudaMalloc(&d_dst, m * 4)) ||
+                (weight && (e = cudaMalloc(&d_w, m * 8)))) {
+                cleanup();
+                rc = set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+                break;
+            }
+            cudaMemcpyAsync(d_src, src, m * 4, cudaMemcpyHostToDevice, s);
+            cudaMemcpyAsync(d_dst, dst, m * 4, cudaMemcpyHostToDevice, s);
+            if (weight) cudaMemcpyAsync(d_w, weight, m * 8, cudaMemcpyHostToDevice, s);
+            k_edge_keys<<<div_up(m, 256), 256, 0, s>>>(m, d_src, d_dst, n, ek, ev, d_err);
+            esort.sort(ek, ev, (uint32_t)m, 64, s);
+            k_edge_flags<<<div_up(m, 256), 256, 0, s>>>((uint32_t)m, ek, eflag);
+            escan.scan(eflag, eexcl, (uint32_t)m, nullptr, 0, ms_d, nullptr, s);
+        }
+        uint32_t hdr[2] = {0, 0};
+        cudaMemcpyAsync(hdr, d_err, sizeof hdr, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&ms, ms_d, 4, cudaMemcpyDeviceToHost, s);
+        if ((e = cudaStreamSynchronize(s))) {
+            cleanup();
+            rc = set_err(GR_CUDA_ERROR, cudaGetErrorString(e));
+            break;
+        }
+        if (hdr[0]) {
+            cleanup();
+            rc = set_err(GR_INVALID_ARGUMENT, "an edge names a node >= n");
+            break;
+        }
+        h->m = ms;
+        uint32_t *slo = nullptr, *shi = nullptr;
+        float *weff = nullptr;
+        if ((e = h->alloc(&h->rp, (size_t)n + 1)) || (e = h->alloc(&h->col, 2 * (size_t)ms)) ||
+            (e = h->alloc(&h->wt, 2 * (size_t)ms)) || (e = h->alloc(&h->pos, n)) ||
+            (e = h->alloc(&h->st, 1)) || (e = h->alloc(&slo, ms)) || (e = h->alloc(&shi, ms)) ||
+            (e = h->alloc(&weff, ms)) || (e = alloc_tick_buffers(h))) {
+            cleanup();
+            rc = set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+            break;
+        }
+        cudaMemsetAsync(h->rp, 0, ((size_t)n + 1) * 4, s);
+        if (ms) {
+            k_edge_emit<<<div_up(m, 256), 256, 0, s>>>((uint32_t)m, ek, ev, eflag, eexcl, d_w, prm[P_INFLUENCE],
+                                                          weff, slo, shi, dk, dv, d_err);
+            esort.sort(dk, dv, 2 * ms, 64, s);
+            k_csr<<<div_up(2 * (uint64_t)ms, 256), 256, 0, s>>>(n, 2 * ms, dk, dv, weff, h->rp, h->col, h->wt);
+        }
+        float *d_xyz = nullptr;
+        if ((e = cudaMalloc(&d_xyz, std::max<size_t>(xyz.size(), 1) * 4))) {
+            cleanup();
+            rc = set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+            break;
+        }
+        if (n) {
+            cudaMemcpyAsync(d_xyz, xyz.data(), xyz.size() * 4, cudaMemcpyHostToDevice, s);
+            if (D == 3)
+                k_init_nodes<3><<<div_up(n, 256), 256, 0, s>>>(n, d_xyz, h->rp, h->pos);
+            else
+                k_init_nodes<2><<<div_up(n, 256), 256, 0, s>>>(n, d_xyz, h->rp, h->pos);
+        }
+        DevState init;
+        memset(&init, 0, sizeof init);
+        init.swing = init.traction = init.speed = init.speed_efficiency = 1.0;
+        init.converged = n == 0 ? 1u : 0u;
+        cudaMemcpyAsync(h->st, &init, sizeof init, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(hdr, d_err, sizeof hdr, cudaMemcpyDeviceToHost, s);
+        e = cudaStreamSynchronize(s);
+        cudaFree(d_xyz);
+        cleanup();
+        if (e) {
+            rc = set_err(GR_CUDA_ERROR, cudaGetErrorString(e));
+            break;
+        }
+        if (hdr[0] & 2u) {
+            rc = set_err(GR_INVALID_ARGUMENT, "edge weights must be finite and > 0 when edge_weight_influence != 0");
+            break;
+        }
+    } while (0);
+    if (rc != GR_OK) {
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return ok();
+}
+
+static int tick_impl(gr_fa2 *h, uint32_t ticks, float *dev_out, uint32_t *done) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    DevState s0;
+    if (int c = read_state(h, &s0)) return c;
+    if (h->n && ticks) {
+        if (int c = build_graph(h)) return c;
+        for (uint32_t t = 0; t < ticks; t++) {
+            CU(cudaGraphLaunch(h->exec, h->stream));
+            if (dev_out) {
+                float *o = dev_out + (size_t)t * h->n * h->dim;
+                if (h->dim == 3)
+                    k_export<3><<<div_up(h->n, 256), 256, 0, h->stream>>>(h->n, h->pos, o);
+                else
+                    k_export<2><<<div_up(h->n, 256), 256, 0, h->stream>>>(h->n, h->pos, o);
+            }
+        }
+    }
+    DevState s1;
+    if (int c = read_state(h, &s1)) return c;
+    if (done) *done = s1.iter_no - s0.iter_no;
+    if (int c = check_device(h, s1)) return c;
+    return ok();
+}
+
+// ------------------------------------------------------------------ ABI -----
+
+extern "C" {
+
+uint32_t gr_abi_version(void) { return GR_ABI_VERSION; }
+int gr_last_error(void) { return g_err; }
+const char *gr_last_error_message(void) { return g_msg; }
+int gr_last_error_index(void) { return g_err_index; }
+
+static const char *kLayouts[] = {"layout.forceatlas2.barnes_hut.cuda"};
+
+uint32_t gr_layout_count(void) { return 1; }
+const char *gr_layout_id(uint32_t i) {
+    if (i >= gr_layout_count()) {
+        set_err(GR_INDEX_OUT_OF_RANGE, "layout index past the end");
+        return nullptr;
+    }
+    ok();
+    return kLayouts[i];
+}
+
+uint32_t gr_fa2_param_count(void) { return kNParams; }
+
+int gr_fa2_param_spec(uint32_t i, const char **name, int *kind, double *min, double *max, double *def,
+                      double *step, const char **doc) {
+    if (i >= kNParams) return set_err(GR_INDEX_OUT_OF_RANGE, "parameter index past the end");
+    const Spec &s = kSpecs[i];
+    if (name) *name = s.name;
+    if (kind) *kind = s.kind;
+    if (min) *min = s.min;
+    if (max) *max = s.max;
+    if (def) *def = s.def;
+    if (step) *step = s.step;
+    if (doc) *doc = s.doc;
+    return ok();
+}
+
+int gr_fa2_params_values(const uint8_t *params, size_t params_len, double *values_out) {
+    double v[16];
+    if (int c = params_values(params, params_len, v)) return c;
+    if (values_out) memcpy(values_out, v, kNParams * sizeof(double));
+    return ok();
+}
+
+int gr_fa2_create(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                  const double *weight, const uint8_t *params, size_t params_len, const float *pos0) {
+    return create_impl(out, n, m, src, dst, weight, params, params_len, pos0);
+}
+
+void gr_fa2_destroy(gr_fa2 *h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    delete h;
+}
+
+int gr_fa2_tick(gr_fa2 *h, uint32_t ticks, uint32_t *done) { return tick_impl(h, ticks, nullptr, done); }
+
+int gr_fa2_run(gr_fa2 *h, uint32_t *done) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    return tick_impl(h, (uint32_t)h->prm[P_MAX_ITER], nullptr, done);
+}
+
+int gr_fa2_tick_record(gr_fa2 *h, uint32_t ticks, float *dev_out, uint32_t *done) {
+    if (!dev_out) return set_err(GR_INVALID_ARGUMENT, "dev_out is null");
+    return tick_impl(h, ticks, dev_out, done);
+}
+
+int gr_fa2_positions(gr_fa2 *h, float *out) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    if (!out) return set_err(GR_INVALID_ARGUMENT, "out is null");
+    if (h->n == 0) return ok();
+    float *d = nullptr;
+    CU(cudaMallocAsync((void **)&d, (size_t)h->n * h->dim * 4, h->stream));
+    if (h->dim == 3)
+        k_export<3><<<div_up(h->n, 256), 256, 0, h->stream>>>(h->n, h->pos, d);
+    else
+        k_export<2><<<div_up(h->n, 256), 256, 0, h->stream>>>(h->n, h->pos, d);
+    cudaMemcpyAsync(out, d, (size_t)h->n * h->dim * 4, cudaMemcpyDeviceToHost, h->stream);
+    cudaFreeAsync(d, h->stream);
+    CU(cudaStreamSynchronize(h->stream));
+    for (size_t i = 0; i < (size_t)h->n * h->dim; i++)
+        if (!std::isfinite(out[i])) return set_err(GR_LAYOUT_FAILED, "non-finite position (StageError::NonFinite)");
+    return ok();
+}
+
+int gr_fa2_set_positions(gr_fa2 *h, const float *pos) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    if (!pos) return set_err(GR_INVALID_ARGUMENT, "pos is null");
+    if (h->n == 0) return ok();
+    for (size_t i = 0; i < (size_t)h->n * h->dim; i++)
+        if (!std::isfinite(pos[i])) return set_err(GR_INVALID_ARGUMENT, "non-finite position");
+    float *d = nullptr;
+    CU(cudaMallocAsync((void **)&d, (size_t)h->n * h->dim * 4, h->stream));
+    cudaMemcpyAsync(d, pos, (size_t)h->n * h->dim * 4, cudaMemcpyHostToDevice, h->stream);
+    if (h->dim == 3)
+        k_import<3><<<div_up(h->n, 256), 256, 0, h->stream>>>(h->n, h->pos, d);
+    else
+        k_import<2><<<div_up(h->n, 256), 256, 0, h->stream>>>(h->n, h->pos, d);
+    cudaFreeAsync(d, h->stream);
+    CU(cudaStreamSynchronize(h->stream));
+    return ok();
+}
+
+int gr_fa2_positions_device(gr_fa2 *h, const void **dev_nodes) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    if (!dev_nodes) return set_err(GR_INVALID_ARGUMENT, "dev_nodes is null");
+    *dev_nodes = h->pos;
+    return ok();
+}
+
+int gr_fa2_forces(gr_fa2 *h, float *out) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    if (!out) return set_err(GR_INVALID_ARGUMENT, "out is null");
+    if (h->n == 0) return ok();
+    DevState s0;
+    if (int c = read_state(h, &s0)) return c;
+    // a converged state still answers: evaluate on a copy that is not converged
+    DevState s = s0;
+    s.converged = 0;
+    CU(cudaMemcpyAsync(h->st, &s, sizeof s, cudaMemcpyHostToDevice, h->stream));
+    enqueue(h, true);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(out, h->U, (size_t)h->n * h->dim * 4, cudaMemcpyDeviceToHost, h->stream));
+    DevState s1;
+    if (int c = read_state(h, &s1)) return c;
+    int rc = check_device(h, s1);
+    // restore the speed controller and tick count; keep the interaction counters
+    s0.far_count = s1.far_count;
+    s0.pair_count = s1.pair_count;
+    s0.n_cells = s1.n_cells;
+    s0.n_unique = s1.n_unique;
+    CU(cudaMemcpyAsync(h->st, &s0, sizeof s0, cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    if (rc) return rc;
+    return ok();
+}
+
+int gr_fa2_get_info(gr_fa2 *h, gr_fa2_info *out) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    if (!out) return set_err(GR_INVALID_ARGUMENT, "out is null");
+    DevState s;
+    if (int c = read_state(h, &s)) return c;
+    out->n = h->n;
+    out->dim = (uint32_t)h->dim;
+    out->m = h->m;
+    out->iter_no = s.iter_no;
+    out->converged = s.converged;
+    out->n_cells = s.n_cells;
+    out->n_leaves = s.n_unique;
+    out->swing = s.swing;
+    out->traction = s.traction;
+    out->speed = s.speed;
+    out->speed_efficiency = s.speed_efficiency;
+    out->moved = s.moved;
+    out->far_count = s.far_count;
+    out->pair_count = s.pair_count;
+    out->device_error = s.error;
+    return ok();
+}
+
+int gr_fa2_set_stream(gr_fa2 *h, void *cuda_stream) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    if (h->stream) CU(cudaStreamSynchronize(h->stream));
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    h->own_stream = false;
+    h->stream = (cudaStream_t)cuda_stream;
+    if (h->exec) {
+        cudaGraphExecDestroy(h->exec);
+        h->exec = nullptr;
+    }
+    if (h->graph) {
+        cudaGraphDestroy(h->graph);
+        h->graph = nullptr;
+    }
+    return ok();
+}
+
+int gr_run(const char *layout_id, uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+           const double *weight, const uint8_t *params, size_t params_len, float *out) {
+    if (!layout_id || strcmp(layout_id, kLayouts[0]) != 0)
+        return set_err(GR_UNKNOWN_LAYOUT_ID, "unknown layout id");
+    gr_fa2 *h = nullptr;
+    if (int c = gr_fa2_create(&h, n, m, src, dst, weight, params, params_len, nullptr)) return c;
+    int rc = gr_fa2_run(h, nullptr);
+    if (rc == GR_OK) rc = gr_fa2_positions(h, out);
+    int keep = g_err, keep_i = g_err_index;
+    char msg[256];
+    memcpy(msg, g_msg, sizeof msg);
+    gr_fa2_destroy(h);
+    g_err = keep;
+    g_err_index = keep_i;
+    memcpy(g_msg, msg, sizeof msg);
+    return rc;
+}
+
+}  // extern "C"

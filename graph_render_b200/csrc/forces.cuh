@@ -1,0 +1,200 @@
+// Attraction, gravity, the FP64 swing/traction reductions, the speed controller
+// and the position update.
+//
+// Reference: crates/graph-core/src/layout/forceatlas2/state.rs:152-162 (attraction),
+// 208-251 (gravity), state/schedule.rs:16-77 (swing/traction, estimate_factor,
+// apply_update); the options graph-core leaves at their defaults follow networkx
+// 3.6 `forceatlas2_layout` (networkx/drawing/layout.py:1806-1872): linlog,
+// distributed_action (dissuade hubs), strong_gravity, weighted adjacency.
+//
+// Attraction is a CSR gather: node i sums w_ij * (p_j - p_i) over its own row in
+// a fixed order, so there is no scatter and no float atomic, and the sum is the
+// same every run. Every reduction folds per-block partials in block order in the
+// grid's last block.
+#pragma once
+
+#include "common.cuh"
+
+namespace gr {
+
+constexpr int FRC_THREADS = 256;
+
+struct ForceParams {
+    uint32_t n;
+    float gravity;
+    int lin_log, strong_gravity, dissuade_hubs;
+    double jitter_tolerance;
+};
+
+// schedule.rs:33-60 estimate_factor (networkx's helper), FP64.
+__device__ __forceinline__ void estimate_factor(DevState *st, double n, double jt) {
+    const double swing = st->swing, traction = st->traction;
+    const double opt_jitter = 0.05 * sqrt(n);
+    const double min_jitter = sqrt(opt_jitter);
+    const double min_se = 0.05;
+    const double other = fmin(10.0, opt_jitter * traction / (n * n));
+    double jitter = jt * fmax(min_jitter, other);
+    double se = st->speed_efficiency, speed = st->speed;
+    if (swing / traction > 2.0) {
+        if (se > min_se) se *= 0.5;
+        jitter = fmax(jitter, jt);
+    }
+    const double target = swing == 0.0 ? INFINITY : jitter * se * traction / swing;
+    if (swing > jitter * traction) {
+        if (se > min_se) se *= 0.7;
+    } else if (speed < 1000.0) {
+        se *= 1.3;
+    }
+    speed += fmin(target - speed, 0.5 * speed);
+    st->speed = speed;
+    st->speed_efficiency = se;
+}
+
+// u_i = attraction + repulsion - gravity; per-block FP64 swing and traction;
+// the last block accumulates them into the state (cumulative, state.rs:141-143)
+// and runs estimate_factor.
+template <int D>
+__global__ void __launch_bounds__(FRC_THREADS)
+k_forces(ForceParams P, DevState *st, const float4 *__restrict__ pos, const uint32_t *__restrict__ rp,
+         const uint32_t *__restrict__ col, const float *__restrict__ wt, const float *__restrict__ rep,
+         float *__restrict__ U, double *__restrict__ part, int speed_update) {
+    if (st->converged) return;
+    __shared__ double s_red[32];
+    __shared__ bool s_last;
+    const uint32_t i = blockIdx.x * FRC_THREADS + threadIdx.x;
+    double sw = 0.0, tr = 0.0;
+    if (i < P.n) {
+        const float4 p = pos[i];
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+        const uint32_t e0 = rp[i], e1 = rp[i + 1];
+        for (uint32_t e = e0; e < e1; e++) {
+            const float4 q = pos[col[e]];
+            const float d0 = q.x - p.x, d1 = q.y - p.y, d2 = (D == 3) ? q.z - p.z : 0.f;
+            float c = wt[e];
+            if (P.lin_log) {
+                const float dist = sqrtf(d0 * d0 + d1 * d1 + d2 * d2);
+                c *= dist > 0.f ? log1pf(dist) / dist : 0.f;
+            }
+            a0 += d0 * c;
+            a1 += d1 * c;
+            if (D == 3) a2 += d2 * c;
+        }
+        if (P.dissuade_hubs) {
+            a0 /= p.w;
+            a1 /= p.w;
+            a2 /= p.w;
+        }
+        float u0 = a0 + rep[(size_t)i * D + 0];
+        float u1 = a1 + rep[(size_t)i * D + 1];
+        float u2 = (D == 3) ? a2 + rep[(size_t)i * D + 2] : 0.f;
+        const float c0 = (float)((double)p.x - st->mean[0]);
+        const float c1 = (float)((double)p.y - st->mean[1]);
+        const float c2 = (D == 3) ? (float)((double)p.z - st->mean[2]) : 0.f;
+        const float g = P.gravity * p.w;
+        if (P.strong_gravity) {
+            u0 -= g * c0;
+            u1 -= g * c1;
+            u2 -= g * c2;
+        } else {
+            const float nrm = sqrtf(c0 * c0 + c1 * c1 + c2 * c2);
+            if (nrm > 0.f) {
+                u0 -= g * (c0 / nrm);
+                u1 -= g * (c1 / nrm);
+                u2 -= g * (c2 / nrm);
+            }
+        }
+        U[(size_t)i * D + 0] = u0;
+        U[(size_t)i * D + 1] = u1;
+        if (D == 3) U[(size_t)i * D + 2] = u2;
+        const double m = (double)p.w;
+        const double b0 = (double)p.x - u0, b1 = (double)p.y - u1, b2 = (D == 3) ? (double)p.z - u2 : 0.0;
+        const double g0 = (double)p.x + u0, g1 = (double)p.y + u1, g2 = (D == 3) ? (double)p.z + u2 : 0.0;
+        sw = m * sqrt(b0 * b0 + b1 * b1 + b2 * b2);
+        tr = 0.5 * m * sqrt(g0 * g0 + g1 * g1 + g2 * g2);
+    }
+    if (!speed_update) return;
+    sw = block_sum_d<FRC_THREADS>(sw, s_red);
+    tr = block_sum_d<FRC_THREADS>(tr, s_red);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = sw;
+        part[2 * blockIdx.x + 1] = tr;
+    }
+    if (!last_block_done(&st->counters[1], &s_last)) return;
+    double a = 0.0, b = 0.0;
+    for (uint32_t k = threadIdx.x; k < gridDim.x; k += FRC_THREADS) {
+        a += __ldcg(&part[2 * k]);
+        b += __ldcg(&part[2 * k + 1]);
+    }
+    a = block_sum_d<FRC_THREADS>(a, s_red);
+    b = block_sum_d<FRC_THREADS>(b, s_red);
+    if (threadIdx.x == 0) {
+        st->swing += a;
+        st->traction += b;
+        estimate_factor(st, (double)P.n, P.jitter_tolerance);
+    }
+}
+
+// schedule.rs:62-77 apply_update: factor = speed / (1 + sqrt(speed * m * |u|)),
+// p += u * factor; FP64 sum of |step| decides the 1e-10 early exit
+// (state.rs:122-128).
+template <int D>
+__global__ void __launch_bounds__(FRC_THREADS)
+k_update(uint32_t n, DevState *st, float4 *__restrict__ pos, const float *__restrict__ U,
+         double *__restrict__ part) {
+    if (st->converged) return;
+    __shared__ double s_red[32];
+    __shared__ bool s_last;
+    const uint32_t i = blockIdx.x * FRC_THREADS + threadIdx.x;
+    double step = 0.0;
+    bool bad = false;
+    if (i < n) {
+        const double speed = st->speed;
+        float4 p = pos[i];
+        const double u0 = U[(size_t)i * D], u1 = U[(size_t)i * D + 1], u2 = (D == 3) ? U[(size_t)i * D + 2] : 0.0;
+        const double nrm = sqrt(u0 * u0 + u1 * u1 + u2 * u2);
+        const double factor = speed / (1.0 + sqrt(speed * (double)p.w * nrm));
+        const float d0 = (float)(u0 * factor), d1 = (float)(u1 * factor), d2 = (float)(u2 * factor);
+        p.x += d0;
+        p.y += d1;
+        if (D == 3) p.z += d2;
+        step = fabs((double)d0) + fabs((double)d1) + ((D == 3) ? fabs((double)d2) : 0.0);
+        bad = !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z));
+        pos[i] = p;
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&st->error, (uint32_t)ERR_NONFINITE);
+    step = block_sum_d<FRC_THREADS>(step, s_red);
+    if (threadIdx.x == 0) part[blockIdx.x] = step;
+    if (!last_block_done(&st->counters[2], &s_last)) return;
+    double a = 0.0;
+    for (uint32_t k = threadIdx.x; k < gridDim.x; k += FRC_THREADS) a += __ldcg(&part[k]);
+    a = block_sum_d<FRC_THREADS>(a, s_red);
+    if (threadIdx.x == 0) {
+        st->moved = a;
+        st->iter_no += 1;
+        if (a < 1e-10 || st->error) st->converged = 1;
+    }
+}
+
+// Row-major n x D copy of the float4 positions (the per-tick buffer).
+template <int D>
+__global__ void k_export(uint32_t n, const float4 *__restrict__ pos, float *__restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = pos[i];
+    out[(size_t)i * D] = p.x;
+    out[(size_t)i * D + 1] = p.y;
+    if (D == 3) out[(size_t)i * D + 2] = p.z;
+}
+
+template <int D>
+__global__ void k_import(uint32_t n, float4 *__restrict__ pos, const float *__restrict__ in) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = pos[i];
+    p.x = in[(size_t)i * D];
+    p.y = in[(size_t)i * D + 1];
+    p.z = (D == 3) ? in[(size_t)i * D + 2] : 0.f;
+    pos[i] = p;
+}
+
+}  // namespace gr

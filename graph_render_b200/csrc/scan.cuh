@@ -1,0 +1,142 @@
+// Device-wide exclusive scan of uint32 counts (reduce, scan-of-block-sums,
+// downsweep). The element count can live in device memory so the launches are
+// sized for a host-side upper bound and stay graph-capturable while the real
+// count changes from tick to tick.
+#pragma once
+
+#include "common.cuh"
+
+namespace gr {
+
+constexpr int SC_THREADS = 256;
+constexpr int SC_ITEMS = 8;
+constexpr int SC_TILE = SC_THREADS * SC_ITEMS;
+
+__device__ __forceinline__ uint32_t scan_count(uint32_t n_host, const uint32_t *n_dev, uint32_t add) {
+    return n_dev ? *n_dev + add : n_host;
+}
+
+__global__ void __launch_bounds__(SC_THREADS)
+sc_reduce(const uint32_t *__restrict__ in, uint32_t n_host, const uint32_t *n_dev, uint32_t n_add,
+          uint32_t *__restrict__ bsum, const uint32_t *skip) {
+    if (skip && *skip) return;
+    uint32_t n = scan_count(n_host, n_dev, n_add);
+    __shared__ uint32_t s[SC_THREADS / GR_WARP];
+    uint64_t base = (uint64_t)blockIdx.x * SC_TILE;
+    uint32_t v = 0;
+    if (base < n) {
+#pragma unroll
+        for (int r = 0; r < SC_ITEMS; r++) {
+            uint64_t i = base + (uint64_t)r * SC_THREADS + threadIdx.x;
+            if (i < n) v += in[i];
+        }
+    }
+    v = __reduce_add_sync(GR_FULL, v);
+    if (threadIdx.x % GR_WARP == 0) s[threadIdx.x / GR_WARP] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < SC_THREADS / GR_WARP; w++) t += s[w];
+        bsum[blockIdx.x] = t;
+    }
+}
+
+// Single block: exclusive scan of the block sums in place; the grand total goes
+// to *total (and optionally to *total2).
+__global__ void __launch_bounds__(1024)
+sc_blocks(uint32_t *__restrict__ bsum, uint32_t nb, uint32_t *total, uint32_t *total2,
+          const uint32_t *skip) {
+    if (skip && *skip) return;
+    __shared__ uint32_t s_w[32];
+    const int t = threadIdx.x, lane = t % GR_WARP, w = t / GR_WARP;
+    uint32_t running = 0;
+    for (uint32_t off = 0; off < nb; off += 1024) {
+        uint32_t i = off + t;
+        uint32_t x = i < nb ? bsum[i] : 0u;
+        uint32_t s = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(GR_FULL, s, o);
+            if (lane >= o) s += y;
+        }
+        __syncthreads();
+        if (lane == 31) s_w[w] = s;
+        __syncthreads();
+        uint32_t wb = 0, tot = 0;
+        for (int k = 0; k < 32; k++) {
+            uint32_t z = s_w[k];
+            if (k < w) wb += z;
+            tot += z;
+        }
+        if (i < nb) bsum[i] = running + wb + s - x;
+        running += tot;
+    }
+    if (t == 0) {
+        if (total) *total = running;
+        if (total2) *total2 = running;
+    }
+}
+
+__global__ void __launch_bounds__(SC_THREADS)
+sc_down(const uint32_t *__restrict__ in, uint32_t *__restrict__ out, uint32_t n_host,
+        const uint32_t *n_dev, uint32_t n_add, const uint32_t *__restrict__ bsum, const uint32_t *skip) {
+    if (skip && *skip) return;
+    uint32_t n = scan_count(n_host, n_dev, n_add);
+    uint64_t base = (uint64_t)blockIdx.x * SC_TILE;
+    if (base >= n) return;
+    __shared__ uint32_t s_w[SC_THREADS / GR_WARP];
+    const int t = threadIdx.x, lane = t % GR_WARP, w = t / GR_WARP;
+    // blocked arrangement: thread t owns items [t*ITEMS, t*ITEMS+ITEMS)
+    uint32_t x[SC_ITEMS];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int r = 0; r < SC_ITEMS; r++) {
+        uint64_t i = base + (uint64_t)t * SC_ITEMS + r;
+        x[r] = i < n ? in[i] : 0u;
+        sum += x[r];
+    }
+    uint32_t s = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(GR_FULL, s, o);
+        if (lane >= o) s += y;
+    }
+    if (lane == 31) s_w[w] = s;
+    __syncthreads();
+    uint32_t wb = 0;
+    for (int k = 0; k < w; k++) wb += s_w[k];
+    uint32_t run = bsum[blockIdx.x] + wb + s - sum;
+#pragma unroll
+    for (int r = 0; r < SC_ITEMS; r++) {
+        uint64_t i = base + (uint64_t)t * SC_ITEMS + r;
+        if (i < n) out[i] = run;
+        run += x[r];
+    }
+}
+
+// Exclusive scan of in[0..n) into out[0..n) (in == out allowed); out[n] is not
+// written, the total goes to *total. n = n_host, or *n_dev + n_add when n_dev
+// is given (n_host is then the launch bound).
+struct Scanner {
+    uint32_t cap = 0, nb = 0;
+    uint32_t *bsum = nullptr;
+    cudaError_t init(uint32_t capacity) {
+        cap = capacity ? capacity : 1;
+        nb = div_up(cap, SC_TILE);
+        return cudaMalloc(&bsum, (size_t)nb * sizeof(uint32_t));
+    }
+    void release() {
+        cudaFree(bsum);
+        bsum = nullptr;
+    }
+    void scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev, uint32_t n_add,
+              uint32_t *total, uint32_t *total2, cudaStream_t s, const uint32_t *skip = nullptr) {
+        if (n_host == 0) return;
+        uint32_t b = div_up(n_host, SC_TILE);
+        sc_reduce<<<b, SC_THREADS, 0, s>>>(in, n_host, n_dev, n_add, bsum, skip);
+        sc_blocks<<<1, 1024, 0, s>>>(bsum, b, total, total2, skip);
+        sc_down<<<b, SC_THREADS, 0, s>>>(in, out, n_host, n_dev, n_add, bsum, skip);
+    }
+};
+
+}  // namespace gr

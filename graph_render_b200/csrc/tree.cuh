@@ -1,0 +1,430 @@
+// Linear quadtree (2D) / octree (3D) build from Morton keys.
+//
+// The reference's tree is d3-quadtree's insertion tree
+// (crates/graph-core/src/layout/force/quadtree.rs:116-195, quadtree/build.rs:26-114):
+// a root square snapped to floor(min) and doubled until it covers every point,
+// split at exact midpoints, so every cell is a dyadic square of the root. A key
+// that interleaves the points' dyadic coordinates in that root square
+// (bit a of each D-bit group = "x_a >= midpoint", the reference's slot order,
+// quadtree/bounds.rs:34-50) therefore sorts the points into the reference's own
+// leaf preorder (quadtree/preorder.rs:56-114), and the cells that branch are
+// exactly the reference's cells that hold two or more distinct keys.
+//
+// Build, all integer except the FP64 sums:
+//   keys -> LSD radix sort -> unique keys (leaves) -> Karras binary radix tree
+//   over the unique keys -> FP64 mass / mass-moment sums bottom-up ->
+//   quad/oct cells = binary nodes whose level (common prefix / D) differs from
+//   their parent's -> preorder index of every cell from an exclusive scan of
+//   "cells starting at leaf s" -> skip(cell) = P[last leaf + 1].
+// A chain of single-child cells in the reference collapses to its deepest
+// member here; the walk's far test is monotone in the cell width and the chain
+// shares one mass and centre, so the collapsed cell opens and approximates
+// exactly where the chain would.
+#pragma once
+
+#include "common.cuh"
+
+namespace gr {
+
+template <int D> struct Levels;
+template <> struct Levels<2> { static constexpr int L = 32; };  // 64-bit keys
+template <> struct Levels<3> { static constexpr int L = 21; };  // 63-bit keys
+
+__device__ __forceinline__ uint64_t spread2(uint64_t x) {  // 32 bits -> even bits
+    x &= 0xffffffffull;
+    x = (x | (x << 16)) & 0x0000ffff0000ffffull;
+    x = (x | (x << 8)) & 0x00ff00ff00ff00ffull;
+    x = (x | (x << 4)) & 0x0f0f0f0f0f0f0f0full;
+    x = (x | (x << 2)) & 0x3333333333333333ull;
+    x = (x | (x << 1)) & 0x5555555555555555ull;
+    return x;
+}
+
+__device__ __forceinline__ uint64_t spread3(uint64_t x) {  // 21 bits -> every third bit
+    x &= 0x1fffffull;
+    x = (x | (x << 32)) & 0x001f00000000ffffull;
+    x = (x | (x << 16)) & 0x001f0000ff0000ffull;
+    x = (x | (x << 8)) & 0x100f00f00f00f00full;
+    x = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
+    x = (x | (x << 2)) & 0x1249249249249249ull;
+    return x;
+}
+
+// ------------------------------------------------------------------ bounds --
+
+constexpr int BND_THREADS = 256;
+
+// Extent and FP64 coordinate sums of the positions; the last block turns them
+// into the root square (quadtree.rs:157-195 cover, both corners) and the mean
+// gravity pulls toward (state.rs:208-218).
+template <int D>
+__global__ void __launch_bounds__(BND_THREADS)
+k_bounds(const float4 *__restrict__ pos, uint32_t n, DevState *st, double *__restrict__ part) {
+    if (st->converged) return;
+    __shared__ double s_red[32];
+    __shared__ float s_f[2 * D][32];
+    __shared__ bool s_last;
+    float lo[D], hi[D];
+    double sum[D];
+#pragma unroll
+    for (int a = 0; a < D; a++) {
+        lo[a] = INFINITY;
+        hi[a] = -INFINITY;
+        sum[a] = 0.0;
+    }
+    bool bad = false;
+    for (uint32_t i = blockIdx.x * BND_THREADS + threadIdx.x; i < n; i += gridDim.x * BND_THREADS) {
+        float4 p = pos[i];
+        float c[3] = {p.x, p.y, p.z};
+#pragma unroll
+        for (int a = 0; a < D; a++) {
+            if (!isfinite(c[a])) bad = true;
+            lo[a] = fminf(lo[a], c[a]);
+            hi[a] = fmaxf(hi[a], c[a]);
+            sum[a] += (double)c[a];
+        }
+    }
+    if (__syncthreads_or(bad)) {
+        if (threadIdx.x == 0) atomicOr(&st->error, (uint32_t)ERR_NONFINITE);
+    }
+    const int lane = threadIdx.x % GR_WARP, w = threadIdx.x / GR_WARP;
+#pragma unroll
+    for (int a = 0; a < D; a++) {
+        float l = lo[a], h = hi[a];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            l = fminf(l, __shfl_xor_sync(GR_FULL, l, o));
+            h = fmaxf(h, __shfl_xor_sync(GR_FULL, h, o));
+        }
+        if (lane == 0) {
+            s_f[a][w] = l;
+            s_f[D + a][w] = h;
+        }
+    }
+    double tot[D];
+#pragma unroll
+    for (int a = 0; a < D; a++) tot[a] = block_sum_d<BND_THREADS>(sum[a], s_red);
+    if (threadIdx.x == 0) {
+        double *q = part + (size_t)blockIdx.x * 3 * D;
+        for (int a = 0; a < D; a++) {
+            float l = INFINITY, h = -INFINITY;
+            for (int k = 0; k < BND_THREADS / GR_WARP; k++) {
+                l = fminf(l, s_f[a][k]);
+                h = fmaxf(h, s_f[D + a][k]);
+            }
+            q[a] = l;
+            q[D + a] = h;
+            q[2 * D + a] = tot[a];
+        }
+    }
+    if (!last_block_done(&st->counters[0], &s_last)) return;
+    // last block: fold the partials in block order
+    double gl[D], gh[D], gs[D];
+#pragma unroll
+    for (int a = 0; a < D; a++) {
+        gl[a] = INFINITY;
+        gh[a] = -INFINITY;
+        gs[a] = 0.0;
+    }
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += BND_THREADS) {
+        const double *q = part + (size_t)b * 3 * D;
+#pragma unroll
+        for (int a = 0; a < D; a++) {
+            gl[a] = fmin(gl[a], __ldcg(q + a));
+            gh[a] = fmax(gh[a], __ldcg(q + D + a));
+            gs[a] += __ldcg(q + 2 * D + a);
+        }
+    }
+    __shared__ double s_l[D][BND_THREADS], s_h[D][BND_THREADS];
+#pragma unroll
+    for (int a = 0; a < D; a++) {
+        s_l[a][threadIdx.x] = gl[a];
+        s_h[a][threadIdx.x] = gh[a];
+    }
+    double S[D];
+#pragma unroll
+    for (int a = 0; a < D; a++) S[a] = block_sum_d<BND_THREADS>(gs[a], s_red);
+    if (threadIdx.x == 0) {
+        double mn[D], mx[D];
+        for (int a = 0; a < D; a++) {
+            mn[a] = INFINITY;
+            mx[a] = -INFINITY;
+            for (int k = 0; k < BND_THREADS; k++) {
+                mn[a] = fmin(mn[a], s_l[a][k]);
+                mx[a] = fmax(mx[a], s_h[a][k]);
+            }
+        }
+        double z = 1.0;
+        bool grow = true;
+        for (int a = 0; a < D; a++) st->root0[a] = floor(mn[a]);
+        while (grow) {
+            grow = false;
+            for (int a = 0; a < D; a++)
+                if (mx[a] >= st->root0[a] + z) grow = true;
+            if (grow) z *= 2.0;
+            if (!isfinite(z)) {
+                atomicOr(&st->error, (uint32_t)ERR_BOUNDS);
+                break;
+            }
+        }
+        st->root_w = z;
+        for (int a = 0; a < D; a++) st->mean[a] = S[a] / (double)n;
+        if (st->error) st->converged = 1;
+    }
+}
+
+// Morton key of every node in the root square: per axis q = floor((x - x0) *
+// 2^L / side), exact in FP64 because the side is a power of two.
+template <int D>
+__global__ void k_keys(const float4 *__restrict__ pos, uint32_t n, const DevState *st,
+                       uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+    if (st->converged) return;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    constexpr int L = Levels<D>::L;
+    const double scale = ldexp(1.0, L) / st->root_w;
+    const double qmax = ldexp(1.0, L) - 1.0;
+    float4 p = pos[i];
+    float c[3] = {p.x, p.y, p.z};
+    uint64_t key = 0;
+#pragma unroll
+    for (int a = 0; a < D; a++) {
+        double q = floor(((double)c[a] - st->root0[a]) * scale);
+        q = fmin(fmax(q, 0.0), qmax);
+        uint64_t qi = (uint64_t)q;
+        key |= (D == 2 ? spread2(qi) : spread3(qi)) << a;
+    }
+    keys[i] = key << (64 - D * L);  // left-aligned: clz of a difference counts levels from the root
+    vals[i] = i;
+}
+
+// Sorted node records and the "first of its key" flags.
+__global__ void k_gather(const float4 *__restrict__ pos, uint32_t n, const DevState *st,
+                         const uint64_t *__restrict__ keys, const uint32_t *__restrict__ perm,
+                         float4 *__restrict__ sp, uint32_t *__restrict__ sorig,
+                         uint32_t *__restrict__ flag) {
+    if (st->converged) return;
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    uint32_t i = perm[p];
+    sp[p] = pos[i];
+    sorig[p] = i;
+    flag[p] = (p == 0 || keys[p] != keys[p - 1]) ? 1u : 0u;
+}
+
+// Unique keys: leaf s starts at the first sorted point with its key.
+__global__ void k_leaves(uint32_t n, const DevState *st, const uint64_t *__restrict__ keys,
+                         const uint32_t *__restrict__ flag, const uint32_t *__restrict__ excl,
+                         uint32_t *__restrict__ leaf_start, uint64_t *__restrict__ ukey,
+                         uint32_t *__restrict__ uid) {
+    if (st->converged) return;
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    uint32_t e = excl[p], f = flag[p];
+    uid[p] = e + f - 1;
+    if (f) {
+        leaf_start[e] = p;
+        ukey[e] = keys[p];
+    }
+    if (p == n - 1) leaf_start[e + f] = n;
+}
+
+// Binary radix tree node arrays (Karras 2012, "Maximizing parallelism in the
+// construction of BVHs, octrees, and k-d trees", HPG): internal node i covers
+// unique leaves [first, last]; children are coded with LEAF_BIT when a leaf.
+constexpr uint32_t LEAF_BIT = 0x80000000u;
+
+struct BinTree {
+    uint32_t *first, *last, *left, *right;
+    int32_t *delta;       // common prefix length of the node's keys
+    int32_t *int_parent;  // internal node -> parent (-1 at the root)
+    int32_t *leaf_parent; // leaf -> parent (-1 when the tree is one leaf)
+    uint32_t *visit;      // bottom-up arrival tickets
+};
+
+__device__ __forceinline__ int kdelta(const uint64_t *__restrict__ k, int32_t a, int32_t b, int32_t nu) {
+    if (b < 0 || b >= nu) return -1;
+    return __clzll(k[a] ^ k[b]);
+}
+
+__global__ void k_karras(const DevState *st, const uint64_t *__restrict__ k, BinTree t) {
+    if (st->converged) return;
+    const int32_t nu = (int32_t)st->n_unique;
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0 && nu == 1) t.leaf_parent[0] = -1;
+    if (i >= nu - 1) return;
+    const int dir = (kdelta(k, i, i + 1, nu) - kdelta(k, i, i - 1, nu)) > 0 ? 1 : -1;
+    const int dmin = kdelta(k, i, i - dir, nu);
+    int32_t lmax = 2;
+    while (kdelta(k, i, i + lmax * dir, nu) > dmin) lmax <<= 1;
+    int32_t l = 0;
+    for (int32_t s = lmax >> 1; s >= 1; s >>= 1)
+        if (kdelta(k, i, i + (l + s) * dir, nu) > dmin) l += s;
+    const int32_t j = i + l * dir;
+    const int dnode = kdelta(k, i, j, nu);
+    int32_t s = 0;
+    int32_t step = l;
+    do {
+        step = (step + 1) >> 1;
+        if (kdelta(k, i, i + (s + step) * dir, nu) > dnode) s += step;
+    } while (step > 1);
+    const int32_t gamma = i + s * dir + (dir < 0 ? -1 : 0);
+    const int32_t first = min(i, j), last = max(i, j);
+    t.first[i] = (uint32_t)first;
+    t.last[i] = (uint32_t)last;
+    t.delta[i] = dnode;
+    t.visit[i] = 0;
+    if (first == gamma) {
+        t.left[i] = (uint32_t)gamma | LEAF_BIT;
+        t.leaf_parent[gamma] = i;
+    } else {
+        t.left[i] = (uint32_t)gamma;
+        t.int_parent[gamma] = i;
+    }
+    if (last == gamma + 1) {
+        t.right[i] = (uint32_t)(gamma + 1) | LEAF_BIT;
+        t.leaf_parent[gamma + 1] = i;
+    } else {
+        t.right[i] = (uint32_t)(gamma + 1);
+        t.int_parent[gamma + 1] = i;
+    }
+    if (i == 0) t.int_parent[0] = -1;
+}
+
+// Leaf sums (mass, mass-weighted coordinates, FP64) and the bottom-up pass:
+// the second thread to reach a node sums its two children, left then right, so
+// every node's value is independent of arrival order.
+template <int D>
+__global__ void k_aggregate(DevState *st, const float4 *__restrict__ sp,
+                            const uint32_t *__restrict__ leaf_start, BinTree t,
+                            Body *__restrict__ leaf_body, Body *__restrict__ int_body,
+                            uint8_t *__restrict__ leaf_coinc) {
+    if (st->converged) return;
+    const uint32_t nu = st->n_unique;
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nu) return;
+    const uint32_t a0 = leaf_start[s], a1 = leaf_start[s + 1];
+    Body b{0.0, 0.0, 0.0, 0.0};
+    const float4 f0 = sp[a0];
+    bool coinc = true;
+    for (uint32_t q = a0; q < a1; q++) {
+        float4 p = sp[q];
+        double m = (double)p.w;
+        b.m += m;
+        b.c0 += m * (double)p.x;
+        b.c1 += m * (double)p.y;
+        if (D == 3) b.c2 += m * (double)p.z;
+        coinc = coinc && p.x == f0.x && p.y == f0.y && (D == 2 || p.z == f0.z);
+    }
+    body_store(&leaf_body[s], b);
+    leaf_coinc[s] = coinc ? 1 : 0;
+    int32_t node = t.leaf_parent[s];
+    // a binary radix tree over 64-bit keys is at most 64 levels deep
+    for (int depth = 0; node >= 0; depth++) {
+        if (depth > 66) {
+            atomicOr(&st->error, (uint32_t)ERR_TREE);
+            return;
+        }
+        __threadfence();
+        if (atomicAdd(&t.visit[node], 1u) == 0u) return;
+        __threadfence();
+        uint32_t l = t.left[node], r = t.right[node];
+        Body bl = (l & LEAF_BIT) ? body_load_cg(&leaf_body[l & ~LEAF_BIT]) : body_load_cg(&int_body[l]);
+        Body br = (r & LEAF_BIT) ? body_load_cg(&leaf_body[r & ~LEAF_BIT]) : body_load_cg(&int_body[r]);
+        body_store(&int_body[node], body_add(bl, br));
+        node = t.int_parent[node];
+    }
+}
+
+template <int D>
+__device__ __forceinline__ bool is_cell(const BinTree &t, int32_t node) {
+    int32_t par = t.int_parent[node];
+    return par < 0 || (t.delta[node] / D) != (t.delta[par] / D);
+}
+
+// cells_at[s]: how many cells start at unique leaf s (the leaf itself plus the
+// cell ancestors whose range begins there).
+template <int D>
+__global__ void k_count(const DevState *st, BinTree t, uint32_t *__restrict__ cells_at) {
+    if (st->converged) return;
+    const uint32_t nu = st->n_unique;
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nu) return;
+    uint32_t c = 1;
+    int32_t par = t.leaf_parent[s];
+    for (int depth = 0; par >= 0 && t.first[par] == s && depth <= 66; depth++) {
+        if (is_cell<D>(t, par)) c++;
+        par = t.int_parent[par];
+    }
+    cells_at[s] = c;
+}
+
+// Cell record, 2D: A = {cx, cy, mass, w^2}, B = {cx_lo, cy_lo, skip | -count, start}.
+// 3D: A = {cx, cy, cz, mass}, B = {cx_lo, cy_lo, cz_lo, w^2}, C = {skip | -count, start}.
+// The centre is an FP32 hi/lo pair of the FP64 centre of mass, so a node at
+// 1e4 still resolves a nearby centre to ~1e-3 ulp instead of a whole FP32 ulp.
+struct Cells {
+    float4 *A, *B;
+    int2 *C;
+};
+
+template <int D>
+__device__ __forceinline__ void write_cell(Cells c, uint32_t idx, const Body &b, int level, double root_w,
+                                           int32_t skip_or_count, uint32_t start) {
+    double inv = 1.0 / b.m;
+    double cc[3] = {b.c0 * inv, b.c1 * inv, b.c2 * inv};
+    float hi[3], lo[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        hi[a] = (float)cc[a];
+        lo[a] = (float)(cc[a] - (double)hi[a]);
+    }
+    double w = ldexp(root_w, -level);
+    float w2 = (float)(w * w);
+    if (D == 2) {
+        c.A[idx] = make_float4(hi[0], hi[1], (float)b.m, w2);
+        c.B[idx] = make_float4(lo[0], lo[1], __int_as_float(skip_or_count), __uint_as_float(start));
+    } else {
+        c.A[idx] = make_float4(hi[0], hi[1], hi[2], (float)b.m);
+        c.B[idx] = make_float4(lo[0], lo[1], lo[2], w2);
+        c.C[idx] = make_int2(skip_or_count, (int32_t)start);
+    }
+}
+
+// Writes every cell at its preorder index: leaf s at P[s] + cells_at[s] - 1,
+// its cell ancestors starting at s above it, skip(cell) = P[last leaf + 1].
+// A leaf of coincident points sits one level below its parent cell (where the
+// reference chains them); a leaf of distinct points the key could not separate
+// sits at the key's last level.
+template <int D>
+__global__ void k_assign(const DevState *st, BinTree t, const uint32_t *__restrict__ P,
+                         const uint32_t *__restrict__ cells_at, const uint32_t *__restrict__ leaf_start,
+                         const Body *__restrict__ leaf_body, const Body *__restrict__ int_body,
+                         const uint8_t *__restrict__ leaf_coinc, Cells cells,
+                         uint32_t *__restrict__ leaf_pre, DevState *stw) {
+    if (st->converged) return;
+    const uint32_t nu = st->n_unique;
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nu) return;
+    constexpr int L = Levels<D>::L;
+    const double rw = st->root_w;
+    uint32_t idx = P[s] + cells_at[s] - 1;
+    int32_t par = t.leaf_parent[s];
+    int level = 0;
+    if (par >= 0) level = leaf_coinc[s] ? t.delta[par] / D + 1 : L;
+    uint32_t a0 = leaf_start[s], a1 = leaf_start[s + 1];
+    write_cell<D>(cells, idx, leaf_body[s], level, rw, -(int32_t)(a1 - a0), a0);
+    leaf_pre[s] = idx;
+    for (int depth = 0; par >= 0 && t.first[par] == s && depth <= 66; depth++) {
+        if (is_cell<D>(t, par)) {
+            idx--;
+            uint32_t end = t.last[par] + 1;
+            uint32_t skip = end == nu ? st->n_cells : P[end];
+            write_cell<D>(cells, idx, int_body[par], t.delta[par] / D, rw, (int32_t)skip, a0);
+        }
+        par = t.int_parent[par];
+    }
+    if (idx != P[s]) atomicOr(&stw->error, (uint32_t)ERR_TREE);
+}
+
+}  // namespace gr

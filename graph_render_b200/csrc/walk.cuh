@@ -1,0 +1,141 @@
+// Repulsion: warp-cooperative stackless preorder walk of the linear tree.
+//
+// Reference: crates/graph-core/src/layout/forceatlas2/state/barnes_hut.rs:115-184.
+// Per node, in preorder: a cell that does not hold the node, with d2 > 0 and
+// w^2 < theta^2 d2 (d to the cell's centre of mass, w its side), acts as one body
+// of its mass and the walk skips its subtree; a leaf that is not far acts pair by
+// pair (with the coincident-pair jiggle, state.rs:185-203); anything else opens.
+//
+// On the GPU a warp walks 32 consecutive Morton-sorted nodes together. The cell
+// index k is warp-uniform; each lane keeps `resume`, the first cell index it
+// takes part in again after it approximated a subtree (its skip). The warp
+// descends (k + 1) when any participating lane opens the cell and jumps to
+// skip otherwise; lanes never see a cell their own walk would not visit, so each
+// node's interaction set is exactly the per-node walk's. Cell loads are
+// warp-uniform broadcasts of float4 records; leaf points come from the sorted
+// float4 node array.
+#pragma once
+
+#include "common.cuh"
+#include "tree.cuh"
+
+namespace gr {
+
+constexpr int WALK_THREADS = 128;
+
+struct WalkParams {
+    uint32_t n;
+    float kr;      // scaling_ratio
+    float theta2;  // theta^2
+    uint32_t seed;
+};
+
+template <int D>
+__global__ void __launch_bounds__(WALK_THREADS)
+k_walk(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 *__restrict__ sp,
+       const uint32_t *__restrict__ sorig, const uint32_t *__restrict__ uid,
+       const uint32_t *__restrict__ leaf_pre, float *__restrict__ rep, DevState *stw) {
+    if (st->converged) return;
+    const uint32_t n = P.n;
+    const uint32_t ncells = st->n_cells;
+    const uint32_t iter = st->iter_no;
+    const uint32_t p = blockIdx.x * WALK_THREADS + threadIdx.x;
+    const bool valid = p < n;
+    if (__all_sync(GR_FULL, !valid)) return;
+    float4 me = valid ? sp[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t mylp = valid ? leaf_pre[uid[p]] : 0xffffffffu;
+    const uint32_t oi = valid ? sorig[p] : 0u;
+    uint32_t resume = valid ? 0u : 0xffffffffu;
+    float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+    uint32_t nfar = 0, npair = 0;
+    const float kr = P.kr, th2 = P.theta2;
+
+    uint32_t k = 0;
+    while (k < ncells) {
+        const float4 A = __ldg(&cells.A[k]);
+        const float4 B = __ldg(&cells.B[k]);
+        int32_t sk;
+        uint32_t start;
+        float cx, cy, cz, cm, w2, lx, ly, lz;
+        if (D == 2) {
+            cx = A.x; cy = A.y; cz = 0.f; cm = A.z; w2 = A.w;
+            lx = B.x; ly = B.y; lz = 0.f;
+            sk = __float_as_int(B.z);
+            start = __float_as_uint(B.w);
+        } else {
+            const int2 Cc = __ldg(&cells.C[k]);
+            cx = A.x; cy = A.y; cz = A.z; cm = A.w;
+            lx = B.x; ly = B.y; lz = B.z; w2 = B.w;
+            sk = Cc.x;
+            start = (uint32_t)Cc.y;
+        }
+        const bool leaf = sk < 0;
+        uint32_t skip = leaf ? k + 1 : (uint32_t)sk;
+        if (skip <= k || skip > ncells) {  // malformed cell: record it, keep the walk finite
+            if ((threadIdx.x % GR_WARP) == 0) atomicOr(&stw->error, (uint32_t)ERR_TREE);
+            skip = k + 1;
+        }
+        const bool active = resume <= k;
+        const bool holds = (k <= mylp) && (mylp < skip);
+        const float dx = (me.x - cx) - lx;
+        const float dy = (me.y - cy) - ly;
+        const float dz = (D == 3) ? (me.z - cz) - lz : 0.f;
+        const float d2 = (D == 3) ? dx * dx + dy * dy + dz * dz : dx * dx + dy * dy;
+        const bool far = active && !holds && d2 > 0.f && w2 < th2 * d2;
+        if (far) {
+            const float f = me.w * cm / d2 * kr;
+            f0 += dx * f;
+            f1 += dy * f;
+            if (D == 3) f2 += dz * f;
+            resume = skip;
+            nfar++;
+        }
+        const bool open = active && !far;
+        if (leaf) {
+            if (__any_sync(GR_FULL, open)) {
+                int32_t cnt = -sk;
+                if (start >= n || (uint32_t)cnt > n - start) {
+                    if ((threadIdx.x % GR_WARP) == 0) atomicOr(&stw->error, (uint32_t)ERR_TREE);
+                    cnt = 0;
+                }
+                for (int32_t q = 0; q < cnt; q++) {
+                    const uint32_t jp = start + (uint32_t)q;
+                    const float4 o = __ldg(&sp[jp]);
+                    if (open && jp != p) {
+                        float ex = me.x - o.x, ey = me.y - o.y, ez = (D == 3) ? me.z - o.z : 0.f;
+                        if (ex == 0.f && ey == 0.f && (D == 2 || ez == 0.f)) {
+                            // repel_delta's jiggle, taken from the lower index
+                            const uint32_t oj = __ldg(&sorig[jp]);
+                            const float sg = oi < oj ? 1.f : -1.f;
+                            ex = sg * (float)jiggle(P.seed, iter, 0, oi, oj);
+                            ey = sg * (float)jiggle(P.seed, iter, 1, oi, oj);
+                            if (D == 3) ez = sg * (float)jiggle(P.seed, iter, 2, oi, oj);
+                        }
+                        const float e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
+                        const float f = me.w * o.w / e2 * kr;
+                        f0 += ex * f;
+                        f1 += ey * f;
+                        if (D == 3) f2 += ez * f;
+                        npair++;
+                    }
+                }
+            }
+            k = k + 1;
+        } else {
+            k = __any_sync(GR_FULL, open) ? k + 1 : skip;
+        }
+    }
+    if (valid) {
+        rep[(size_t)oi * D + 0] = f0;
+        rep[(size_t)oi * D + 1] = f1;
+        if (D == 3) rep[(size_t)oi * D + 2] = f2;
+    }
+    nfar = __reduce_add_sync(GR_FULL, nfar);
+    npair = __reduce_add_sync(GR_FULL, npair);
+    if ((threadIdx.x % GR_WARP) == 0) {
+        atomicAdd(&stw->far_count, (unsigned long long)nfar);
+        atomicAdd(&stw->pair_count, (unsigned long long)npair);
+    }
+}
+
+}  // namespace gr

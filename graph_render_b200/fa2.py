@@ -1,0 +1,153 @@
+"""ForceAtlas2 / Barnes-Hut on the GPU, through the C ABI.
+
+``Fa2`` owns one engine handle (``gr_fa2_create`` .. ``gr_fa2_destroy``) and
+exposes the per-tick surface the reference lacks (``tick``, ``positions``,
+``forces``, ``tick_record``); ``run_values`` is the registry's
+``Capability::run_values`` for ``layout.forceatlas2.barnes_hut.cuda``
+(crates/graph-core/src/layout/forceatlas2.rs:51-61 ``ForceAtlas2BarnesHut::run``
+then ``settle``).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, Optional, Sequence, Union
+
+import numpy as np
+
+from . import _native as N
+from .registry import Geometry, StageError, Topology, encode_params
+
+PARAM_NAMES = ("max_iter", "jitter_tolerance", "scaling_ratio", "gravity", "seed", "dim", "theta",
+               "lin_log", "strong_gravity", "dissuade_hubs", "edge_weight_influence")
+DEFAULTS = dict(max_iter=100, jitter_tolerance=1.0, scaling_ratio=2.0, gravity=1.0, seed=0, dim=2,
+                theta=0.8, lin_log=0, strong_gravity=0, dissuade_hubs=0, edge_weight_influence=0.0)
+
+
+def params_bytes(params: Union[None, bytes, Dict[str, float], Sequence[float]] = None, **kw) -> bytes:
+    """A parameter buffer from a dict / keywords (unnamed ones at their defaults)."""
+    if isinstance(params, (bytes, bytearray)):
+        return bytes(params)
+    vals = dict(DEFAULTS)
+    if isinstance(params, dict):
+        vals.update(params)
+    elif params is not None:
+        return encode_params(list(params))
+    vals.update(kw)
+    unknown = set(vals) - set(PARAM_NAMES)
+    if unknown:
+        raise KeyError(f"unknown parameters {sorted(unknown)}")
+    return encode_params([vals[k] for k in PARAM_NAMES])
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Fa2:
+    """One graph's layout state on the GPU."""
+
+    def __init__(self, n: int, src, dst, weight=None, params=None, pos0=None, **kw):
+        L = N.lib()
+        self._L = L
+        self.n = int(n)
+        src = np.ascontiguousarray(src, np.uint32)
+        dst = np.ascontiguousarray(dst, np.uint32)
+        if len(src) != len(dst):
+            raise ValueError("src and dst differ in length")
+        w = None if weight is None else np.ascontiguousarray(weight, np.float64)
+        pb = params_bytes(params, **kw)
+        self.params_buffer = pb
+        vals = (C.c_double * 11)()
+        N.check(L.gr_fa2_params_values(C.c_char_p(pb) if pb else None, len(pb), vals))
+        self.values = list(vals)
+        self.dim = int(self.values[5])
+        p0 = None
+        if pos0 is not None:
+            p0 = np.ascontiguousarray(pos0, np.float32).reshape(self.n, self.dim)
+        h = C.c_void_p()
+        N.check(L.gr_fa2_create(C.byref(h), self.n, len(src), _ptr(src), _ptr(dst), _ptr(w),
+                                C.c_char_p(pb) if pb else None, len(pb), _ptr(p0)))
+        self.h = h
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self._L.gr_fa2_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def tick(self, ticks: int = 1) -> int:
+        done = C.c_uint32()
+        N.check(self._L.gr_fa2_tick(self.h, int(ticks), C.byref(done)))
+        return done.value
+
+    def run(self) -> int:
+        done = C.c_uint32()
+        N.check(self._L.gr_fa2_run(self.h, C.byref(done)))
+        return done.value
+
+    def tick_record(self, ticks: int, dev_out_ptr: int) -> int:
+        """Per-tick positions into a device buffer of ticks * n * dim float32."""
+        done = C.c_uint32()
+        N.check(self._L.gr_fa2_tick_record(self.h, int(ticks), C.c_void_p(dev_out_ptr), C.byref(done)))
+        return done.value
+
+    def positions(self) -> np.ndarray:
+        out = np.zeros((self.n, self.dim), np.float32)
+        N.check(self._L.gr_fa2_positions(self.h, _ptr(out)))
+        return out
+
+    def set_positions(self, pos) -> None:
+        pos = np.ascontiguousarray(pos, np.float32).reshape(self.n, self.dim)
+        N.check(self._L.gr_fa2_set_positions(self.h, _ptr(pos)))
+
+    def device_nodes(self) -> int:
+        p = C.c_void_p()
+        N.check(self._L.gr_fa2_positions_device(self.h, C.byref(p)))
+        return int(p.value or 0)
+
+    def forces(self) -> np.ndarray:
+        out = np.zeros((self.n, self.dim), np.float32)
+        N.check(self._L.gr_fa2_forces(self.h, _ptr(out)))
+        return out
+
+    def info(self) -> dict:
+        inf = N.Info()
+        N.check(self._L.gr_fa2_get_info(self.h, C.byref(inf)))
+        return inf.as_dict()
+
+    def set_stream(self, stream_ptr: int) -> None:
+        N.check(self._L.gr_fa2_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+
+def run_values(topology: Topology, values) -> Geometry:
+    """Capability::run_values for layout.forceatlas2.barnes_hut.cuda: create,
+    run max_iter ticks, settle (NonFinite refused), release."""
+    pb = encode_params(values)
+    try:
+        with Fa2(topology.node_count, topology.source, topology.target, topology.strength, params=pb) as eng:
+            eng.run()
+            pos = eng.positions()
+    except N.EngineError as e:
+        if e.code == N.GR_LAYOUT_FAILED:
+            raise StageError("NonFinite", "node.x", code=e.code) from None
+        raise
+    return Geometry.points(pos)
+
+
+def layout(topology: Topology, params=None, **kw) -> Geometry:
+    """One-shot run of the registered FA2 layout with a parameter buffer / dict."""
+    from .registry import find, FA2_ID
+
+    return find(FA2_ID).run_params(topology, params_bytes(params, **kw))

@@ -1,0 +1,146 @@
+/*
+ * graph_cuda.h — C ABI of the B200 (sm_100a) ForceAtlas2 / Barnes-Hut engine.
+ *
+ * The engine is a drop-in for graph-core's layout-registry row
+ * `layout.forceatlas2.barnes_hut` (crates/graph-core/src/registry/layouts.rs:264-267),
+ * reached in the reference through `Capability::run_params(&Topology, &[u8])`
+ * (crates/graph-core/src/registry/params.rs:156-181) from `gm_run`
+ * (crates/graph-wasm/src/exports/build.rs:69-101). It registers under its own id,
+ * "layout.forceatlas2.barnes_hut.cuda", as the reference's own-id rule for a GPU
+ * tier asks (docs/decisions/gpu-force-tier.md:34-38).
+ *
+ * Conventions (mirroring the reference's wasm ABI, docs/contract/wasm-abi.md):
+ *   - Every call returns a status code; 0 is success. The numbering is graph-wasm's
+ *     `Code` (crates/graph-wasm/src/errors.rs:18-122); gr_last_error() returns the
+ *     last call's code and gr_last_error_message() a one-line reason.
+ *   - Parameters travel as little-endian f64 values in schema order
+ *     (crates/graph-contract/src/params.rs:154-170): an empty buffer means the
+ *     defaults; a wrong length is refused (GR_PARAMS_MALFORMED); a non-finite,
+ *     out-of-range, non-integral Int or non-0/1 Bool value is refused
+ *     (GR_PARAM_OUT_OF_RANGE, index in gr_last_error_index()) and never clamped.
+ *     The first five values are the reference's own FA2 schema
+ *     (crates/graph-core/src/registry/tunable.rs:229-240); the rest are appended, so
+ *     a reference-length (5-value) buffer keeps its meaning.
+ *   - Buffers are copied in; the callee never frees a caller's buffer.
+ *   - Positions are FP32, row-major n x dim, in topology node order
+ *     (crates/graph-core/src/layout/mod.rs:54-66 Geometry columns, interleaved).
+ */
+#ifndef GRAPH_CUDA_H
+#define GRAPH_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GR_ABI_VERSION 1
+
+/* status codes (graph-wasm Code numbering; >= 100 are this library's own) */
+#define GR_OK 0
+#define GR_INVALID_HANDLE 1
+#define GR_ALLOC_FAILED 2
+#define GR_UNKNOWN_LAYOUT_ID 5
+#define GR_LAYOUT_FAILED 8
+#define GR_INDEX_OUT_OF_RANGE 12
+#define GR_PARAM_OUT_OF_RANGE 20
+#define GR_PARAMS_MALFORMED 21
+#define GR_PARAMS_NOT_ACCEPTED 22
+#define GR_INVALID_ARGUMENT 100
+#define GR_CUDA_ERROR 101
+#define GR_DEVICE_FAULT 102
+
+/* parameter kinds (graph-contract ParamKind tags) */
+#define GR_KIND_INT 0
+#define GR_KIND_FLOAT 1
+#define GR_KIND_BOOL 2
+
+typedef struct gr_fa2 gr_fa2;
+
+typedef struct gr_fa2_info {
+    uint32_t n;              /* nodes */
+    uint32_t dim;            /* 2 or 3 */
+    uint64_t m;              /* simple edges */
+    uint32_t iter_no;        /* ticks completed */
+    uint32_t converged;      /* a tick moved the layout by < 1e-10 (state.rs:122-128) */
+    uint32_t n_cells;        /* tree cells in the last tick */
+    uint32_t n_leaves;       /* distinct keys (leaves) in the last tick */
+    double swing, traction;  /* cumulative (state.rs:141-143) */
+    double speed, speed_efficiency;
+    double moved;            /* last tick's summed |step| */
+    uint64_t far_count;      /* far-cell interactions since creation */
+    uint64_t pair_count;     /* leaf pair interactions since creation */
+    uint32_t device_error;   /* device error bits (1 non-finite, 2 tree, 4 bounds) */
+} gr_fa2_info;
+
+/* ABI revision. */
+uint32_t gr_abi_version(void);
+
+/* Last call's status code, its one-line reason, and for GR_PARAM_OUT_OF_RANGE the
+ * index of the refused value. Thread-local; reading them changes nothing. */
+int gr_last_error(void);
+const char *gr_last_error_message(void);
+int gr_last_error_index(void);
+
+/* Registry face (gm_layout_count / gm_layout_id, crates/graph-wasm/src/exports/build.rs:23-60). */
+uint32_t gr_layout_count(void);
+const char *gr_layout_id(uint32_t i);
+
+/* Parameter schema (gm_layout_params; crates/graph-contract/src/params.rs:50-83 ParamSpec). */
+uint32_t gr_fa2_param_count(void);
+int gr_fa2_param_spec(uint32_t i, const char **name, int *kind, double *min, double *max,
+                      double *def, double *step, const char **doc);
+/* ParamsView::validate + values (crates/graph-contract/src/params.rs:147-170): writes
+ * gr_fa2_param_count() values (defaults for the ones a short buffer leaves out). */
+int gr_fa2_params_values(const uint8_t *params, size_t params_len, double *values_out);
+
+/* Fa2State::new (crates/graph-core/src/layout/forceatlas2/state.rs:83-102) over a
+ * topology's raw edges: self-loops dropped, parallel edges merged first-wins
+ * (layout/force/mod.rs:101-120), mass = simple degree + 1. `weight` (nullable) is
+ * the per-raw-edge weight the edge_weight_influence parameter raises; `pos0`
+ * (nullable, n x dim) replaces the Mulberry32(seed) start (state.rs:272-283).
+ * Device memory is allocated here and freed by gr_fa2_destroy. */
+int gr_fa2_create(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                  const double *weight, const uint8_t *params, size_t params_len, const float *pos0);
+void gr_fa2_destroy(gr_fa2 *h);
+
+/* Runs up to `ticks` ticks of Fa2State::iterate (state.rs:130-148), stopping early
+ * once a tick moves the layout by < 1e-10 (state.rs:122-128). *done (nullable)
+ * receives the ticks actually run. gr_fa2_run runs the max_iter parameter. */
+int gr_fa2_tick(gr_fa2 *h, uint32_t ticks, uint32_t *done);
+int gr_fa2_run(gr_fa2 *h, uint32_t *done);
+
+/* Per-tick position buffer: runs up to `ticks` ticks and after each writes the
+ * positions (row-major n x dim, FP32) to dev_out + t * n * dim, a DEVICE pointer. */
+int gr_fa2_tick_record(gr_fa2 *h, uint32_t ticks, float *dev_out, uint32_t *done);
+
+/* Current positions to a host buffer (n x dim), refusing non-finite ones as
+ * `settle` does (crates/graph-core/src/layout/forceatlas2.rs:82-91). */
+int gr_fa2_positions(gr_fa2 *h, float *out);
+/* Replace the positions (host, n x dim). */
+int gr_fa2_set_positions(gr_fa2 *h, const float *pos);
+/* Device view of the node records: float4 {x, y, z, mass} per node, valid until the
+ * next tick or destroy. */
+int gr_fa2_positions_device(gr_fa2 *h, const void **dev_nodes);
+
+/* One force evaluation at the current positions, without moving anything: the
+ * tick's accumulator u = attraction + repulsion - gravity (state.rs:130-137),
+ * n x dim to a host buffer. */
+int gr_fa2_forces(gr_fa2 *h, float *out);
+
+int gr_fa2_get_info(gr_fa2 *h, gr_fa2_info *out);
+
+/* The stream every call of this handle enqueues on (default: the handle's own). */
+int gr_fa2_set_stream(gr_fa2 *h, void *cuda_stream);
+
+/* One-shot registry run, Capability::run_params (crates/graph-core/src/registry/params.rs:156-181):
+ * create, run max_iter, write n x dim positions to a host buffer, destroy. */
+int gr_run(const char *layout_id, uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+           const double *weight, const uint8_t *params, size_t params_len, float *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRAPH_CUDA_H */

@@ -1,0 +1,136 @@
+"""GPU parity: the CUDA engine (through the C ABI) against the FP64 oracle.
+
+Per-tick forces from identical positions must match within 1e-5 relative L2 on
+the same tree (the oracle's insertion tree capped at the engine's Morton depth)
+and the same theta. Integer structure (cell count, interaction counts) must
+match the oracle's exactly or to the few borderline far tests FP32 can flip.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from graph_render_b200 import Fa2, synth
+from tests.gpu_util import collapsed_cells, force_parity, oracle_state, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _check(n, src, dst, w, pos, prm, tol=TOL):
+    rel, info, sc = force_parity(n, src, dst, w, pos, prm)
+    assert info["device_error"] == 0
+    assert rel < tol, rel
+    return rel, info, sc
+
+
+def test_sbm1500_forces_match_oracle():
+    wl = synth.sbm_1500()
+    rel, info, sc = _check(wl.n, wl.src, wl.dst, wl.weight, wl.pos0, wl.params)
+    # the same tree: same cell count, and the same interactions up to FP32 borderline flips
+    st = oracle_state(wl.n, wl.src, wl.dst, wl.weight, wl.pos0, wl.params)
+    st.accumulate(7)
+    assert info["n_cells"] == collapsed_cells(st)
+    far_ref, pair_ref = st.scalars()["far"], st.scalars()["pair"]
+    assert abs(info["far_count"] - far_ref) <= 1e-3 * far_ref + 2
+    assert abs(info["pair_count"] - pair_ref) <= 1e-3 * pair_ref + 2
+
+
+def test_sbm1500_forces_match_after_clustering():
+    wl = synth.sbm_1500()
+    with Fa2(wl.n, wl.src, wl.dst, params=wl.params, pos0=wl.pos0) as eng:
+        eng.tick(60)
+        pos = eng.positions()
+    _check(wl.n, wl.src, wl.dst, None, pos, wl.params)
+
+
+@pytest.mark.parametrize("gate_n", [2, 3, 5, 17, 64, 300, 601])
+def test_gate_model_default_params(gate_n):
+    s, d, _ = O.gate_edges(gate_n)
+    pos = O.initial_positions(gate_n, 0, 2).astype(np.float32)
+    _check(gate_n, s, d, None, pos, dict(theta=0.8))
+
+
+def test_ba_linlog_dissuade_weighted():
+    wl = synth.ba_100k(n=20_000)
+    _check(wl.n, wl.src, wl.dst, wl.weight, wl.pos0, wl.params)
+
+
+def test_powerlaw_3d_strong_gravity():
+    wl = synth.powerlaw_1m(n=50_000, dim=3)
+    _check(wl.n, wl.src, wl.dst, None, wl.pos0, wl.params)
+
+
+def test_theta_zero_is_the_exact_sum():
+    wl = synth.sbm_1500()
+    prm = dict(wl.params, theta=0.0)
+    rel, info, _ = force_parity(wl.n, wl.src, wl.dst, None, wl.pos0, prm, dense_oracle=True)
+    assert rel < TOL
+    assert info["far_count"] == 0 and info["pair_count"] == wl.n * (wl.n - 1)
+
+
+def test_coincident_points_take_the_jiggle():
+    rng = np.random.default_rng(4)
+    n = 3000
+    pos = np.round(rng.uniform(0, 40, (n, 2))).astype(np.float32)  # many exact duplicates
+    s, d = synth.sbm([n], 0.002, 0.0, 9)
+    _check(n, s, d, None, pos, dict(theta=1.2, seed=5))
+
+
+def test_3d_coincident_and_theta0():
+    rng = np.random.default_rng(6)
+    n = 2000
+    pos = np.round(rng.uniform(0, 12, (n, 3))).astype(np.float32)
+    s, d = synth.ba(n, 2, 3)
+    rel, info, _ = force_parity(n, s, d, None, pos, dict(dim=3, theta=0.0), dense_oracle=True)
+    assert rel < TOL
+
+
+def test_large_2d_powerlaw_forces():
+    wl = synth.powerlaw_1m(n=1_000_000, dim=2)
+    rel, info, sc = _check(wl.n, wl.src, wl.dst, None, wl.pos0, wl.params)
+    assert abs(info["far_count"] - sc["far"]) <= 1e-3 * sc["far"]
+
+
+def test_run_is_deterministic():
+    wl = synth.sbm_1500()
+    outs = []
+    for _ in range(2):
+        with Fa2(wl.n, wl.src, wl.dst, params=wl.params, pos0=wl.pos0) as eng:
+            eng.tick(100)
+            outs.append(eng.positions())
+    assert np.array_equal(outs[0], outs[1])
+    assert np.isfinite(outs[0]).all()
+
+
+def test_early_exit_when_nothing_moves():
+    n = 50
+    pos = synth.uniform(n, 2, 0, 10, 1)
+    with Fa2(n, [], [], params=dict(gravity=0.0, scaling_ratio=0.0), pos0=pos) as eng:
+        done = eng.tick(10)
+        assert done == 1
+        assert eng.info()["converged"] == 1
+        assert np.array_equal(eng.positions(), pos)
+
+
+def test_empty_and_single_node():
+    with Fa2(0, [], []) as eng:
+        assert eng.tick(5) == 0
+        assert eng.positions().shape == (0, 2)
+    with Fa2(1, [], []) as eng:
+        eng.tick(100)
+        assert np.isfinite(eng.positions()).all()
+
+
+def test_trajectory_tracks_the_oracle_for_a_few_ticks():
+    """Two ticks (the reference's gated budget): FP32 engine vs FP64 oracle."""
+    wl = synth.sbm_1500()
+    with Fa2(wl.n, wl.src, wl.dst, params=wl.params, pos0=wl.pos0) as eng:
+        eng.tick(2)
+        g = eng.positions().astype(np.float64)
+    st = oracle_state(wl.n, wl.src, wl.dst, None, wl.pos0, wl.params)
+    st.run(2)
+    r = st.positions()
+    ext = (r.max(0) - r.min(0)).max()
+    assert np.abs(g - r).max() / ext < 1e-4
