@@ -1,0 +1,370 @@
+#!/usr/bin/env python3
+"""Benchmark: ForceAtlas2 / Barnes-Hut node-ticks/s on B200.
+
+A step is one FA2 tick over the whole graph (tree build, repulsion walk,
+attraction, gravity, FP64 swing/traction, speed, update). The default workload
+is the 1M-node power-law configuration-model graph laid out in 2D (theta 1.2),
+the north-star size; every rank runs its own replica (weak scaling: the single
+graph has no exchange step to shard).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One JSON line on rank 0. See DESIGN.md for the definitions of the roofline
+numbers and the CPU baseline.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L2_BYTES = 126 * 2 ** 20
+FLUSH_BYTES = 256 * 2 ** 20
+FLOPS_PER_INTERACTION = {2: 10, 3: 13}
+REF_1M_NODE_TICKS = 1_000_000 * 100 / 123.03169  # perf-fa2bh.md:60-63, 1 thread, other host
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="graph_render_b200", choices=["graph_render_b200", "reference"])
+    ap.add_argument("--workload", default="powerlaw-2d",
+                    choices=["powerlaw-2d", "powerlaw-3d", "sbm1500", "ba100k"])
+    ap.add_argument("--n", type=int, default=0, help="override the node count (profiling cases)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-ticks", type=int, default=100)
+    ap.add_argument("--cpu-budget-s", type=float, default=20.0)
+    return ap.parse_args()
+
+
+def workload(name: str, n: int = 0):
+    from graph_render_b200 import synth
+
+    if name == "powerlaw-2d":
+        return synth.powerlaw_1m(n=n or 1_000_000, dim=2)
+    if name == "powerlaw-3d":
+        return synth.powerlaw_1m(n=n or 1_000_000, dim=3)
+    if name == "sbm1500":
+        return synth.sbm_1500()
+    if name == "ba100k":
+        return synth.ba_100k(n=n or 100_000)
+    raise ValueError(name)
+
+
+# ----------------------------------------------------------------- clocks --
+
+class ClockSampler:
+    """nvidia-smi samples of this GPU's clocks and throttle reasons."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_id: str):
+        self.dev = device_id
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.dev, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, pw, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+                pw.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        loaded = [s for s in sm if s > 600] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(pw) if pw else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------ distributed --
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+
+    def init(self, backend: str):
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        if self.world > 1:
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            if self.pg.get_backend() == "nccl":
+                import torch
+
+                self.pg.barrier(device_ids=[self.local])
+            else:
+                self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+
+        dev = "cuda" if self.pg.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def done(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# -------------------------------------------------------------- CPU arms --
+
+def cpu_port_rate(wl, threads: int, budget_s: float, min_ticks: int = 1, max_ticks: int = 1000):
+    """The oracle (FP64 restatement of graph-core's tick) on the host cores:
+    (node-ticks/s, ticks timed, seconds)."""
+    from oracle import oracle as O
+
+    lo, hi, ws = O.simple_graph(wl.n, wl.src, wl.dst, wl.weight)
+    p = wl.params
+    st = O.State(wl.n, lo, hi, w=ws, pos0=wl.pos0.astype(np.float64), dim=p.get("dim", 2),
+                 theta=p.get("theta", 0.8), lin_log=p.get("lin_log", 0),
+                 strong_gravity=p.get("strong_gravity", 0), dissuade_hubs=p.get("dissuade_hubs", 0),
+                 edge_weight_influence=p.get("edge_weight_influence", 0.0), seed=p.get("seed", 0),
+                 threads=threads)
+    t0 = time.perf_counter()
+    ticks = 0
+    while ticks < max_ticks:
+        st.iterate()
+        ticks += 1
+        el = time.perf_counter() - t0
+        if ticks >= min_ticks and el > budget_s * 0.5:
+            break
+    el = time.perf_counter() - t0
+    return wl.n * ticks / el, ticks, el
+
+
+def run_reference(args, dist: Dist):
+    """--impl reference: the reference's algorithm (the oracle port, FP64, OpenMP
+    walk) on this box's host cores, rank 0 only."""
+    if dist.rank != 0:
+        return
+    wl = workload(args.workload, args.n)
+    threads = os.cpu_count() or 1
+    from oracle import oracle as O
+
+    lo, hi, ws = O.simple_graph(wl.n, wl.src, wl.dst, wl.weight)
+    p = wl.params
+    st = O.State(wl.n, lo, hi, w=ws, pos0=wl.pos0.astype(np.float64), dim=p.get("dim", 2),
+                 theta=p.get("theta", 0.8), lin_log=p.get("lin_log", 0),
+                 strong_gravity=p.get("strong_gravity", 0), dissuade_hubs=p.get("dissuade_hubs", 0),
+                 edge_weight_influence=p.get("edge_weight_influence", 0.0), seed=p.get("seed", 0),
+                 threads=threads)
+    budget = 150.0
+    warm = 0
+    t0 = time.perf_counter()
+    while warm < args.warmup and time.perf_counter() - t0 < budget * 0.2:
+        st.iterate()
+        warm += 1
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < args.steps:
+        st.iterate()
+        steps += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    el = time.perf_counter() - t0
+    v = wl.n * steps / el
+    print(json.dumps({
+        "impl": "reference", "metric": "FA2 node-ticks/s at 1M nodes", "value": v, "unit": "node-ticks/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": 1e3 * el / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": v / REF_1M_NODE_TICKS, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": wl.name, "n": wl.n, "m_raw": wl.m, "theta": p.get("theta"), "dim": p.get("dim")},
+        "cpu_baseline": {"value": v, "unit": "node-ticks/s", "cores": threads, "kind": "port",
+                         "sample": f"{steps} full ticks of the {wl.name} workload after {warm} warm-up ticks"},
+        "e2e": {"value": v, "unit": "node-ticks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "graph-core is Rust (no cargo here or on the GPU box); the reference arm is the FP64 C "
+                "restatement of its FA2 tick (oracle/), OpenMP over per-node walks",
+    }), flush=True)
+
+
+# --------------------------------------------------------------- GPU arm --
+
+def run_gpu(args, dist: Dist):
+    import torch
+
+    from graph_render_b200 import Fa2
+
+    dev = dist.local if dist.world > 1 else 0
+    torch.cuda.set_device(dev)
+    wl = workload(args.workload, args.n)
+    dim = int(wl.params.get("dim", 2))
+    eng = Fa2(wl.n, wl.src, wl.dst, wl.weight, params=wl.params, pos0=wl.pos0)
+    eng.tick(max(args.warmup, 3))
+    torch.cuda.synchronize()
+    info0 = eng.info()
+    uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    sampler = ClockSampler(uuid if uuid.startswith("GPU-") else f"GPU-{uuid}")
+    sampler.start()
+    time.sleep(0.3)
+    dist.barrier()
+    torch.cuda.synchronize()
+    ms = eng.tick_timed(args.steps, l2_flush_bytes=FLUSH_BYTES)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = sampler.stop()
+    info1 = eng.info()
+    done = len(ms)
+    total_ms = float(ms[:, 3].sum())
+    max_ms = dist.max(total_ms)
+    value = dist.world * wl.n * done / (max_ms / 1e3)
+    walk_ms = float(ms[:, 1].mean())
+    tree_ms = float(ms[:, 0].mean())
+    fin_ms = float(ms[:, 2].mean())
+    far = (info1["far_count"] - info0["far_count"]) / max(done, 1)
+    pair = (info1["pair_count"] - info0["pair_count"]) / max(done, 1)
+    flops = (far + pair) * FLOPS_PER_INTERACTION[dim]
+    sm_max = clocks.get("sm_max_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_max * 1e6
+    achieved = flops / (walk_ms / 1e3)
+    eng.close()
+
+    # e2e: the public one-shot path from pinned host buffers, create -> ticks -> positions
+    e2e = None
+    if not args.no_e2e:
+        from graph_render_b200 import Fa2 as F
+
+        src = torch.from_numpy(wl.src).pin_memory().numpy()
+        dst = torch.from_numpy(wl.dst).pin_memory().numpy()
+        pos0 = torch.from_numpy(np.ascontiguousarray(wl.pos0)).pin_memory().numpy()
+        w = None if wl.weight is None else torch.from_numpy(wl.weight).pin_memory().numpy()
+        T = args.e2e_ticks
+        prm = dict(wl.params, max_iter=T)
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with F(wl.n, src, dst, w, params=prm, pos0=pos0) as e:
+            ran = e.run()
+            out = e.positions()
+        el = time.perf_counter() - t0
+        el = dist.max(el)
+        h2d = wl.m * 8 + wl.n * dim * 4 + (0 if w is None else wl.m * 8)
+        d2h = wl.n * dim * 4
+        e2e = {"value": dist.world * wl.n * ran / el, "unit": "node-ticks/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "step": f"one layout call: create from host edges + {ran} ticks + positions back",
+               "seconds": el}
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, ticks, el = cpu_port_rate(wl, threads, args.cpu_budget_s)
+        cpu = {"value": v, "unit": "node-ticks/s", "cores": threads, "kind": "port",
+               "sample": f"{ticks} full FP64 ticks of the same {wl.n}-node graph from the same start, "
+                         f"{el:.1f} s (tree build serial, walks OpenMP)"}
+
+    if dist.rank == 0:
+        line = {
+            "metric": "FA2 node-ticks/s at 1M nodes",
+            "value": value,
+            "unit": "node-ticks/s",
+            "n_gpus": dist.world,
+            "steps": done,
+            "warmup": max(args.warmup, 3),
+            "ms_per_step": max_ms / max(done, 1),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": value / REF_1M_NODE_TICKS if wl.n == 1_000_000 else None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": wl.name, "n": wl.n, "m_raw": wl.m, "m_simple": int(info1["m"]),
+                       "dim": dim, "theta": wl.params.get("theta"),
+                       "l2": f"{FLUSH_BYTES >> 20} MiB buffer overwritten before every timed tick "
+                             "(outside the events)",
+                       "parallelism": f"{dist.world} independent replicas" if dist.world > 1 else "1 GPU",
+                       "phase_ms": {"tree": tree_ms, "walk": walk_ms, "finish": fin_ms}},
+            "clocks": clocks,
+            "e2e": e2e,
+            "gpu_launches": int(info1["graph_kernels"]) * done,
+            "roofline": {"kernel": "k_walk", "bound": "fp32", "achieved": achieved / 1e12,
+                         "peak": fp32_peak / 1e12, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                         "traffic": None,
+                         "peak_source": "nominal FP32 FMA rate, 148 SM x 128 lanes x 2 x sm_max_mhz "
+                                        "(MEASURED_PEAKS.json has no non-tensor FP32 figure)",
+                         "interactions_per_tick": {"far": far, "pair": pair},
+                         "flops_per_interaction": FLOPS_PER_INTERACTION[dim]},
+            "cpu_baseline": cpu,
+            "vs_baseline_basis": "reference's own 1M-node FA2-BH run, 1 thread, other host "
+                                 "(perf-fa2bh.md:60-63; theta 0.8, its gate-model graph)",
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    if args.impl == "reference":
+        run_reference(args, dist)  # rank 0 only; no collective involved
+        return
+    dist.init("nccl")
+    try:
+        run_gpu(args, dist)
+    finally:
+        dist.done()
+
+
+if __name__ == "__main__":
+    main()

@@ -46,6 +46,7 @@ class Info(C.Structure):
         ("far_count", C.c_uint64),
         ("pair_count", C.c_uint64),
         ("device_error", C.c_uint32),
+        ("graph_kernels", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -72,6 +73,7 @@ SIGNATURES = {
     "gr_fa2_tick": ([P, C.c_uint32, C.POINTER(C.c_uint32)], C.c_int),
     "gr_fa2_run": ([P, C.POINTER(C.c_uint32)], C.c_int),
     "gr_fa2_tick_record": ([P, C.c_uint32, P, C.POINTER(C.c_uint32)], C.c_int),
+    "gr_fa2_tick_timed": ([P, C.c_uint32, C.c_size_t, P, C.POINTER(C.c_uint32)], C.c_int),
     "gr_fa2_positions": ([P, f32p], C.c_int),
     "gr_fa2_set_positions": ([P, f32p], C.c_int),
     "gr_fa2_positions_device": ([P, C.POINTER(P)], C.c_int),

@@ -118,6 +118,10 @@ struct gr_fa2 {
     // graph
     uint32_t *rp = nullptr, *col = nullptr;
     float *wt = nullptr;
+    uint32_t nseg = 0;                 // heavy-row segments
+    uint32_t *seg_row = nullptr;       // segment -> row
+    uint32_t *seg_first = nullptr;     // row -> its first segment (heavy rows)
+    float *seg_out = nullptr;          // segment sums, D per segment
     float4 *pos = nullptr;
 
     // per-tick buffers
@@ -137,6 +141,13 @@ struct gr_fa2 {
 
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    uint32_t graph_kernels = 0;
+    // the same tick as three graphs (tree, walk, forces+update) for per-phase timing
+    cudaGraph_t pgraph[3] = {nullptr, nullptr, nullptr};
+    cudaGraphExec_t pexec[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    void *flush = nullptr;
+    size_t flush_bytes = 0;
 
     std::vector<void *> allocs;
 
@@ -146,9 +157,23 @@ struct gr_fa2 {
         if (e == cudaSuccess) allocs.push_back((void *)*p);
         return e;
     }
-    ~gr_fa2() {
+    void drop_graphs() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        for (int i = 0; i < 3; i++) {
+            if (pexec[i]) cudaGraphExecDestroy(pexec[i]);
+            if (pgraph[i]) cudaGraphDestroy(pgraph[i]);
+            pexec[i] = nullptr;
+            pgraph[i] = nullptr;
+        }
+    }
+    ~gr_fa2() {
+        drop_graphs();
+        for (int i = 0; i < 4; i++)
+            if (ev[i]) cudaEventDestroy(ev[i]);
+        if (flush) cudaFree(flush);
         for (void *p : allocs) cudaFree(p);
         sorter.release();
         scanner.release();
@@ -198,58 +223,95 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
     return cudaSuccess;
 }
 
+enum Phase { PH_TREE = 1, PH_WALK = 2, PH_FINISH = 4, PH_ALL = 7 };
+
 template <int D>
-static void enqueue_tick(gr_fa2 *h, bool forces_only) {
+static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
     const uint32_t n = h->n;
     cudaStream_t s = h->stream;
     const uint32_t gn = div_up(n, 256);
     DevState *st = h->st;
     const uint32_t *conv = &st->converged;
-    k_bounds<D><<<h->bnd_blocks(), BND_THREADS, 0, s>>>(h->pos, n, st, h->part);
-    k_keys<D><<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals);
-    h->sorter.sort(h->keys, h->vals, n, 64, s, conv);
-    k_gather<<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals, h->sp, h->sorig, h->flag);
-    h->scanner.scan(h->flag, h->excl, n, nullptr, 0, &st->n_unique, nullptr, s, conv);
-    k_leaves<<<gn, 256, 0, s>>>(n, st, h->keys, h->flag, h->excl, h->leaf_start, h->ukey, h->uid);
-    k_karras<<<gn, 256, 0, s>>>(st, h->ukey, h->bt);
-    k_aggregate<D><<<gn, 256, 0, s>>>(st, h->sp, h->leaf_start, h->bt, h->leaf_body, h->int_body, h->leaf_coinc);
-    k_count<D><<<gn, 256, 0, s>>>(st, h->bt, h->cells_at);
-    h->scanner.scan(h->cells_at, h->P, n, &st->n_unique, 0, &st->n_cells, nullptr, s, conv);
-    k_assign<D><<<gn, 256, 0, s>>>(st, h->bt, h->P, h->cells_at, h->leaf_start, h->leaf_body, h->int_body,
-                                   h->leaf_coinc, h->cells, h->leaf_pre, st);
-    WalkParams wp;
-    wp.n = n;
-    wp.kr = (float)h->prm[P_SCALING];
-    wp.theta2 = (float)(h->prm[P_THETA] * h->prm[P_THETA]);
-    wp.seed = (uint32_t)h->prm[P_SEED];
-    k_walk<D><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig, h->uid,
-                                                                h->leaf_pre, h->rep, st);
-    ForceParams fp;
-    fp.n = n;
-    fp.gravity = (float)h->prm[P_GRAVITY];
-    fp.lin_log = (int)h->prm[P_LINLOG];
-    fp.strong_gravity = (int)h->prm[P_STRONG];
-    fp.dissuade_hubs = (int)h->prm[P_DISSUADE];
-    fp.jitter_tolerance = h->prm[P_JT];
-    k_forces<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(fp, st, h->pos, h->rp, h->col, h->wt, h->rep,
-                                                                h->U, h->part, forces_only ? 0 : 1);
-    if (!forces_only) k_update<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(n, st, h->pos, h->U, h->part);
+    if (phases & PH_TREE) {
+        k_bounds<D><<<h->bnd_blocks(), BND_THREADS, 0, s>>>(h->pos, n, st, h->part);
+        k_keys<D><<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals);
+        h->sorter.sort(h->keys, h->vals, n, 64, s, conv);
+        k_gather<<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals, h->sp, h->sorig, h->flag);
+        h->scanner.scan(h->flag, h->excl, n, nullptr, 0, &st->n_unique, nullptr, s, conv);
+        k_leaves<<<gn, 256, 0, s>>>(n, st, h->keys, h->flag, h->excl, h->leaf_start, h->ukey, h->uid);
+        k_karras<<<gn, 256, 0, s>>>(st, h->ukey, h->bt);
+        k_aggregate<D><<<gn, 256, 0, s>>>(st, h->sp, h->leaf_start, h->bt, h->leaf_body, h->int_body,
+                                          h->leaf_coinc);
+        k_count<D><<<gn, 256, 0, s>>>(st, h->bt, h->cells_at);
+        h->scanner.scan(h->cells_at, h->P, n, &st->n_unique, 0, &st->n_cells, nullptr, s, conv);
+        k_assign<D><<<gn, 256, 0, s>>>(st, h->bt, h->sp, h->P, h->cells_at, h->leaf_start, h->leaf_body, h->int_body,
+                                       h->leaf_coinc, h->cells, h->leaf_pre, st);
+    }
+    if (phases & PH_WALK) {
+        WalkParams wp;
+        wp.n = n;
+        wp.kr = (float)h->prm[P_SCALING];
+        wp.theta2 = (float)(h->prm[P_THETA] * h->prm[P_THETA]);
+        wp.seed = (uint32_t)h->prm[P_SEED];
+        k_walk<D><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig, h->uid,
+                                                                    h->leaf_pre, h->rep, st);
+    }
+    if (phases & PH_FINISH) {
+        ForceParams fp;
+        fp.n = n;
+        fp.gravity = (float)h->prm[P_GRAVITY];
+        fp.lin_log = (int)h->prm[P_LINLOG];
+        fp.strong_gravity = (int)h->prm[P_STRONG];
+        fp.dissuade_hubs = (int)h->prm[P_DISSUADE];
+        fp.jitter_tolerance = h->prm[P_JT];
+        if (h->nseg)
+            k_attract_seg<D><<<div_up((uint64_t)h->nseg * GR_WARP, FRC_THREADS), FRC_THREADS, 0, s>>>(
+                h->nseg, fp.lin_log, st, h->pos, h->rp, h->col, h->wt, h->seg_row, h->seg_first, h->seg_out);
+        k_forces<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(fp, st, h->pos, h->rp, h->col, h->wt,
+                                                                    h->seg_first, h->seg_out, h->rep, h->U,
+                                                                    h->part, forces_only ? 0 : 1);
+        if (!forces_only)
+            k_update<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(n, st, h->pos, h->U, h->part);
+    }
 }
 
-static void enqueue(gr_fa2 *h, bool forces_only) {
+static void enqueue(gr_fa2 *h, bool forces_only, int phases = PH_ALL) {
     if (h->dim == 3)
-        enqueue_tick<3>(h, forces_only);
+        enqueue_tick<3>(h, forces_only, phases);
     else
-        enqueue_tick<2>(h, forces_only);
+        enqueue_tick<2>(h, forces_only, phases);
+}
+
+static int capture(gr_fa2 *h, int phases, cudaGraph_t *g, cudaGraphExec_t *x) {
+    CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue(h, false, phases);
+    cudaError_t e = cudaStreamEndCapture(h->stream, g);
+    if (e != cudaSuccess) return set_err(GR_CUDA_ERROR, cudaGetErrorString(e));
+    CU(cudaGraphInstantiate(x, *g, 0));
+    return GR_OK;
 }
 
 static int build_graph(gr_fa2 *h) {
     if (h->exec) return GR_OK;
-    CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue(h, false);
-    cudaError_t e = cudaStreamEndCapture(h->stream, &h->graph);
-    if (e != cudaSuccess) return set_err(GR_CUDA_ERROR, cudaGetErrorString(e));
-    CU(cudaGraphInstantiate(&h->exec, h->graph, 0));
+    if (int c = capture(h, PH_ALL, &h->graph, &h->exec)) return c;
+    size_t nn = 0;
+    CU(cudaGraphGetNodes(h->graph, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    CU(cudaGraphGetNodes(h->graph, nodes.data(), &nn));
+    h->graph_kernels = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        CU(cudaGraphNodeGetType(nd, &t));
+        if (t == cudaGraphNodeTypeKernel) h->graph_kernels++;
+    }
+    return GR_OK;
+}
+
+static int build_phase_graphs(gr_fa2 *h) {
+    if (h->pexec[0]) return GR_OK;
+    const int ph[3] = {PH_TREE, PH_WALK, PH_FINISH};
+    for (int i = 0; i < 3; i++)
+        if (int c = capture(h, ph[i], &h->pgraph[i], &h->pexec[i])) return c;
     return GR_OK;
 }
 
@@ -266,6 +328,31 @@ static int check_device(gr_fa2 *h, const DevState &s) {
         snprintf(b, sizeof b, "device error bits 0x%x", s.error);
         return set_err(GR_DEVICE_FAULT, b);
     }
+    return GR_OK;
+}
+
+// Heavy rows (degree > LIGHT_MAX) split into SEG-entry segments for the
+// warp-per-segment attraction pass.
+static int build_segments(gr_fa2 *h) {
+    const uint32_t n = h->n;
+    if (n == 0 || h->m == 0) return GR_OK;
+    std::vector<uint32_t> rp((size_t)n + 1);
+    CU(cudaMemcpy(rp.data(), h->rp, rp.size() * 4, cudaMemcpyDeviceToHost));
+    std::vector<uint32_t> first(n, 0), srow;
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t d = rp[i + 1] - rp[i];
+        if (d <= LIGHT_MAX) continue;
+        first[i] = (uint32_t)srow.size();
+        for (uint32_t k = 0; k < (d + SEG - 1) / SEG; k++) srow.push_back(i);
+    }
+    h->nseg = (uint32_t)srow.size();
+    if (!h->nseg) return GR_OK;
+    cudaError_t e;
+    if ((e = h->alloc(&h->seg_row, h->nseg)) || (e = h->alloc(&h->seg_first, n)) ||
+        (e = h->alloc(&h->seg_out, (size_t)h->nseg * h->dim)))
+        return set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+    CU(cudaMemcpy(h->seg_row, srow.data(), srow.size() * 4, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(h->seg_first, first.data(), (size_t)n * 4, cudaMemcpyHostToDevice));
     return GR_OK;
 }
 
@@ -420,6 +507,10 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
             rc = set_err(GR_INVALID_ARGUMENT, "edge weights must be finite and > 0 when edge_weight_influence != 0");
             break;
         }
+        if (int c = build_segments(h)) {
+            rc = c;
+            break;
+        }
     } while (0);
     if (rc != GR_OK) {
         delete h;
@@ -513,6 +604,50 @@ int gr_fa2_tick(gr_fa2 *h, uint32_t ticks, uint32_t *done) { return tick_impl(h,
 int gr_fa2_run(gr_fa2 *h, uint32_t *done) {
     if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
     return tick_impl(h, (uint32_t)h->prm[P_MAX_ITER], nullptr, done);
+}
+
+int gr_fa2_tick_timed(gr_fa2 *h, uint32_t ticks, size_t l2_flush_bytes, float *ms_out, uint32_t *done) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    if (!ms_out) return set_err(GR_INVALID_ARGUMENT, "ms_out is null");
+    DevState s0;
+    if (int c = read_state(h, &s0)) return c;
+    if (h->n && ticks) {
+        if (int c = build_phase_graphs(h)) return c;
+        if (int c = build_graph(h)) return c;
+        for (int i = 0; i < 4; i++)
+            if (!h->ev[i]) CU(cudaEventCreate(&h->ev[i]));
+        if (l2_flush_bytes && l2_flush_bytes != h->flush_bytes) {
+            if (h->flush) cudaFree(h->flush);
+            h->flush = nullptr;
+            CU(cudaMalloc(&h->flush, l2_flush_bytes));
+            h->flush_bytes = l2_flush_bytes;
+        }
+        for (uint32_t t = 0; t < ticks; t++) {
+            if (l2_flush_bytes) CU(cudaMemsetAsync(h->flush, (int)(t & 0xff), l2_flush_bytes, h->stream));
+            CU(cudaEventRecord(h->ev[0], h->stream));
+            CU(cudaGraphLaunch(h->pexec[0], h->stream));
+            CU(cudaEventRecord(h->ev[1], h->stream));
+            CU(cudaGraphLaunch(h->pexec[1], h->stream));
+            CU(cudaEventRecord(h->ev[2], h->stream));
+            CU(cudaGraphLaunch(h->pexec[2], h->stream));
+            CU(cudaEventRecord(h->ev[3], h->stream));
+            CU(cudaEventSynchronize(h->ev[3]));
+            float a = 0.f, b = 0.f, c = 0.f, d = 0.f;
+            CU(cudaEventElapsedTime(&a, h->ev[0], h->ev[1]));
+            CU(cudaEventElapsedTime(&b, h->ev[1], h->ev[2]));
+            CU(cudaEventElapsedTime(&c, h->ev[2], h->ev[3]));
+            CU(cudaEventElapsedTime(&d, h->ev[0], h->ev[3]));
+            ms_out[4 * t + 0] = a;
+            ms_out[4 * t + 1] = b;
+            ms_out[4 * t + 2] = c;
+            ms_out[4 * t + 3] = d;
+        }
+    }
+    DevState s1;
+    if (int c = read_state(h, &s1)) return c;
+    if (done) *done = s1.iter_no - s0.iter_no;
+    if (int c = check_device(h, s1)) return c;
+    return ok();
 }
 
 int gr_fa2_tick_record(gr_fa2 *h, uint32_t ticks, float *dev_out, uint32_t *done) {
@@ -610,6 +745,7 @@ int gr_fa2_get_info(gr_fa2 *h, gr_fa2_info *out) {
     out->far_count = s.far_count;
     out->pair_count = s.pair_count;
     out->device_error = s.error;
+    out->graph_kernels = h->graph_kernels;
     return ok();
 }
 
@@ -619,14 +755,7 @@ int gr_fa2_set_stream(gr_fa2 *h, void *cuda_stream) {
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     h->own_stream = false;
     h->stream = (cudaStream_t)cuda_stream;
-    if (h->exec) {
-        cudaGraphExecDestroy(h->exec);
-        h->exec = nullptr;
-    }
-    if (h->graph) {
-        cudaGraphDestroy(h->graph);
-        h->graph = nullptr;
-    }
+    h->drop_graphs();
     return ok();
 }
 

@@ -18,6 +18,57 @@
 namespace gr {
 
 constexpr int FRC_THREADS = 256;
+// Rows longer than LIGHT_MAX are summed in SEG-entry segments, one warp each,
+// so a hub of 30k neighbours costs ~120 warps instead of one thread's 30k steps.
+constexpr uint32_t LIGHT_MAX = 32;
+constexpr uint32_t SEG = 256;
+
+// One edge's pull on node p from neighbour q: w * (q - p), or with linlog
+// w * log(1 + d) / d * (q - p) (networkx layout.py:1806-1813).
+template <int D>
+__device__ __forceinline__ void attr_term(const float4 &p, const float4 &q, float w, int lin_log, float &a0,
+                                          float &a1, float &a2) {
+    const float d0 = q.x - p.x, d1 = q.y - p.y, d2 = (D == 3) ? q.z - p.z : 0.f;
+    float c = w;
+    if (lin_log) {
+        const float dist = sqrtf(d0 * d0 + d1 * d1 + d2 * d2);
+        c *= dist > 0.f ? log1pf(dist) / dist : 0.f;
+    }
+    a0 += d0 * c;
+    a1 += d1 * c;
+    if (D == 3) a2 += d2 * c;
+}
+
+// Heavy rows: warp s sums entries [seg_begin(s), seg_begin(s) + SEG) of row
+// seg_row[s] (lanes stride by 32, then a fixed butterfly), writing D floats.
+template <int D>
+__global__ void __launch_bounds__(FRC_THREADS)
+k_attract_seg(uint32_t nseg, int lin_log, const DevState *st, const float4 *__restrict__ pos,
+              const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col, const float *__restrict__ wt,
+              const uint32_t *__restrict__ seg_row, const uint32_t *__restrict__ seg_first,
+              float *__restrict__ seg_out) {
+    if (st->converged) return;
+    const uint32_t s = (blockIdx.x * FRC_THREADS + threadIdx.x) / GR_WARP;
+    const uint32_t lane = threadIdx.x % GR_WARP;
+    if (s >= nseg) return;
+    const uint32_t row = seg_row[s];
+    const uint32_t e0 = rp[row] + (s - seg_first[row]) * SEG;
+    const uint32_t e1 = min(e0 + SEG, rp[row + 1]);
+    const float4 p = pos[row];
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    for (uint32_t e = e0 + lane; e < e1; e += GR_WARP) attr_term<D>(p, pos[col[e]], wt[e], lin_log, a0, a1, a2);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(GR_FULL, a0, o);
+        a1 += __shfl_xor_sync(GR_FULL, a1, o);
+        if (D == 3) a2 += __shfl_xor_sync(GR_FULL, a2, o);
+    }
+    if (lane == 0) {
+        seg_out[(size_t)s * D] = a0;
+        seg_out[(size_t)s * D + 1] = a1;
+        if (D == 3) seg_out[(size_t)s * D + 2] = a2;
+    }
+}
 
 struct ForceParams {
     uint32_t n;
@@ -56,8 +107,9 @@ __device__ __forceinline__ void estimate_factor(DevState *st, double n, double j
 template <int D>
 __global__ void __launch_bounds__(FRC_THREADS)
 k_forces(ForceParams P, DevState *st, const float4 *__restrict__ pos, const uint32_t *__restrict__ rp,
-         const uint32_t *__restrict__ col, const float *__restrict__ wt, const float *__restrict__ rep,
-         float *__restrict__ U, double *__restrict__ part, int speed_update) {
+         const uint32_t *__restrict__ col, const float *__restrict__ wt, const uint32_t *__restrict__ seg_first,
+         const float *__restrict__ seg_out, const float *__restrict__ rep, float *__restrict__ U,
+         double *__restrict__ part, int speed_update) {
     if (st->converged) return;
     __shared__ double s_red[32];
     __shared__ bool s_last;
@@ -67,17 +119,15 @@ k_forces(ForceParams P, DevState *st, const float4 *__restrict__ pos, const uint
         const float4 p = pos[i];
         float a0 = 0.f, a1 = 0.f, a2 = 0.f;
         const uint32_t e0 = rp[i], e1 = rp[i + 1];
-        for (uint32_t e = e0; e < e1; e++) {
-            const float4 q = pos[col[e]];
-            const float d0 = q.x - p.x, d1 = q.y - p.y, d2 = (D == 3) ? q.z - p.z : 0.f;
-            float c = wt[e];
-            if (P.lin_log) {
-                const float dist = sqrtf(d0 * d0 + d1 * d1 + d2 * d2);
-                c *= dist > 0.f ? log1pf(dist) / dist : 0.f;
+        if (e1 - e0 <= LIGHT_MAX) {
+            for (uint32_t e = e0; e < e1; e++) attr_term<D>(p, pos[col[e]], wt[e], P.lin_log, a0, a1, a2);
+        } else {  // the row's segment sums, in segment order
+            const uint32_t s0 = seg_first[i], ns = (e1 - e0 + SEG - 1) / SEG;
+            for (uint32_t s = s0; s < s0 + ns; s++) {
+                a0 += seg_out[(size_t)s * D];
+                a1 += seg_out[(size_t)s * D + 1];
+                if (D == 3) a2 += seg_out[(size_t)s * D + 2];
             }
-            a0 += d0 * c;
-            a1 += d1 * c;
-            if (D == 3) a2 += d2 * c;
         }
         if (P.dissuade_hubs) {
             a0 /= p.w;

@@ -370,9 +370,14 @@ struct Cells {
 
 template <int D>
 __device__ __forceinline__ void write_cell(Cells c, uint32_t idx, const Body &b, int level, double root_w,
-                                           int32_t skip_or_count, uint32_t start) {
+                                           int32_t skip_or_count, uint32_t start, const float4 *point = nullptr) {
     double inv = 1.0 / b.m;
     double cc[3] = {b.c0 * inv, b.c1 * inv, b.c2 * inv};
+    if (point) {  // a one-point leaf's centre is the point itself, exactly
+        cc[0] = point->x;
+        cc[1] = point->y;
+        cc[2] = point->z;
+    }
     float hi[3], lo[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
@@ -397,7 +402,7 @@ __device__ __forceinline__ void write_cell(Cells c, uint32_t idx, const Body &b,
 // reference chains them); a leaf of distinct points the key could not separate
 // sits at the key's last level.
 template <int D>
-__global__ void k_assign(const DevState *st, BinTree t, const uint32_t *__restrict__ P,
+__global__ void k_assign(const DevState *st, BinTree t, const float4 *__restrict__ sp, const uint32_t *__restrict__ P,
                          const uint32_t *__restrict__ cells_at, const uint32_t *__restrict__ leaf_start,
                          const Body *__restrict__ leaf_body, const Body *__restrict__ int_body,
                          const uint8_t *__restrict__ leaf_coinc, Cells cells,
@@ -413,7 +418,8 @@ __global__ void k_assign(const DevState *st, BinTree t, const uint32_t *__restri
     int level = 0;
     if (par >= 0) level = leaf_coinc[s] ? t.delta[par] / D + 1 : L;
     uint32_t a0 = leaf_start[s], a1 = leaf_start[s + 1];
-    write_cell<D>(cells, idx, leaf_body[s], level, rw, -(int32_t)(a1 - a0), a0);
+    const float4 one = sp[a0];
+    write_cell<D>(cells, idx, leaf_body[s], level, rw, -(int32_t)(a1 - a0), a0, a1 - a0 == 1 ? &one : nullptr);
     leaf_pre[s] = idx;
     for (int depth = 0; par >= 0 && t.first[par] == s && depth <= 66; depth++) {
         if (is_cell<D>(t, par)) {

@@ -83,7 +83,7 @@ k_walk(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 
         const float d2 = (D == 3) ? dx * dx + dy * dy + dz * dz : dx * dx + dy * dy;
         const bool far = active && !holds && d2 > 0.f && w2 < th2 * d2;
         if (far) {
-            const float f = me.w * cm / d2 * kr;
+            const float f = __fdividef(me.w * cm, d2) * kr;
             f0 += dx * f;
             f1 += dy * f;
             if (D == 3) f2 += dz * f;
@@ -91,7 +91,28 @@ k_walk(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 
             nfar++;
         }
         const bool open = active && !far;
-        if (leaf) {
+        if (sk == -1) {
+            // One-point leaf: the exact pair (barnes_hut.rs:163-184) is the body
+            // term above with the point as its own centre; only an exact
+            // coincidence (d2 == 0) takes repel_delta's jiggle.
+            if (open && !holds) {
+                float ex = dx, ey = dy, ez = dz, e2 = d2;
+                if (!(d2 > 0.f)) {
+                    const uint32_t oj = __ldg(&sorig[start]);
+                    const float sg = oi < oj ? 1.f : -1.f;
+                    ex = sg * (float)jiggle(P.seed, iter, 0, oi, oj);
+                    ey = sg * (float)jiggle(P.seed, iter, 1, oi, oj);
+                    if (D == 3) ez = sg * (float)jiggle(P.seed, iter, 2, oi, oj);
+                    e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
+                }
+                const float f = __fdividef(me.w * cm, e2) * kr;
+                f0 += ex * f;
+                f1 += ey * f;
+                if (D == 3) f2 += ez * f;
+                npair++;
+            }
+            k = k + 1;
+        } else if (leaf) {
             if (__any_sync(GR_FULL, open)) {
                 int32_t cnt = -sk;
                 if (start >= n || (uint32_t)cnt > n - start) {
@@ -112,7 +133,7 @@ k_walk(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 
                             if (D == 3) ez = sg * (float)jiggle(P.seed, iter, 2, oi, oj);
                         }
                         const float e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
-                        const float f = me.w * o.w / e2 * kr;
+                        const float f = __fdividef(me.w * o.w, e2) * kr;
                         f0 += ex * f;
                         f1 += ey * f;
                         if (D == 3) f2 += ez * f;

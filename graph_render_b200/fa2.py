@@ -103,6 +103,13 @@ class Fa2:
         N.check(self._L.gr_fa2_tick_record(self.h, int(ticks), C.c_void_p(dev_out_ptr), C.byref(done)))
         return done.value
 
+    def tick_timed(self, ticks: int, l2_flush_bytes: int = 0) -> np.ndarray:
+        """Per-tick device times (ms): columns tree, walk, finish, whole tick."""
+        out = np.zeros((int(ticks), 4), np.float32)
+        done = C.c_uint32()
+        N.check(self._L.gr_fa2_tick_timed(self.h, int(ticks), int(l2_flush_bytes), _ptr(out), C.byref(done)))
+        return out[:done.value]
+
     def positions(self) -> np.ndarray:
         out = np.zeros((self.n, self.dim), np.float32)
         N.check(self._L.gr_fa2_positions(self.h, _ptr(out)))

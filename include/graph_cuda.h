@@ -72,6 +72,7 @@ typedef struct gr_fa2_info {
     uint64_t far_count;      /* far-cell interactions since creation */
     uint64_t pair_count;     /* leaf pair interactions since creation */
     uint32_t device_error;   /* device error bits (1 non-finite, 2 tree, 4 bounds) */
+    uint32_t graph_kernels;  /* kernel launches in one captured tick (0 before the first tick) */
 } gr_fa2_info;
 
 /* ABI revision. */
@@ -114,6 +115,14 @@ int gr_fa2_run(gr_fa2 *h, uint32_t *done);
 /* Per-tick position buffer: runs up to `ticks` ticks and after each writes the
  * positions (row-major n x dim, FP32) to dev_out + t * n * dim, a DEVICE pointer. */
 int gr_fa2_tick_record(gr_fa2 *h, uint32_t ticks, float *dev_out, uint32_t *done);
+
+/* Measurement face: runs up to `ticks` ticks, each as three captured graphs
+ * (tree build, repulsion walk, forces + update) bracketed by CUDA events on the
+ * handle's stream, and writes 4 floats per tick to ms_out: tree, walk, finish and
+ * whole-tick milliseconds. With l2_flush_bytes > 0 a buffer of that size is
+ * overwritten before each tick, outside the events, so every tick starts with a
+ * cold L2. No counterpart in the reference (which has no clock, stage.rs:4-8). */
+int gr_fa2_tick_timed(gr_fa2 *h, uint32_t ticks, size_t l2_flush_bytes, float *ms_out, uint32_t *done);
 
 /* Current positions to a host buffer (n x dim), refusing non-finite ones as
  * `settle` does (crates/graph-core/src/layout/forceatlas2.rs:82-91). */
