@@ -81,6 +81,7 @@ SIGNATURES = {
     "gr_fa2_get_info": ([P, C.POINTER(Info)], C.c_int),
     "gr_fa2_set_stream": ([P, P], C.c_int),
     "gr_run": ([C.c_char_p, C.c_uint32, C.c_uint64, u32p, u32p, f64p, u8p, C.c_size_t, f32p], C.c_int),
+    "gr_fa2_forces_static": ([C.c_uint32, P, P, P, P, u8p, C.c_size_t, C.c_uint32, P, P], C.c_int),
 }
 
 _lib = None

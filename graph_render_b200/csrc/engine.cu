@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -775,6 +776,160 @@ int gr_run(const char *layout_id, uint32_t n, uint64_t m, const uint32_t *src, c
     g_err_index = keep_i;
     memcpy(g_msg, msg, sizeof msg);
     return rc;
+}
+
+}  // extern "C"
+
+// ------------------------------------------- allocation-free force pass ----
+//
+// gr_fa2_forces_static: one force evaluation (the same kernels as
+// gr_fa2_forces) for callers that cannot allocate device memory at all — code
+// running inside another runtime's stream-ordered or pooled allocator, a plugin
+// that is only handed device buffers by its host, or a stream that is being
+// captured into a CUDA graph, where a cudaMalloc would break the capture. Its
+// scratch is the file-scope array below, sized for STATIC_MAX_N nodes; every GPU
+// that loads this library holds that array until the process exits. The caller
+// passes inputs and outputs in device memory; nothing here calls cudaMalloc,
+// cudaFree or any allocating routine.
+
+constexpr uint32_t STATIC_MAX_N = GR_FORCES_STATIC_MAX_N;
+constexpr size_t STATIC_BYTES_PER_NODE = 320;
+constexpr size_t STATIC_BYTES = STATIC_BYTES_PER_NODE * STATIC_MAX_N + (1u << 20);
+
+static __device__ __align__(256) unsigned char g_static_scratch[STATIC_BYTES];
+
+// Host-side device addresses of g_static_scratch, one per device. In host code
+// the symbol itself is only a stand-in, never a device address.
+static std::mutex g_static_mu;
+static unsigned char *g_static_base[256];
+
+static int static_base(unsigned char **out) {
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return set_err(GR_INVALID_ARGUMENT, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_base[dev]) {
+        void *p = nullptr;
+        CU(cudaGetSymbolAddress(&p, g_static_scratch));
+        g_static_base[dev] = (unsigned char *)p;
+    }
+    *out = g_static_base[dev];
+    return GR_OK;
+}
+
+// Bump layout of the per-call buffers inside the static array (256-byte aligned).
+struct Carve {
+    unsigned char *base;
+    size_t off = 0;
+    template <typename T>
+    T *take(size_t count) {
+        off = (off + 255) & ~(size_t)255;
+        T *p = (T *)(base + off);
+        off += (count ? count : 1) * sizeof(T);
+        return p;
+    }
+};
+
+__global__ void k_static_init(DevState *st, uint32_t tick) {
+    DevState z;
+    memset(&z, 0, sizeof z);
+    z.swing = z.traction = z.speed = z.speed_efficiency = 1.0;
+    z.iter_no = tick;
+    *st = z;
+}
+
+template <int D>
+static int forces_static(uint32_t n, const float4 *nodes, const uint32_t *rp, const uint32_t *col,
+                         const float *wt, const double *prm, uint32_t tick, float *out, cudaStream_t s) {
+    unsigned char *base = nullptr;
+    if (int c = static_base(&base)) return c;
+    Carve cv{base};
+    gr_fa2 h;  // a view over static memory: owns nothing, allocates nothing
+    h.dim = D;
+    h.n = n;
+    memcpy(h.prm, prm, sizeof h.prm);
+    h.stream = s;
+    h.own_stream = false;
+    h.st = cv.take<DevState>(1);
+    h.keys = cv.take<uint64_t>(n);
+    h.vals = cv.take<uint32_t>(n);
+    h.ukey = cv.take<uint64_t>(n);
+    h.sorig = cv.take<uint32_t>(n);
+    h.flag = cv.take<uint32_t>(n);
+    h.excl = cv.take<uint32_t>(n);
+    h.uid = cv.take<uint32_t>(n);
+    h.leaf_start = cv.take<uint32_t>((size_t)n + 1);
+    h.cells_at = cv.take<uint32_t>(n);
+    h.P = cv.take<uint32_t>((size_t)n + 1);
+    h.leaf_pre = cv.take<uint32_t>(n);
+    h.sp = cv.take<float4>(n);
+    h.bt.first = cv.take<uint32_t>(n);
+    h.bt.last = cv.take<uint32_t>(n);
+    h.bt.left = cv.take<uint32_t>(n);
+    h.bt.right = cv.take<uint32_t>(n);
+    h.bt.delta = cv.take<int32_t>(n);
+    h.bt.int_parent = cv.take<int32_t>(n);
+    h.bt.leaf_parent = cv.take<int32_t>(n);
+    h.bt.visit = cv.take<uint32_t>(n);
+    h.leaf_body = cv.take<Body>(n);
+    h.int_body = cv.take<Body>(n);
+    h.leaf_coinc = cv.take<uint8_t>(n);
+    h.cells.A = cv.take<float4>(2 * (size_t)n);
+    h.cells.B = cv.take<float4>(2 * (size_t)n);
+    h.cells.C = D == 3 ? cv.take<int2>(2 * (size_t)n) : nullptr;
+    h.rep = cv.take<float>((size_t)n * D);
+    h.part = cv.take<double>(std::max<size_t>((size_t)h.bnd_blocks() * 3 * D, 2 * (size_t)div_up(n, FRC_THREADS)) + 8);
+    h.sorter.cap = n;
+    h.sorter.ntiles = div_up(n, RS_TILE);
+    h.sorter.k_alt = cv.take<uint64_t>(n);
+    h.sorter.v_alt = cv.take<uint32_t>(n);
+    h.sorter.hist = cv.take<uint32_t>((size_t)RS_BINS * h.sorter.ntiles);
+    h.sorter.totals = cv.take<uint32_t>(8 * RS_BINS);
+    h.scanner.cap = n;
+    h.scanner.nb = div_up(n, SC_TILE);
+    h.scanner.bsum = cv.take<uint32_t>(h.scanner.nb);
+    if (cv.off > STATIC_BYTES) return set_err(GR_INVALID_ARGUMENT, "static scratch layout exceeds the array");
+    h.rp = const_cast<uint32_t *>(rp);
+    h.col = const_cast<uint32_t *>(col);
+    h.wt = const_cast<float *>(wt);
+    h.pos = const_cast<float4 *>(nodes);
+    h.U = out;
+    // seg_first stays null: every row takes the row loop.
+    k_static_init<<<1, 1, 0, s>>>(h.st, tick);
+    enqueue_tick<D>(&h, true, PH_ALL);
+    cudaError_t e = cudaGetLastError();
+    // the view must not release what it points at
+    h.rp = nullptr;
+    h.col = nullptr;
+    h.wt = nullptr;
+    h.pos = nullptr;
+    h.U = nullptr;
+    h.sorter = RadixSorter();
+    h.scanner = Scanner();
+    h.allocs.clear();
+    if (e != cudaSuccess) return set_err(GR_CUDA_ERROR, cudaGetErrorString(e));
+    return GR_OK;
+}
+
+extern "C" {
+
+int gr_fa2_forces_static(uint32_t n, const void *nodes, const uint32_t *row_ptr, const uint32_t *col,
+                         const float *weight, const uint8_t *params, size_t params_len, uint32_t tick,
+                         float *out, void *stream) {
+    double prm[16];
+    if (int c = params_values(params, params_len, prm)) return c;
+    if (n > STATIC_MAX_N) {
+        char b[160];
+        snprintf(b, sizeof b, "n = %u is beyond the static scratch's maximum of %u nodes", n, STATIC_MAX_N);
+        return set_err(GR_INVALID_ARGUMENT, b);
+    }
+    if (n == 0) return ok();
+    if (!nodes || !row_ptr || !out || !weight) return set_err(GR_INVALID_ARGUMENT, "a device buffer is null");
+    const cudaStream_t s = (cudaStream_t)stream;
+    int rc = (int)prm[P_DIM] == 3 ? forces_static<3>(n, (const float4 *)nodes, row_ptr, col, weight, prm, tick, out, s)
+                                  : forces_static<2>(n, (const float4 *)nodes, row_ptr, col, weight, prm, tick, out, s);
+    if (rc) return rc;
+    return ok();
 }
 
 }  // extern "C"

@@ -119,7 +119,7 @@ k_forces(ForceParams P, DevState *st, const float4 *__restrict__ pos, const uint
         const float4 p = pos[i];
         float a0 = 0.f, a1 = 0.f, a2 = 0.f;
         const uint32_t e0 = rp[i], e1 = rp[i + 1];
-        if (e1 - e0 <= LIGHT_MAX) {
+        if (seg_first == nullptr || e1 - e0 <= LIGHT_MAX) {
             for (uint32_t e = e0; e < e1; e++) attr_term<D>(p, pos[col[e]], wt[e], P.lin_log, a0, a1, a2);
         } else {  // the row's segment sums, in segment order
             const uint32_t s0 = seg_first[i], ns = (e1 - e0 + SEG - 1) / SEG;

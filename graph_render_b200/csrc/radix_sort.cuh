@@ -162,10 +162,10 @@ struct RadixSorter {
         return cudaSuccess;
     }
     void release() {
-        cudaFree(k_alt);
-        cudaFree(v_alt);
-        cudaFree(hist);
-        cudaFree(totals);
+        if (k_alt) cudaFree(k_alt);
+        if (v_alt) cudaFree(v_alt);
+        if (hist) cudaFree(hist);
+        if (totals) cudaFree(totals);
         k_alt = nullptr;
         v_alt = nullptr;
         hist = nullptr;

@@ -126,7 +126,7 @@ struct Scanner {
         return cudaMalloc(&bsum, (size_t)nb * sizeof(uint32_t));
     }
     void release() {
-        cudaFree(bsum);
+        if (bsum) cudaFree(bsum);
         bsum = nullptr;
     }
     void scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev, uint32_t n_add,

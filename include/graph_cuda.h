@@ -143,6 +143,40 @@ int gr_fa2_get_info(gr_fa2 *h, gr_fa2_info *out);
 /* The stream every call of this handle enqueues on (default: the handle's own). */
 int gr_fa2_set_stream(gr_fa2 *h, void *cuda_stream);
 
+/* Allocation-free force evaluation. No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: code that only receives device
+ * buffers from its host (a plugin inside another GPU runtime or memory pool),
+ * or a stream being captured into a CUDA graph, where an allocation would break
+ * the capture. It computes what gr_fa2_forces computes (u = attraction +
+ * repulsion - gravity at the given positions; the same tree build and walk) but
+ * takes every input and output as device memory and keeps its scratch in a
+ * fixed array compiled into this library, sized for GR_FORCES_STATIC_MAX_N
+ * nodes (about 11.5 MB, held on every GPU that loads the library until the
+ * process exits). It calls no cudaMalloc, cudaFree or other allocating routine.
+ *
+ *   nodes    device, n x float4 {x, y, z (0 in 2D), mass}; FA2's mass is degree + 1
+ *   row_ptr  device, n + 1 CSR offsets over both endpoints of every simple edge
+ *   col      device, neighbour per CSR entry
+ *   weight   device, attraction weight per CSR entry (1.0 for unit weights)
+ *   params   host, the usual parameter buffer (dim, theta, scaling, gravity,
+ *            lin_log, strong_gravity, dissuade_hubs are read)
+ *   tick     the tick number the coincident-pair jiggle is keyed on
+ *   out      device, n x dim forces
+ *   stream   the CUDA stream to enqueue on (NULL = legacy default stream)
+ *
+ * Enqueued asynchronously; only argument refusals are reported (n beyond
+ * GR_FORCES_STATIC_MAX_N is refused with GR_INVALID_ARGUMENT). The first call on
+ * each device looks up the array's device address (cudaGetSymbolAddress, with
+ * that device current): make that first call before any stream capture. Every
+ * call shares the one array, so calls that overlap on the GPU (different streams,
+ * or different host threads on the same device) race and corrupt each other's
+ * results; serialise them on one stream. */
+#define GR_FORCES_STATIC_MAX_N 32768
+int gr_fa2_forces_static(uint32_t n, const void *nodes, const uint32_t *row_ptr, const uint32_t *col,
+                         const float *weight, const uint8_t *params, size_t params_len, uint32_t tick,
+                         float *out, void *stream);
+
 /* One-shot registry run, Capability::run_params (crates/graph-core/src/registry/params.rs:156-181):
  * create, run max_iter, write n x dim positions to a host buffer, destroy. */
 int gr_run(const char *layout_id, uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
