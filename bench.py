@@ -49,6 +49,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-ticks", type=int, default=100)
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-graphs", type=int, default=4096, help="graphs per GPU")
+    ap.add_argument("--batched-ticks", type=int, default=200)
+    ap.add_argument("--batched-sample", type=int, default=48, help="graphs timed one launch sequence each")
     return ap.parse_args()
 
 
@@ -241,6 +245,66 @@ def run_reference(args, dist: Dist):
     }), flush=True)
 
 
+# ---------------------------------------------------------- batched arm --
+
+def run_batched(args, dist: Dist):
+    """The mixed batch (SBM / BA / grid, n log-uniform in [50, 20000]), this rank's
+    shard of graphs_per_gpu x world graphs, 200 ticks each in one persistent
+    launch after autotuning; against the one-graph engine on a uniform sample of
+    the same graphs, each run by itself (device-resident inputs both ways)."""
+    import torch
+
+    from graph_render_b200 import Fa2, batch
+
+    total = args.batched_graphs * dist.world
+    costs = [batch.graph_cost(4, i) for i in range(total)]
+    mine = batch.shard(costs, dist.world)[dist.rank]
+    graphs = [batch.mixed_graph(4, i, ticks=args.batched_ticks) for i in mine]
+    nodes = int(sum(g.n for g in graphs))
+    t0 = time.perf_counter()
+    b = batch.Batch(graphs)
+    create_s = time.perf_counter() - t0
+    chosen, tune_ms = b.tune(2)
+    warm = max(1, min(args.warmup, 3))
+    b.run(warm)  # warm-up ticks, untimed
+    dist.barrier()
+    torch.cuda.synchronize()
+    ms = b.run(args.batched_ticks)
+    torch.cuda.synchronize()
+    dist.barrier()
+    st = b.stats()
+    b.close()
+    ms_max = dist.max(ms)
+    rate = dist.world * len(graphs) / (ms_max / 1e3)
+    # one-by-one: a uniform sample of this rank's graphs through the one-graph engine
+    rng = np.random.default_rng(1234 + dist.rank)
+    pick = sorted(rng.choice(len(graphs), size=min(args.batched_sample, len(graphs)), replace=False).tolist())
+    one_s = 0.0
+    for i in pick:
+        g = graphs[i]
+        with Fa2(g.n, g.src, g.dst, params=g.params, pos0=g.pos0) as e:
+            e.tick(1)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            e.tick(args.batched_ticks)
+            torch.cuda.synchronize()
+            one_s += time.perf_counter() - t1
+    one_rate = len(pick) / one_s if one_s > 0 else None
+    one_rate = dist.max(-one_rate) * -1 if one_rate else None  # the slowest rank
+    return {
+        "metric": "batched graphs/s", "value": rate, "unit": "graphs/s",
+        "graphs": dist.world * len(graphs), "nodes_per_gpu": nodes, "ticks": args.batched_ticks,
+        "ms": ms_max, "cta_threads": chosen, "tune_ms": tune_ms, "create_s": create_s,
+        "one_by_one": {"value": one_rate, "unit": "graphs/s", "sample": len(pick),
+                       "how": "the one-graph engine (captured tick graph, ~45 kernels a tick) per graph, "
+                              "inputs resident, timed over the same 200 ticks"},
+        "speedup_vs_one_by_one": (rate / dist.world) / one_rate if one_rate else None,
+        "converged_graphs": int((st["ticks"] < warm + args.batched_ticks).sum()),
+        "device_errors": int((st["errors"] != 0).sum()),
+        "scaling": "weak (graphs_per_gpu fixed, LPT shard of the global batch)",
+    }
+
+
 # --------------------------------------------------------------- GPU arm --
 
 def run_gpu(args, dist: Dist):
@@ -316,6 +380,10 @@ def run_gpu(args, dist: Dist):
                "sample": f"{ticks} full FP64 ticks of the same {wl.n}-node graph from the same start, "
                          f"{el:.1f} s (tree build serial, walks OpenMP)"}
 
+    batched = None
+    if not args.no_batched:
+        batched = run_batched(args, dist)
+
     if dist.rank == 0:
         line = {
             "metric": "FA2 node-ticks/s at 1M nodes",
@@ -347,6 +415,7 @@ def run_gpu(args, dist: Dist):
                          "interactions_per_tick": {"far": far, "pair": pair},
                          "flops_per_interaction": FLOPS_PER_INTERACTION[dim]},
             "cpu_baseline": cpu,
+            "batched": batched,
             "vs_baseline_basis": "reference's own 1M-node FA2-BH run, 1 thread, other host "
                                  "(perf-fa2bh.md:60-63; theta 0.8, its gate-model graph)",
         }

@@ -11,6 +11,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -26,6 +27,7 @@
 #include "simple_graph.cuh"
 #include "tree.cuh"
 #include "walk.cuh"
+#include "batch.cuh"
 
 using namespace gr;
 
@@ -358,7 +360,8 @@ static int build_segments(gr_fa2 *h) {
 }
 
 static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
-                       const double *weight, const uint8_t *params, size_t params_len, const float *pos0) {
+                       const double *weight, const uint8_t *params, size_t params_len, const float *pos0,
+                       bool tick_buffers = true) {
     if (!out) return set_err(GR_INVALID_ARGUMENT, "out is null");
     *out = nullptr;
     double prm[16];
@@ -466,7 +469,7 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
         if ((e = h->alloc(&h->rp, (size_t)n + 1)) || (e = h->alloc(&h->col, 2 * (size_t)ms)) ||
             (e = h->alloc(&h->wt, 2 * (size_t)ms)) || (e = h->alloc(&h->pos, n)) ||
             (e = h->alloc(&h->st, 1)) || (e = h->alloc(&slo, ms)) || (e = h->alloc(&shi, ms)) ||
-            (e = h->alloc(&weff, ms)) || (e = alloc_tick_buffers(h))) {
+            (e = h->alloc(&weff, ms)) || (tick_buffers && (e = alloc_tick_buffers(h)))) {
             cleanup();
             rc = set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
             break;
@@ -929,6 +932,375 @@ int gr_fa2_forces_static(uint32_t n, const void *nodes, const uint32_t *row_ptr,
     int rc = (int)prm[P_DIM] == 3 ? forces_static<3>(n, (const float4 *)nodes, row_ptr, col, weight, prm, tick, out, s)
                                   : forces_static<2>(n, (const float4 *)nodes, row_ptr, col, weight, prm, tick, out, s);
     if (rc) return rc;
+    return ok();
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ batch --
+//
+// Thousands of independent graphs in one persistent launch (batch.cuh). The
+// concatenated graph (node ids offset per graph) goes through the one-graph
+// create path for its simple-graph pass, CSR and start positions; the batch
+// adds the per-graph table, the per-graph FP64 controller state, the work queue
+// and one scratch slot per resident CTA.
+
+struct gr_fa2_batch {
+    gr_fa2 *g = nullptr;
+    int dim = 2;
+    uint32_t ngraphs = 0, nmax = 0, total_n = 0;
+    std::vector<uint32_t> n_of, off_of;
+    BatchGraph *d_graphs = nullptr;
+    BatchState *d_state = nullptr;
+    uint32_t *d_order = nullptr, *d_next = nullptr, *d_heavy = nullptr;
+    unsigned char *d_slots = nullptr;
+    size_t slot_bytes = 0;
+    uint32_t max_slots = 0;
+    int threads = 512;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t graph_ticks = 0;
+    int graph_threads = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    void drop_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+    ~gr_fa2_batch() {
+        drop_graph();
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        for (void *p : {(void *)d_graphs, (void *)d_state, (void *)d_order, (void *)d_next, (void *)d_heavy,
+                        (void *)d_slots})
+            if (p) cudaFree(p);
+        if (g) {
+            if (g->stream) cudaStreamSynchronize(g->stream);
+            delete g;
+        }
+    }
+};
+
+template <int D, int BT>
+static int batch_slots(uint32_t *slots) {
+    int dev = 0, sms = 0, per = 0;
+    CU(cudaGetDevice(&dev));
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch<D, BT>, BT, 0));
+    *slots = (uint32_t)std::max(1, per) * (uint32_t)sms;
+    return GR_OK;
+}
+
+static int batch_slots_for(int dim, int bt, uint32_t *slots) {
+    if (dim == 3) {
+        if (bt == 256) return batch_slots<3, 256>(slots);
+        if (bt == 1024) return batch_slots<3, 1024>(slots);
+        return batch_slots<3, 512>(slots);
+    }
+    if (bt == 256) return batch_slots<2, 256>(slots);
+    if (bt == 1024) return batch_slots<2, 1024>(slots);
+    return batch_slots<2, 512>(slots);
+}
+
+template <int D, int BT>
+static void batch_launch(gr_fa2_batch *b, uint32_t ticks, uint32_t slots) {
+    BatchArgs a;
+    a.graphs = b->d_graphs;
+    a.state = b->d_state;
+    a.order = b->d_order;
+    a.ngraphs = b->ngraphs;
+    a.next = b->d_next;
+    a.pos = b->g->pos;
+    a.rp = b->g->rp;
+    a.col = b->g->col;
+    a.wt = b->g->wt;
+    a.heavy = b->d_heavy;
+    a.slots = b->d_slots;
+    a.slot_bytes = b->slot_bytes;
+    a.nmax = b->nmax;
+    a.ticks = ticks;
+    cudaMemsetAsync(b->d_next, 0, sizeof(uint32_t), b->g->stream);
+    k_batch<D, BT><<<slots, BT, 0, b->g->stream>>>(a);
+}
+
+static int batch_enqueue(gr_fa2_batch *b, uint32_t ticks) {
+    uint32_t slots = 0;
+    if (int c = batch_slots_for(b->dim, b->threads, &slots)) return c;
+    slots = std::min(slots, b->max_slots);
+    if (b->dim == 3) {
+        if (b->threads == 256) batch_launch<3, 256>(b, ticks, slots);
+        else if (b->threads == 1024) batch_launch<3, 1024>(b, ticks, slots);
+        else batch_launch<3, 512>(b, ticks, slots);
+    } else {
+        if (b->threads == 256) batch_launch<2, 256>(b, ticks, slots);
+        else if (b->threads == 1024) batch_launch<2, 1024>(b, ticks, slots);
+        else batch_launch<2, 512>(b, ticks, slots);
+    }
+    return GR_OK;
+}
+
+static int batch_run_impl(gr_fa2_batch *b, uint32_t ticks, float *ms) {
+    cudaStream_t s = b->g->stream;
+    if (!b->exec || b->graph_ticks != ticks || b->graph_threads != b->threads) {
+        b->drop_graph();
+        CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        int c = batch_enqueue(b, ticks);
+        cudaError_t e = cudaStreamEndCapture(s, &b->graph);
+        if (c) return c;
+        if (e != cudaSuccess) return set_err(GR_CUDA_ERROR, cudaGetErrorString(e));
+        CU(cudaGraphInstantiate(&b->exec, b->graph, 0));
+        b->graph_ticks = ticks;
+        b->graph_threads = b->threads;
+    }
+    if (!b->ev0) CU(cudaEventCreate(&b->ev0));
+    if (!b->ev1) CU(cudaEventCreate(&b->ev1));
+    CU(cudaEventRecord(b->ev0, s));
+    CU(cudaGraphLaunch(b->exec, s));
+    CU(cudaEventRecord(b->ev1, s));
+    CU(cudaEventSynchronize(b->ev1));
+    CU(cudaGetLastError());
+    if (ms) CU(cudaEventElapsedTime(ms, b->ev0, b->ev1));
+    return GR_OK;
+}
+
+extern "C" {
+
+int gr_fa2_batch_create(gr_fa2_batch **out, uint32_t ngraphs, const uint32_t *node_counts,
+                        const uint64_t *edge_counts, const uint32_t *src, const uint32_t *dst, const double *weight,
+                        const double *params, uint32_t params_per_graph, const float *pos0) {
+    if (!out) return set_err(GR_INVALID_ARGUMENT, "out is null");
+    *out = nullptr;
+    if (ngraphs == 0 || !node_counts || !edge_counts) return set_err(GR_INVALID_ARGUMENT, "no graphs");
+    if (params_per_graph != 0 && params_per_graph != kRefParams && params_per_graph != kNParams)
+        return set_err(GR_PARAMS_MALFORMED, "params_per_graph must be 0, 5 or 11");
+    if (params_per_graph && !params) return set_err(GR_INVALID_ARGUMENT, "params is null");
+    std::vector<double> prm((size_t)ngraphs * 16);
+    int dim = -1;
+    for (uint32_t g = 0; g < ngraphs; g++) {
+        std::vector<uint8_t> b((size_t)params_per_graph * 8);
+        if (params_per_graph) memcpy(b.data(), params + (size_t)g * params_per_graph, b.size());
+        if (int c = params_values(b.data(), b.size(), &prm[(size_t)g * 16])) {
+            char m[256];
+            snprintf(m, sizeof m, "graph %u: %.200s", g, g_msg);
+            int idx = g_err_index;
+            return set_err(c, m, idx);
+        }
+        const int d = (int)prm[(size_t)g * 16 + P_DIM];
+        if (dim >= 0 && d != dim) return set_err(GR_INVALID_ARGUMENT, "every graph of a batch has the same dim");
+        dim = d;
+    }
+    uint64_t total_n = 0, total_m = 0;
+    std::vector<uint32_t> off(ngraphs);
+    uint32_t nmax = 1;
+    for (uint32_t g = 0; g < ngraphs; g++) {
+        off[g] = (uint32_t)total_n;
+        total_n += node_counts[g];
+        total_m += edge_counts[g];
+        nmax = std::max(nmax, node_counts[g]);
+    }
+    if (total_n >= 0x7fffffffull || total_m > 0x7fffffffull)
+        return set_err(GR_INVALID_ARGUMENT, "batch larger than 2^31 nodes or edges");
+    if (total_m && (!src || !dst)) return set_err(GR_INVALID_ARGUMENT, "edge arrays are null");
+    // global edge ids, effective weights (w ^ influence of the edge's graph)
+    std::vector<uint32_t> gs(total_m), gd(total_m);
+    std::vector<double> gw;
+    bool any_influence = false;
+    for (uint32_t g = 0; g < ngraphs; g++) any_influence |= prm[(size_t)g * 16 + P_INFLUENCE] != 0.0;
+    if (weight && any_influence) gw.resize(total_m);
+    uint64_t e = 0;
+    for (uint32_t g = 0; g < ngraphs; g++) {
+        const double infl = prm[(size_t)g * 16 + P_INFLUENCE];
+        for (uint64_t k = 0; k < edge_counts[g]; k++, e++) {
+            if (src[e] >= node_counts[g] || dst[e] >= node_counts[g])
+                return set_err(GR_INVALID_ARGUMENT, "an edge names a node outside its graph");
+            gs[e] = src[e] + off[g];
+            gd[e] = dst[e] + off[g];
+            if (!gw.empty()) {
+                const double x = weight[e];
+                if (infl != 0.0 && !(std::isfinite(x) && x > 0.0))
+                    return set_err(GR_INVALID_ARGUMENT, "edge weights must be finite and > 0");
+                gw[e] = infl == 0.0 ? 1.0 : (infl == 1.0 ? x : std::pow(x, infl));
+            }
+        }
+    }
+    // start positions: given, or Mulberry32(seed of the graph) per graph
+    std::vector<float> xyz;
+    const float *p0 = pos0;
+    if (!pos0) {
+        xyz.resize(total_n * dim);
+        for (uint32_t g = 0; g < ngraphs; g++) {
+            uint32_t s = (uint32_t)prm[(size_t)g * 16 + P_SEED];
+            float *o = xyz.data() + (size_t)off[g] * dim;
+            for (size_t i = 0; i < (size_t)node_counts[g] * dim; i++) {
+                s += 0x6D2B79F5u;
+                uint32_t a = s;
+                uint32_t t = (a ^ (a >> 15)) * (1u | a);
+                t = (t + ((t ^ (t >> 7)) * (61u | t))) ^ t;
+                o[i] = (float)((double)(t ^ (t >> 14)) / 4294967296.0);
+            }
+        }
+        p0 = xyz.data();
+    }
+    double base[11];
+    for (uint32_t i = 0; i < kNParams; i++) base[i] = kSpecs[i].def;
+    base[P_DIM] = dim;
+    base[P_INFLUENCE] = gw.empty() ? 0.0 : 1.0;
+    uint8_t bb[11 * 8];
+    memcpy(bb, base, sizeof bb);
+    gr_fa2 *G = nullptr;
+    if (int c = create_impl(&G, (uint32_t)total_n, total_m, gs.data(), gd.data(), gw.empty() ? nullptr : gw.data(),
+                            bb, sizeof bb, p0, false))
+        return c;
+    gr_fa2_batch *b = new (std::nothrow) gr_fa2_batch();
+    if (!b) {
+        gr_fa2_destroy(G);
+        return set_err(GR_ALLOC_FAILED, "host allocation failed");
+    }
+    b->g = G;
+    b->dim = dim;
+    b->ngraphs = ngraphs;
+    b->nmax = nmax;
+    b->total_n = (uint32_t)total_n;
+    b->n_of.assign(node_counts, node_counts + ngraphs);
+    b->off_of = off;
+    // heavy rows and the per-graph table
+    std::vector<uint32_t> rp(total_n + 1);
+    if (cudaMemcpy(rp.data(), G->rp, rp.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        delete b;
+        return set_err(GR_CUDA_ERROR, "reading the CSR offsets failed");
+    }
+    std::vector<uint32_t> heavy;
+    std::vector<BatchGraph> tab(ngraphs);
+    std::vector<BatchState> st(ngraphs);
+    for (uint32_t g = 0; g < ngraphs; g++) {
+        const double *v = &prm[(size_t)g * 16];
+        BatchGraph &t = tab[g];
+        memset(&t, 0, sizeof t);
+        t.off = off[g];
+        t.n = node_counts[g];
+        t.heavy0 = (uint32_t)heavy.size();
+        for (uint32_t i = off[g]; i < off[g] + node_counts[g]; i++)
+            if (rp[i + 1] - rp[i] > LIGHT_MAX) heavy.push_back(i);
+        t.heavy1 = (uint32_t)heavy.size();
+        t.kr = (float)v[P_SCALING];
+        t.th2 = (float)(v[P_THETA] * v[P_THETA]);
+        t.gravity = (float)v[P_GRAVITY];
+        t.seed = (uint32_t)v[P_SEED];
+        t.lin_log = (int)v[P_LINLOG];
+        t.strong_gravity = (int)v[P_STRONG];
+        t.dissuade_hubs = (int)v[P_DISSUADE];
+        t.jitter_tolerance = v[P_JT];
+        memset(&st[g], 0, sizeof st[g]);
+        st[g].swing = st[g].traction = st[g].speed = st[g].speed_efficiency = 1.0;
+    }
+    std::vector<uint32_t> order(ngraphs);
+    for (uint32_t g = 0; g < ngraphs; g++) order[g] = g;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t c) { return node_counts[a] > node_counts[c]; });
+    uint32_t slots = 0;
+    for (int bt : {256, 512, 1024}) {
+        uint32_t sl = 0;
+        if (int c = batch_slots_for(dim, bt, &sl)) {
+            delete b;
+            return c;
+        }
+        slots = std::max(slots, sl);
+    }
+    slots = std::min(slots, ngraphs);
+    SlotView sv;
+    b->slot_bytes = slot_carve(nullptr, nmax, dim, sv);
+    b->max_slots = slots;
+    cudaError_t ce;
+    if ((ce = cudaMalloc(&b->d_graphs, ngraphs * sizeof(BatchGraph))) ||
+        (ce = cudaMalloc(&b->d_state, ngraphs * sizeof(BatchState))) ||
+        (ce = cudaMalloc(&b->d_order, ngraphs * sizeof(uint32_t))) || (ce = cudaMalloc(&b->d_next, 4)) ||
+        (ce = cudaMalloc(&b->d_heavy, std::max<size_t>(heavy.size(), 1) * 4)) ||
+        (ce = cudaMalloc(&b->d_slots, b->slot_bytes * slots))) {
+        delete b;
+        return set_err(GR_ALLOC_FAILED, cudaGetErrorString(ce));
+    }
+    cudaMemcpy(b->d_graphs, tab.data(), ngraphs * sizeof(BatchGraph), cudaMemcpyHostToDevice);
+    cudaMemcpy(b->d_state, st.data(), ngraphs * sizeof(BatchState), cudaMemcpyHostToDevice);
+    cudaMemcpy(b->d_order, order.data(), ngraphs * 4, cudaMemcpyHostToDevice);
+    if (!heavy.empty()) cudaMemcpy(b->d_heavy, heavy.data(), heavy.size() * 4, cudaMemcpyHostToDevice);
+    if ((ce = cudaDeviceSynchronize())) {
+        delete b;
+        return set_err(GR_CUDA_ERROR, cudaGetErrorString(ce));
+    }
+    *out = b;
+    return ok();
+}
+
+void gr_fa2_batch_destroy(gr_fa2_batch *b) { delete b; }
+
+int gr_fa2_batch_set_threads(gr_fa2_batch *b, int threads) {
+    if (!b) return set_err(GR_INVALID_HANDLE, "null batch");
+    if (threads != 256 && threads != 512 && threads != 1024)
+        return set_err(GR_INVALID_ARGUMENT, "threads per CTA must be 256, 512 or 1024");
+    b->threads = threads;
+    return ok();
+}
+
+int gr_fa2_batch_run(gr_fa2_batch *b, uint32_t ticks, float *ms) {
+    if (!b) return set_err(GR_INVALID_HANDLE, "null batch");
+    if (ticks == 0) return ok();
+    if (int c = batch_run_impl(b, ticks, ms)) return c;
+    return ok();
+}
+
+int gr_fa2_batch_tune(gr_fa2_batch *b, uint32_t sample_ticks, int *chosen, float *ms_each) {
+    if (!b) return set_err(GR_INVALID_HANDLE, "null batch");
+    if (sample_ticks == 0) sample_ticks = 1;
+    // time each CTA size on a copy of the state, then put the state back
+    const size_t pb = (size_t)b->total_n * sizeof(float4), sb = (size_t)b->ngraphs * sizeof(BatchState);
+    void *save_p = nullptr, *save_s = nullptr;
+    CU(cudaMalloc(&save_p, std::max<size_t>(pb, 16)));
+    CU(cudaMalloc(&save_s, sb));
+    CU(cudaMemcpy(save_p, b->g->pos, pb, cudaMemcpyDeviceToDevice));
+    CU(cudaMemcpy(save_s, b->d_state, sb, cudaMemcpyDeviceToDevice));
+    const int cands[3] = {256, 512, 1024};
+    float best = 1e30f;
+    int pick = b->threads, rc = GR_OK;
+    for (int i = 0; i < 3 && rc == GR_OK; i++) {
+        b->threads = cands[i];
+        float ms = 0.f;
+        rc = batch_run_impl(b, sample_ticks, &ms);
+        if (ms_each) ms_each[i] = ms;
+        if (rc == GR_OK && ms < best) {
+            best = ms;
+            pick = cands[i];
+        }
+        cudaMemcpy(b->g->pos, save_p, pb, cudaMemcpyDeviceToDevice);
+        cudaMemcpy(b->d_state, save_s, sb, cudaMemcpyDeviceToDevice);
+    }
+    cudaFree(save_p);
+    cudaFree(save_s);
+    b->drop_graph();
+    b->threads = pick;
+    if (chosen) *chosen = pick;
+    if (rc) return rc;
+    CU(cudaDeviceSynchronize());
+    return ok();
+}
+
+int gr_fa2_batch_positions(gr_fa2_batch *b, float *out) {
+    if (!b) return set_err(GR_INVALID_HANDLE, "null batch");
+    return gr_fa2_positions(b->g, out);
+}
+
+int gr_fa2_batch_stats(gr_fa2_batch *b, uint32_t *ticks_done, uint32_t *errors, uint64_t *interactions) {
+    if (!b) return set_err(GR_INVALID_HANDLE, "null batch");
+    std::vector<BatchState> st(b->ngraphs);
+    CU(cudaMemcpy(st.data(), b->d_state, st.size() * sizeof(BatchState), cudaMemcpyDeviceToHost));
+    for (uint32_t g = 0; g < b->ngraphs; g++) {
+        if (ticks_done) ticks_done[g] = st[g].iter_no;
+        if (errors) errors[g] = st[g].error;
+        if (interactions) {
+            interactions[2 * g] = st[g].far_count;
+            interactions[2 * g + 1] = st[g].pair_count;
+        }
+    }
     return ok();
 }
 

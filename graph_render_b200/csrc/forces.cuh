@@ -101,9 +101,88 @@ __device__ __forceinline__ void estimate_factor(DevState *st, double n, double j
     st->speed_efficiency = se;
 }
 
-// u_i = attraction + repulsion - gravity; per-block FP64 swing and traction;
-// the last block accumulates them into the state (cumulative, state.rs:141-143)
-// and runs estimate_factor.
+// Node i's force accumulator given its attraction (a*) and repulsion (r*):
+// u = attraction (/ mass with dissuade hubs) + repulsion - gravity, gravity the
+// unit vector first (state.rs:223-251) or strong (layout.py:1830-1832); writes u
+// and returns the node's FP64 swing and traction terms (schedule.rs:16-30).
+template <int D>
+__device__ __forceinline__ void node_force(const ForceParams &P, const float4 &p, float a0, float a1, float a2,
+                                           float r0, float r1, float r2, const double *mean, float *__restrict__ u,
+                                           double &sw, double &tr) {
+    if (P.dissuade_hubs) {
+        a0 /= p.w;
+        a1 /= p.w;
+        a2 /= p.w;
+    }
+    float u0 = a0 + r0;
+    float u1 = a1 + r1;
+    float u2 = (D == 3) ? a2 + r2 : 0.f;
+    const float c0 = (float)((double)p.x - mean[0]);
+    const float c1 = (float)((double)p.y - mean[1]);
+    const float c2 = (D == 3) ? (float)((double)p.z - mean[2]) : 0.f;
+    const float g = P.gravity * p.w;
+    if (P.strong_gravity) {
+        u0 -= g * c0;
+        u1 -= g * c1;
+        u2 -= g * c2;
+    } else {
+        const float nrm = sqrtf(c0 * c0 + c1 * c1 + c2 * c2);
+        if (nrm > 0.f) {
+            u0 -= g * (c0 / nrm);
+            u1 -= g * (c1 / nrm);
+            u2 -= g * (c2 / nrm);
+        }
+    }
+    u[0] = u0;
+    u[1] = u1;
+    if (D == 3) u[2] = u2;
+    const double m = (double)p.w;
+    const double b0 = (double)p.x - u0, b1 = (double)p.y - u1, b2 = (D == 3) ? (double)p.z - u2 : 0.0;
+    const double g0 = (double)p.x + u0, g1 = (double)p.y + u1, g2 = (D == 3) ? (double)p.z + u2 : 0.0;
+    sw = m * sqrt(b0 * b0 + b1 * b1 + b2 * b2);
+    tr = 0.5 * m * sqrt(g0 * g0 + g1 * g1 + g2 * g2);
+}
+
+// schedule.rs:62-77 apply_update for one node: factor = speed / (1 + sqrt(speed
+// * m * |u|)), p += u * factor; returns |step| summed over the axes (FP64).
+template <int D>
+__device__ __forceinline__ double node_update(float4 &p, const float *__restrict__ u, double speed, bool &bad) {
+    const double u0 = u[0], u1 = u[1], u2 = (D == 3) ? u[2] : 0.0;
+    const double nrm = sqrt(u0 * u0 + u1 * u1 + u2 * u2);
+    const double factor = speed / (1.0 + sqrt(speed * (double)p.w * nrm));
+    const float d0 = (float)(u0 * factor), d1 = (float)(u1 * factor), d2 = (float)(u2 * factor);
+    p.x += d0;
+    p.y += d1;
+    if (D == 3) p.z += d2;
+    bad = !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z));
+    return fabs((double)d0) + fabs((double)d1) + ((D == 3) ? fabs((double)d2) : 0.0);
+}
+
+// Attraction of node i over its own CSR row (rows of <= LIGHT_MAX entries), or
+// its segment sums in segment order (longer rows, when seg_first is given).
+template <int D>
+__device__ __forceinline__ void node_attraction(uint32_t i, const float4 &p, int lin_log,
+                                                const float4 *__restrict__ pos, const uint32_t *__restrict__ rp,
+                                                const uint32_t *__restrict__ col, const float *__restrict__ wt,
+                                                const uint32_t *__restrict__ seg_first,
+                                                const float *__restrict__ seg_out, float &a0, float &a1, float &a2) {
+    a0 = a1 = a2 = 0.f;
+    const uint32_t e0 = rp[i], e1 = rp[i + 1];
+    if (seg_first == nullptr || e1 - e0 <= LIGHT_MAX) {
+        for (uint32_t e = e0; e < e1; e++) attr_term<D>(p, pos[col[e]], wt[e], lin_log, a0, a1, a2);
+    } else {  // the row's segment sums, in segment order
+        const uint32_t s0 = seg_first[i], ns = (e1 - e0 + SEG - 1) / SEG;
+        for (uint32_t s = s0; s < s0 + ns; s++) {
+            a0 += seg_out[(size_t)s * D];
+            a1 += seg_out[(size_t)s * D + 1];
+            if (D == 3) a2 += seg_out[(size_t)s * D + 2];
+        }
+    }
+}
+
+// u_i for every node; per-block FP64 swing and traction; the last block
+// accumulates them into the state (cumulative, state.rs:141-143) and runs
+// estimate_factor.
 template <int D>
 __global__ void __launch_bounds__(FRC_THREADS)
 k_forces(ForceParams P, DevState *st, const float4 *__restrict__ pos, const uint32_t *__restrict__ rp,
@@ -117,50 +196,10 @@ k_forces(ForceParams P, DevState *st, const float4 *__restrict__ pos, const uint
     double sw = 0.0, tr = 0.0;
     if (i < P.n) {
         const float4 p = pos[i];
-        float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-        const uint32_t e0 = rp[i], e1 = rp[i + 1];
-        if (seg_first == nullptr || e1 - e0 <= LIGHT_MAX) {
-            for (uint32_t e = e0; e < e1; e++) attr_term<D>(p, pos[col[e]], wt[e], P.lin_log, a0, a1, a2);
-        } else {  // the row's segment sums, in segment order
-            const uint32_t s0 = seg_first[i], ns = (e1 - e0 + SEG - 1) / SEG;
-            for (uint32_t s = s0; s < s0 + ns; s++) {
-                a0 += seg_out[(size_t)s * D];
-                a1 += seg_out[(size_t)s * D + 1];
-                if (D == 3) a2 += seg_out[(size_t)s * D + 2];
-            }
-        }
-        if (P.dissuade_hubs) {
-            a0 /= p.w;
-            a1 /= p.w;
-            a2 /= p.w;
-        }
-        float u0 = a0 + rep[(size_t)i * D + 0];
-        float u1 = a1 + rep[(size_t)i * D + 1];
-        float u2 = (D == 3) ? a2 + rep[(size_t)i * D + 2] : 0.f;
-        const float c0 = (float)((double)p.x - st->mean[0]);
-        const float c1 = (float)((double)p.y - st->mean[1]);
-        const float c2 = (D == 3) ? (float)((double)p.z - st->mean[2]) : 0.f;
-        const float g = P.gravity * p.w;
-        if (P.strong_gravity) {
-            u0 -= g * c0;
-            u1 -= g * c1;
-            u2 -= g * c2;
-        } else {
-            const float nrm = sqrtf(c0 * c0 + c1 * c1 + c2 * c2);
-            if (nrm > 0.f) {
-                u0 -= g * (c0 / nrm);
-                u1 -= g * (c1 / nrm);
-                u2 -= g * (c2 / nrm);
-            }
-        }
-        U[(size_t)i * D + 0] = u0;
-        U[(size_t)i * D + 1] = u1;
-        if (D == 3) U[(size_t)i * D + 2] = u2;
-        const double m = (double)p.w;
-        const double b0 = (double)p.x - u0, b1 = (double)p.y - u1, b2 = (D == 3) ? (double)p.z - u2 : 0.0;
-        const double g0 = (double)p.x + u0, g1 = (double)p.y + u1, g2 = (D == 3) ? (double)p.z + u2 : 0.0;
-        sw = m * sqrt(b0 * b0 + b1 * b1 + b2 * b2);
-        tr = 0.5 * m * sqrt(g0 * g0 + g1 * g1 + g2 * g2);
+        float a0, a1, a2;
+        node_attraction<D>(i, p, P.lin_log, pos, rp, col, wt, seg_first, seg_out, a0, a1, a2);
+        node_force<D>(P, p, a0, a1, a2, rep[(size_t)i * D + 0], rep[(size_t)i * D + 1],
+                      D == 3 ? rep[(size_t)i * D + 2] : 0.f, st->mean, U + (size_t)i * D, sw, tr);
     }
     if (!speed_update) return;
     sw = block_sum_d<FRC_THREADS>(sw, s_red);
@@ -184,8 +223,7 @@ k_forces(ForceParams P, DevState *st, const float4 *__restrict__ pos, const uint
     }
 }
 
-// schedule.rs:62-77 apply_update: factor = speed / (1 + sqrt(speed * m * |u|)),
-// p += u * factor; FP64 sum of |step| decides the 1e-10 early exit
+// The update for every node; FP64 sum of |step| decides the 1e-10 early exit
 // (state.rs:122-128).
 template <int D>
 __global__ void __launch_bounds__(FRC_THREADS)
@@ -198,17 +236,8 @@ k_update(uint32_t n, DevState *st, float4 *__restrict__ pos, const float *__rest
     double step = 0.0;
     bool bad = false;
     if (i < n) {
-        const double speed = st->speed;
         float4 p = pos[i];
-        const double u0 = U[(size_t)i * D], u1 = U[(size_t)i * D + 1], u2 = (D == 3) ? U[(size_t)i * D + 2] : 0.0;
-        const double nrm = sqrt(u0 * u0 + u1 * u1 + u2 * u2);
-        const double factor = speed / (1.0 + sqrt(speed * (double)p.w * nrm));
-        const float d0 = (float)(u0 * factor), d1 = (float)(u1 * factor), d2 = (float)(u2 * factor);
-        p.x += d0;
-        p.y += d1;
-        if (D == 3) p.z += d2;
-        step = fabs((double)d0) + fabs((double)d1) + ((D == 3) ? fabs((double)d2) : 0.0);
-        bad = !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z));
+        step = node_update<D>(p, U + (size_t)i * D, st->speed, bad);
         pos[i] = p;
     }
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&st->error, (uint32_t)ERR_NONFINITE);

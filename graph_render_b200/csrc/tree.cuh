@@ -50,6 +50,46 @@ __device__ __forceinline__ uint64_t spread3(uint64_t x) {  // 21 bits -> every t
     return x;
 }
 
+// The reference's root square (quadtree.rs:157-195, cover of the minimum then
+// the maximum corner): corner floor(min), side the smallest power of two >= 1
+// that holds the maximum. Returns the side; ok is false if it overflowed.
+template <int D>
+__device__ __forceinline__ double root_square(const double *mn, const double *mx, double *root0, bool &ok) {
+    double z = 1.0;
+    ok = true;
+    for (int a = 0; a < D; a++) root0[a] = floor(mn[a]);
+    for (bool grow = true; grow;) {
+        grow = false;
+        for (int a = 0; a < D; a++)
+            if (mx[a] >= root0[a] + z) grow = true;
+        if (grow) z *= 2.0;
+        if (!isfinite(z)) {
+            ok = false;
+            break;
+        }
+    }
+    return z;
+}
+
+// Left-aligned Morton key of one node in the root square: per axis
+// q = floor((x - x0) * 2^L / side), exact in FP64 because the side is a power of
+// two; bit a of each D-bit group is axis a (the reference's slot order).
+template <int D>
+__device__ __forceinline__ uint64_t morton_key(const float4 &p, const double *root0, double root_w) {
+    constexpr int L = Levels<D>::L;
+    const double scale = ldexp(1.0, L) / root_w;
+    const double qmax = ldexp(1.0, L) - 1.0;
+    const float c[3] = {p.x, p.y, p.z};
+    uint64_t key = 0;
+#pragma unroll
+    for (int a = 0; a < D; a++) {
+        double q = floor(((double)c[a] - root0[a]) * scale);
+        q = fmin(fmax(q, 0.0), qmax);
+        key |= (D == 2 ? spread2((uint64_t)q) : spread3((uint64_t)q)) << a;
+    }
+    return key << (64 - D * L);  // clz of a difference counts levels from the root
+}
+
 // ------------------------------------------------------------------ bounds --
 
 constexpr int BND_THREADS = 256;
@@ -154,19 +194,9 @@ k_bounds(const float4 *__restrict__ pos, uint32_t n, DevState *st, double *__res
                 mx[a] = fmax(mx[a], s_h[a][k]);
             }
         }
-        double z = 1.0;
-        bool grow = true;
-        for (int a = 0; a < D; a++) st->root0[a] = floor(mn[a]);
-        while (grow) {
-            grow = false;
-            for (int a = 0; a < D; a++)
-                if (mx[a] >= st->root0[a] + z) grow = true;
-            if (grow) z *= 2.0;
-            if (!isfinite(z)) {
-                atomicOr(&st->error, (uint32_t)ERR_BOUNDS);
-                break;
-            }
-        }
+        bool ok = true;
+        const double z = root_square<D>(mn, mx, st->root0, ok);
+        if (!ok) atomicOr(&st->error, (uint32_t)ERR_BOUNDS);
         st->root_w = z;
         for (int a = 0; a < D; a++) st->mean[a] = S[a] / (double)n;
         if (st->error) st->converged = 1;
@@ -181,20 +211,7 @@ __global__ void k_keys(const float4 *__restrict__ pos, uint32_t n, const DevStat
     if (st->converged) return;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    constexpr int L = Levels<D>::L;
-    const double scale = ldexp(1.0, L) / st->root_w;
-    const double qmax = ldexp(1.0, L) - 1.0;
-    float4 p = pos[i];
-    float c[3] = {p.x, p.y, p.z};
-    uint64_t key = 0;
-#pragma unroll
-    for (int a = 0; a < D; a++) {
-        double q = floor(((double)c[a] - st->root0[a]) * scale);
-        q = fmin(fmax(q, 0.0), qmax);
-        uint64_t qi = (uint64_t)q;
-        key |= (D == 2 ? spread2(qi) : spread3(qi)) << a;
-    }
-    keys[i] = key << (64 - D * L);  // left-aligned: clz of a difference counts levels from the root
+    keys[i] = morton_key<D>(pos[i], st->root0, st->root_w);
     vals[i] = i;
 }
 
@@ -247,12 +264,8 @@ __device__ __forceinline__ int kdelta(const uint64_t *__restrict__ k, int32_t a,
     return __clzll(k[a] ^ k[b]);
 }
 
-__global__ void k_karras(const DevState *st, const uint64_t *__restrict__ k, BinTree t) {
-    if (st->converged) return;
-    const int32_t nu = (int32_t)st->n_unique;
-    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0 && nu == 1) t.leaf_parent[0] = -1;
-    if (i >= nu - 1) return;
+// Internal node i of the binary radix tree over nu unique keys.
+__device__ __forceinline__ void karras_node(int32_t i, int32_t nu, const uint64_t *__restrict__ k, BinTree t) {
     const int dir = (kdelta(k, i, i + 1, nu) - kdelta(k, i, i - 1, nu)) > 0 ? 1 : -1;
     const int dmin = kdelta(k, i, i - dir, nu);
     int32_t lmax = 2;
@@ -291,18 +304,23 @@ __global__ void k_karras(const DevState *st, const uint64_t *__restrict__ k, Bin
     if (i == 0) t.int_parent[0] = -1;
 }
 
-// Leaf sums (mass, mass-weighted coordinates, FP64) and the bottom-up pass:
-// the second thread to reach a node sums its two children, left then right, so
-// every node's value is independent of arrival order.
-template <int D>
-__global__ void k_aggregate(DevState *st, const float4 *__restrict__ sp,
-                            const uint32_t *__restrict__ leaf_start, BinTree t,
-                            Body *__restrict__ leaf_body, Body *__restrict__ int_body,
-                            uint8_t *__restrict__ leaf_coinc) {
+__global__ void k_karras(const DevState *st, const uint64_t *__restrict__ k, BinTree t) {
     if (st->converged) return;
-    const uint32_t nu = st->n_unique;
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nu) return;
+    const int32_t nu = (int32_t)st->n_unique;
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0 && nu == 1) t.leaf_parent[0] = -1;
+    if (i >= nu - 1) return;
+    karras_node(i, nu, k, t);
+}
+
+// Leaf s's FP64 sums, then the bottom-up pass: the second thread to reach a
+// node sums its two children, left then right, so every node's value is
+// independent of arrival order.
+template <int D>
+__device__ __forceinline__ void aggregate_leaf(uint32_t s, const float4 *__restrict__ sp,
+                                               const uint32_t *__restrict__ leaf_start, BinTree t,
+                                               Body *__restrict__ leaf_body, Body *__restrict__ int_body,
+                                               uint8_t *__restrict__ leaf_coinc, uint32_t *err) {
     const uint32_t a0 = leaf_start[s], a1 = leaf_start[s + 1];
     Body b{0.0, 0.0, 0.0, 0.0};
     const float4 f0 = sp[a0];
@@ -322,7 +340,7 @@ __global__ void k_aggregate(DevState *st, const float4 *__restrict__ sp,
     // a binary radix tree over 64-bit keys is at most 64 levels deep
     for (int depth = 0; node >= 0; depth++) {
         if (depth > 66) {
-            atomicOr(&st->error, (uint32_t)ERR_TREE);
+            atomicOr(err, (uint32_t)ERR_TREE);
             return;
         }
         __threadfence();
@@ -337,26 +355,43 @@ __global__ void k_aggregate(DevState *st, const float4 *__restrict__ sp,
 }
 
 template <int D>
+__global__ void k_aggregate(DevState *st, const float4 *__restrict__ sp,
+                            const uint32_t *__restrict__ leaf_start, BinTree t,
+                            Body *__restrict__ leaf_body, Body *__restrict__ int_body,
+                            uint8_t *__restrict__ leaf_coinc) {
+    if (st->converged) return;
+    const uint32_t nu = st->n_unique;
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nu) return;
+    aggregate_leaf<D>(s, sp, leaf_start, t, leaf_body, int_body, leaf_coinc, &st->error);
+}
+
+template <int D>
 __device__ __forceinline__ bool is_cell(const BinTree &t, int32_t node) {
     int32_t par = t.int_parent[node];
     return par < 0 || (t.delta[node] / D) != (t.delta[par] / D);
 }
 
-// cells_at[s]: how many cells start at unique leaf s (the leaf itself plus the
-// cell ancestors whose range begins there).
+// How many cells start at unique leaf s (the leaf itself plus the cell
+// ancestors whose range begins there).
 template <int D>
-__global__ void k_count(const DevState *st, BinTree t, uint32_t *__restrict__ cells_at) {
-    if (st->converged) return;
-    const uint32_t nu = st->n_unique;
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nu) return;
+__device__ __forceinline__ uint32_t count_leaf(uint32_t s, const BinTree &t) {
     uint32_t c = 1;
     int32_t par = t.leaf_parent[s];
     for (int depth = 0; par >= 0 && t.first[par] == s && depth <= 66; depth++) {
         if (is_cell<D>(t, par)) c++;
         par = t.int_parent[par];
     }
-    cells_at[s] = c;
+    return c;
+}
+
+template <int D>
+__global__ void k_count(const DevState *st, BinTree t, uint32_t *__restrict__ cells_at) {
+    if (st->converged) return;
+    const uint32_t nu = st->n_unique;
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nu) return;
+    cells_at[s] = count_leaf<D>(s, t);
 }
 
 // Cell record, 2D: A = {cx, cy, mass, w^2}, B = {cx_lo, cy_lo, skip | -count, start}.
@@ -402,17 +437,14 @@ __device__ __forceinline__ void write_cell(Cells c, uint32_t idx, const Body &b,
 // reference chains them); a leaf of distinct points the key could not separate
 // sits at the key's last level.
 template <int D>
-__global__ void k_assign(const DevState *st, BinTree t, const float4 *__restrict__ sp, const uint32_t *__restrict__ P,
-                         const uint32_t *__restrict__ cells_at, const uint32_t *__restrict__ leaf_start,
-                         const Body *__restrict__ leaf_body, const Body *__restrict__ int_body,
-                         const uint8_t *__restrict__ leaf_coinc, Cells cells,
-                         uint32_t *__restrict__ leaf_pre, DevState *stw) {
-    if (st->converged) return;
-    const uint32_t nu = st->n_unique;
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nu) return;
+__device__ __forceinline__ void assign_leaf(uint32_t s, uint32_t nu, uint32_t ncells, double rw, const BinTree &t,
+                                            const float4 *__restrict__ sp, const uint32_t *__restrict__ P,
+                                            const uint32_t *__restrict__ cells_at,
+                                            const uint32_t *__restrict__ leaf_start,
+                                            const Body *__restrict__ leaf_body, const Body *__restrict__ int_body,
+                                            const uint8_t *__restrict__ leaf_coinc, Cells cells,
+                                            uint32_t *__restrict__ leaf_pre, uint32_t *err) {
     constexpr int L = Levels<D>::L;
-    const double rw = st->root_w;
     uint32_t idx = P[s] + cells_at[s] - 1;
     int32_t par = t.leaf_parent[s];
     int level = 0;
@@ -425,12 +457,26 @@ __global__ void k_assign(const DevState *st, BinTree t, const float4 *__restrict
         if (is_cell<D>(t, par)) {
             idx--;
             uint32_t end = t.last[par] + 1;
-            uint32_t skip = end == nu ? st->n_cells : P[end];
+            uint32_t skip = end == nu ? ncells : P[end];
             write_cell<D>(cells, idx, int_body[par], t.delta[par] / D, rw, (int32_t)skip, a0);
         }
         par = t.int_parent[par];
     }
-    if (idx != P[s]) atomicOr(&stw->error, (uint32_t)ERR_TREE);
+    if (idx != P[s]) atomicOr(err, (uint32_t)ERR_TREE);
+}
+
+template <int D>
+__global__ void k_assign(const DevState *st, BinTree t, const float4 *__restrict__ sp, const uint32_t *__restrict__ P,
+                         const uint32_t *__restrict__ cells_at, const uint32_t *__restrict__ leaf_start,
+                         const Body *__restrict__ leaf_body, const Body *__restrict__ int_body,
+                         const uint8_t *__restrict__ leaf_coinc, Cells cells,
+                         uint32_t *__restrict__ leaf_pre, DevState *stw) {
+    if (st->converged) return;
+    const uint32_t nu = st->n_unique;
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nu) return;
+    assign_leaf<D>(s, nu, st->n_cells, st->root_w, t, sp, P, cells_at, leaf_start, leaf_body, int_body, leaf_coinc,
+                   cells, leaf_pre, &stw->error);
 }
 
 }  // namespace gr

@@ -30,25 +30,34 @@ struct WalkParams {
     uint32_t seed;
 };
 
+// What one walk reads: the tree of this tick and the sorted nodes.
+struct WalkView {
+    Cells cells;
+    const float4 *sp;
+    const uint32_t *sorig, *uid, *leaf_pre;
+    uint32_t n, ncells, iter, seed;
+    float kr, th2;
+    uint32_t *err;
+};
+
+// The whole warp calls this for the sorted nodes p = base + lane (lanes with
+// p >= n take part in the votes only). Returns each lane's repulsion and its
+// far / pair interaction counts.
 template <int D>
-__global__ void __launch_bounds__(WALK_THREADS)
-k_walk(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 *__restrict__ sp,
-       const uint32_t *__restrict__ sorig, const uint32_t *__restrict__ uid,
-       const uint32_t *__restrict__ leaf_pre, float *__restrict__ rep, DevState *stw) {
-    if (st->converged) return;
-    const uint32_t n = P.n;
-    const uint32_t ncells = st->n_cells;
-    const uint32_t iter = st->iter_no;
-    const uint32_t p = blockIdx.x * WALK_THREADS + threadIdx.x;
+__device__ __forceinline__ void walk_group(const WalkView &V, uint32_t p, float &f0, float &f1, float &f2,
+                                           uint32_t &nfar, uint32_t &npair) {
+    const Cells cells = V.cells;
+    const float4 *__restrict__ sp = V.sp;
+    const uint32_t n = V.n, ncells = V.ncells, iter = V.iter;
     const bool valid = p < n;
-    if (__all_sync(GR_FULL, !valid)) return;
-    float4 me = valid ? sp[p] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const uint32_t mylp = valid ? leaf_pre[uid[p]] : 0xffffffffu;
-    const uint32_t oi = valid ? sorig[p] : 0u;
+    const float4 me = valid ? sp[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t mylp = valid ? V.leaf_pre[V.uid[p]] : 0xffffffffu;
+    const uint32_t oi = valid ? V.sorig[p] : 0u;
     uint32_t resume = valid ? 0u : 0xffffffffu;
-    float f0 = 0.f, f1 = 0.f, f2 = 0.f;
-    uint32_t nfar = 0, npair = 0;
-    const float kr = P.kr, th2 = P.theta2;
+    f0 = f1 = f2 = 0.f;
+    nfar = npair = 0;
+    const float kr = V.kr, th2 = V.th2;
+    const uint32_t lane = threadIdx.x % GR_WARP;
 
     uint32_t k = 0;
     while (k < ncells) {
@@ -72,7 +81,7 @@ k_walk(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 
         const bool leaf = sk < 0;
         uint32_t skip = leaf ? k + 1 : (uint32_t)sk;
         if (skip <= k || skip > ncells) {  // malformed cell: record it, keep the walk finite
-            if ((threadIdx.x % GR_WARP) == 0) atomicOr(&stw->error, (uint32_t)ERR_TREE);
+            if (lane == 0) atomicOr(V.err, (uint32_t)ERR_TREE);
             skip = k + 1;
         }
         const bool active = resume <= k;
@@ -98,11 +107,11 @@ k_walk(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 
             if (open && !holds) {
                 float ex = dx, ey = dy, ez = dz, e2 = d2;
                 if (!(d2 > 0.f)) {
-                    const uint32_t oj = __ldg(&sorig[start]);
+                    const uint32_t oj = __ldg(&V.sorig[start]);
                     const float sg = oi < oj ? 1.f : -1.f;
-                    ex = sg * (float)jiggle(P.seed, iter, 0, oi, oj);
-                    ey = sg * (float)jiggle(P.seed, iter, 1, oi, oj);
-                    if (D == 3) ez = sg * (float)jiggle(P.seed, iter, 2, oi, oj);
+                    ex = sg * (float)jiggle(V.seed, iter, 0, oi, oj);
+                    ey = sg * (float)jiggle(V.seed, iter, 1, oi, oj);
+                    if (D == 3) ez = sg * (float)jiggle(V.seed, iter, 2, oi, oj);
                     e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
                 }
                 const float f = __fdividef(me.w * cm, e2) * kr;
@@ -116,7 +125,7 @@ k_walk(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 
             if (__any_sync(GR_FULL, open)) {
                 int32_t cnt = -sk;
                 if (start >= n || (uint32_t)cnt > n - start) {
-                    if ((threadIdx.x % GR_WARP) == 0) atomicOr(&stw->error, (uint32_t)ERR_TREE);
+                    if (lane == 0) atomicOr(V.err, (uint32_t)ERR_TREE);
                     cnt = 0;
                 }
                 for (int32_t q = 0; q < cnt; q++) {
@@ -126,11 +135,11 @@ k_walk(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 
                         float ex = me.x - o.x, ey = me.y - o.y, ez = (D == 3) ? me.z - o.z : 0.f;
                         if (ex == 0.f && ey == 0.f && (D == 2 || ez == 0.f)) {
                             // repel_delta's jiggle, taken from the lower index
-                            const uint32_t oj = __ldg(&sorig[jp]);
+                            const uint32_t oj = __ldg(&V.sorig[jp]);
                             const float sg = oi < oj ? 1.f : -1.f;
-                            ex = sg * (float)jiggle(P.seed, iter, 0, oi, oj);
-                            ey = sg * (float)jiggle(P.seed, iter, 1, oi, oj);
-                            if (D == 3) ez = sg * (float)jiggle(P.seed, iter, 2, oi, oj);
+                            ex = sg * (float)jiggle(V.seed, iter, 0, oi, oj);
+                            ey = sg * (float)jiggle(V.seed, iter, 1, oi, oj);
+                            if (D == 3) ez = sg * (float)jiggle(V.seed, iter, 2, oi, oj);
                         }
                         const float e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
                         const float f = __fdividef(me.w * o.w, e2) * kr;
@@ -146,7 +155,22 @@ k_walk(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 
             k = __any_sync(GR_FULL, open) ? k + 1 : skip;
         }
     }
-    if (valid) {
+}
+
+template <int D>
+__global__ void __launch_bounds__(WALK_THREADS)
+k_walk(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 *__restrict__ sp,
+       const uint32_t *__restrict__ sorig, const uint32_t *__restrict__ uid,
+       const uint32_t *__restrict__ leaf_pre, float *__restrict__ rep, DevState *stw) {
+    if (st->converged) return;
+    const uint32_t p = blockIdx.x * WALK_THREADS + threadIdx.x;
+    if (__all_sync(GR_FULL, p >= P.n)) return;
+    WalkView V{cells, sp, sorig, uid, leaf_pre, P.n, st->n_cells, st->iter_no, P.seed, P.kr, P.theta2, &stw->error};
+    float f0, f1, f2;
+    uint32_t nfar, npair;
+    walk_group<D>(V, p, f0, f1, f2, nfar, npair);
+    if (p < P.n) {
+        const uint32_t oi = sorig[p];
         rep[(size_t)oi * D + 0] = f0;
         rep[(size_t)oi * D + 1] = f1;
         if (D == 3) rep[(size_t)oi * D + 2] = f2;

@@ -177,6 +177,39 @@ int gr_fa2_forces_static(uint32_t n, const void *nodes, const uint32_t *row_ptr,
                          const float *weight, const uint8_t *params, size_t params_len, uint32_t tick,
                          float *out, void *stream);
 
+/* Batched layouts: many independent graphs in one persistent launch (one CTA per
+ * graph at a time, largest first; every tick of a graph inside its CTA). No
+ * counterpart in the reference, which lays out one graph per call.
+ *
+ *   node_counts[g], edge_counts[g]   sizes of graph g
+ *   src, dst                         concatenated raw edges, node ids local to their graph
+ *   weight                           concatenated raw edge weights (nullable)
+ *   params                           params_per_graph (0, 5 or 11) f64 values per graph,
+ *                                    validated like a parameter buffer; every graph has
+ *                                    the same dim
+ *   pos0                             concatenated n x dim start positions (nullable:
+ *                                    Mulberry32(seed of the graph) per graph) */
+typedef struct gr_fa2_batch gr_fa2_batch;
+int gr_fa2_batch_create(gr_fa2_batch **out, uint32_t graphs, const uint32_t *node_counts,
+                        const uint64_t *edge_counts, const uint32_t *src, const uint32_t *dst,
+                        const double *weight, const double *params, uint32_t params_per_graph,
+                        const float *pos0);
+void gr_fa2_batch_destroy(gr_fa2_batch *b);
+/* CTA size of the persistent kernel: 256, 512 (default) or 1024 threads. */
+int gr_fa2_batch_set_threads(gr_fa2_batch *b, int threads);
+/* Autotuner: times sample_ticks ticks of the whole batch at each CTA size on a copy
+ * of the state (restored afterwards) and keeps the fastest; ms_each (nullable, 3
+ * floats) receives the times for 256, 512, 1024. */
+int gr_fa2_batch_tune(gr_fa2_batch *b, uint32_t sample_ticks, int *chosen, float *ms_each);
+/* Runs every graph up to `ticks` ticks (a converged graph stops) in one persistent
+ * launch, captured once into a CUDA graph; *ms (nullable) receives its device time. */
+int gr_fa2_batch_run(gr_fa2_batch *b, uint32_t ticks, float *ms);
+/* Concatenated positions (sum of n x dim), graph order. */
+int gr_fa2_batch_positions(gr_fa2_batch *b, float *out);
+/* Per graph: ticks done, device error bits, far and pair interaction counts (2 per
+ * graph); any pointer may be NULL. */
+int gr_fa2_batch_stats(gr_fa2_batch *b, uint32_t *ticks_done, uint32_t *errors, uint64_t *interactions);
+
 /* One-shot registry run, Capability::run_params (crates/graph-core/src/registry/params.rs:156-181):
  * create, run max_iter, write n x dim positions to a host buffer, destroy. */
 int gr_run(const char *layout_id, uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,

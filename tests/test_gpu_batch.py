@@ -1,0 +1,106 @@
+"""The batched persistent kernel against the one-graph engine and the oracle.
+
+Every graph of a batch is an independent FA2 run; the persistent kernel runs
+the same per-item functions as the one-graph engine at block scope, so after a
+tick each graph's positions match the one-graph engine's (the FP64 sums fold in
+a different order, hence a tolerance) and the oracle's within the parity bar.
+"""
+
+import numpy as np
+import pytest
+
+from graph_render_b200 import Fa2, batch, synth
+from tests.gpu_util import oracle_state
+
+pytestmark = pytest.mark.gpu
+
+
+def small_mix(count=48, seed=11, nmax=3000):
+    return [batch.mixed_graph(seed, i, nmin=2, nmax=nmax) for i in range(count)]
+
+
+def rel_extent(a, b):
+    ext = max(float((b.max(0) - b.min(0)).max()), 1e-30)
+    return float(np.abs(a - b).max() / ext)
+
+
+@pytest.mark.parametrize("threads", [256, 512, 1024])
+def test_batch_matches_the_one_graph_engine(threads):
+    gs = small_mix()
+    with batch.Batch(gs) as b:
+        b.set_threads(threads)
+        b.run(2)
+        got = b.positions()
+        st = b.stats()
+    assert (st["errors"] == 0).all()
+    assert (st["ticks"] == 2).all()
+    for g, pos in zip(gs, got):
+        with Fa2(g.n, g.src, g.dst, params=g.params, pos0=g.pos0) as eng:
+            eng.tick(2)
+            want = eng.positions()
+        assert rel_extent(pos, want) < 1e-5, (g.kind, g.n)
+
+
+def test_first_tick_interactions_equal_the_one_graph_engine():
+    gs = small_mix(16, seed=3)
+    with batch.Batch(gs) as b:
+        b.run(1)
+        st = b.stats()
+    for i, g in enumerate(gs):
+        with Fa2(g.n, g.src, g.dst, params=g.params, pos0=g.pos0) as eng:
+            eng.tick(1)
+            inf = eng.info()
+        assert (int(st["far"][i]), int(st["pair"][i])) == (inf["far_count"], inf["pair_count"]), g.n
+
+
+def test_batch_tracks_the_oracle():
+    gs = small_mix(12, seed=5, nmax=1500)
+    with batch.Batch(gs) as b:
+        b.run(2)
+        got = b.positions()
+    for g, pos in zip(gs, got):
+        st = oracle_state(g.n, g.src, g.dst, None, g.pos0, g.params)
+        st.run(2)
+        assert rel_extent(pos, st.positions()) < 1e-4, (g.kind, g.n)
+
+
+def test_batch_is_deterministic_and_tuning_restores_the_state():
+    gs = small_mix(32, seed=7)
+    with batch.Batch(gs) as b:
+        chosen, times = b.tune(2)
+        assert chosen in (256, 512, 1024) and all(t > 0 for t in times.values())
+        b.run(5)
+        a = b.positions()
+    with batch.Batch(gs) as b:
+        b.set_threads(chosen)
+        b.run(5)
+        c = b.positions()
+    for x, y in zip(a, c):
+        assert np.array_equal(x, y)
+
+
+def test_converged_graphs_stop_and_others_continue():
+    still = batch.GraphSpec(20, np.zeros(0, np.uint32), np.zeros(0, np.uint32),
+                            dict(gravity=0.0, scaling_ratio=0.0, dim=2), pos0=synth.uniform(20, 2, 0, 5, 1))
+    moving = small_mix(3, seed=9)
+    with batch.Batch([still] + moving) as b:
+        b.run(10)
+        st = b.stats()
+        pos = b.positions()
+    assert st["ticks"][0] == 1
+    assert (st["ticks"][1:] == 10).all()
+    assert np.array_equal(pos[0], still.pos0)
+
+
+def test_batch_3d():
+    gs = []
+    for i in range(10):
+        w = synth.powerlaw_1m(seed=30 + i, n=200 + 300 * i, dim=3)
+        gs.append(batch.GraphSpec(w.n, w.src, w.dst, w.params, None, w.pos0, "powerlaw3d"))
+    with batch.Batch(gs) as b:
+        b.run(2)
+        got = b.positions()
+    for g, pos in zip(gs, got):
+        with Fa2(g.n, g.src, g.dst, params=g.params, pos0=g.pos0) as eng:
+            eng.tick(2)
+            assert rel_extent(pos, eng.positions()) < 1e-5
