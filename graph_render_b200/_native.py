@@ -53,6 +53,11 @@ class Info(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Controller(C.Structure):
+    _fields_ = [("swing", C.c_double), ("traction", C.c_double), ("speed", C.c_double),
+                ("speed_efficiency", C.c_double), ("iter_no", C.c_uint32), ("converged", C.c_uint32)]
+
+
 # Every symbol the header declares, with its ctypes signature.
 P = C.c_void_p
 u8p, u32p, f32p, f64p = C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p
@@ -89,6 +94,10 @@ SIGNATURES = {
     "gr_fa2_batch_tune": ([P, C.c_uint32, C.POINTER(C.c_int), P], C.c_int),
     "gr_fa2_batch_positions": ([P, P], C.c_int),
     "gr_fa2_batch_stats": ([P, P, P, P], C.c_int),
+    "gr_fa2_get_controller": ([P, P], C.c_int),
+    "gr_fa2_set_controller": ([P, P], C.c_int),
+    "gr_fa2_adjoint_forward": ([P, C.c_uint32, C.c_uint32], C.c_int),
+    "gr_fa2_adjoint_backward": ([P, P, P, P], C.c_int),
 }
 
 _lib = None

@@ -28,6 +28,7 @@
 #include "tree.cuh"
 #include "walk.cuh"
 #include "batch.cuh"
+#include "adjoint.cuh"
 
 using namespace gr;
 
@@ -110,6 +111,9 @@ static int params_values(const uint8_t *bytes, size_t len, double *out) {
 
 // ------------------------------------------------------------- engine ------
 
+struct Adjoint;
+static void adjoint_release(Adjoint *a);
+
 struct gr_fa2 {
     int dim = 2;
     uint32_t n = 0;
@@ -121,6 +125,11 @@ struct gr_fa2 {
     // graph
     uint32_t *rp = nullptr, *col = nullptr;
     float *wt = nullptr;
+    uint32_t *csr_simple = nullptr;    // CSR entry -> simple edge
+    uint32_t *simple_raw = nullptr;    // simple edge -> surviving raw edge
+    float *simple_dcdw = nullptr;      // simple edge -> d(coefficient)/d(raw weight)
+    uint64_t m_raw = 0;
+    struct Adjoint *adj = nullptr;     // recorded run for the backward pass
     uint32_t nseg = 0;                 // heavy-row segments
     uint32_t *seg_row = nullptr;       // segment -> row
     uint32_t *seg_first = nullptr;     // row -> its first segment (heavy rows)
@@ -173,6 +182,7 @@ struct gr_fa2 {
         }
     }
     ~gr_fa2() {
+        if (adj) adjoint_release(adj);
         drop_graphs();
         for (int i = 0; i < 4; i++)
             if (ev[i]) cudaEventDestroy(ev[i]);
@@ -466,10 +476,13 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
         h->m = ms;
         uint32_t *slo = nullptr, *shi = nullptr;
         float *weff = nullptr;
+        h->m_raw = m;
         if ((e = h->alloc(&h->rp, (size_t)n + 1)) || (e = h->alloc(&h->col, 2 * (size_t)ms)) ||
             (e = h->alloc(&h->wt, 2 * (size_t)ms)) || (e = h->alloc(&h->pos, n)) ||
             (e = h->alloc(&h->st, 1)) || (e = h->alloc(&slo, ms)) || (e = h->alloc(&shi, ms)) ||
-            (e = h->alloc(&weff, ms)) || (tick_buffers && (e = alloc_tick_buffers(h)))) {
+            (e = h->alloc(&weff, ms)) || (e = h->alloc(&h->simple_raw, ms)) ||
+            (e = h->alloc(&h->simple_dcdw, ms)) || (e = h->alloc(&h->csr_simple, 2 * (size_t)ms)) ||
+            (tick_buffers && (e = alloc_tick_buffers(h)))) {
             cleanup();
             rc = set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
             break;
@@ -477,9 +490,11 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
         cudaMemsetAsync(h->rp, 0, ((size_t)n + 1) * 4, s);
         if (ms) {
             k_edge_emit<<<div_up(m, 256), 256, 0, s>>>((uint32_t)m, ek, ev, eflag, eexcl, d_w, prm[P_INFLUENCE],
-                                                          weff, slo, shi, dk, dv, d_err);
+                                                          weff, slo, shi, dk, dv, d_err, h->simple_raw,
+                                                          h->simple_dcdw);
             esort.sort(dk, dv, 2 * ms, 64, s);
             k_csr<<<div_up(2 * (uint64_t)ms, 256), 256, 0, s>>>(n, 2 * ms, dk, dv, weff, h->rp, h->col, h->wt);
+            cudaMemcpyAsync(h->csr_simple, dv, 2 * (size_t)ms * 4, cudaMemcpyDeviceToDevice, s);
         }
         float *d_xyz = nullptr;
         if ((e = cudaMalloc(&d_xyz, std::max<size_t>(xyz.size(), 1) * 4))) {
@@ -750,6 +765,40 @@ int gr_fa2_get_info(gr_fa2 *h, gr_fa2_info *out) {
     out->pair_count = s.pair_count;
     out->device_error = s.error;
     out->graph_kernels = h->graph_kernels;
+    return ok();
+}
+
+int gr_fa2_get_controller(gr_fa2 *h, gr_fa2_controller *out) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    if (!out) return set_err(GR_INVALID_ARGUMENT, "out is null");
+    DevState s;
+    if (int c = read_state(h, &s)) return c;
+    out->swing = s.swing;
+    out->traction = s.traction;
+    out->speed = s.speed;
+    out->speed_efficiency = s.speed_efficiency;
+    out->iter_no = s.iter_no;
+    out->converged = s.converged;
+    return ok();
+}
+
+int gr_fa2_set_controller(gr_fa2 *h, const gr_fa2_controller *in) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    if (!in) return set_err(GR_INVALID_ARGUMENT, "in is null");
+    if (!(std::isfinite(in->swing) && std::isfinite(in->traction) && std::isfinite(in->speed) &&
+          std::isfinite(in->speed_efficiency)))
+        return set_err(GR_INVALID_ARGUMENT, "non-finite controller state");
+    DevState s;
+    if (int c = read_state(h, &s)) return c;
+    s.swing = in->swing;
+    s.traction = in->traction;
+    s.speed = in->speed;
+    s.speed_efficiency = in->speed_efficiency;
+    s.iter_no = in->iter_no;
+    s.converged = (in->converged || h->n == 0) ? 1u : 0u;
+    s.error = 0;
+    CU(cudaMemcpyAsync(h->st, &s, sizeof s, cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
     return ok();
 }
 
@@ -1301,6 +1350,196 @@ int gr_fa2_batch_stats(gr_fa2_batch *b, uint32_t *ticks_done, uint32_t *errors, 
             interactions[2 * g + 1] = st[g].pair_count;
         }
     }
+    return ok();
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- adjoint --
+//
+// gr_fa2_adjoint_forward records a run (positions and controller every K
+// ticks); gr_fa2_adjoint_backward replays each K-tick segment forward from its
+// checkpoint, keeping every tick's state, then runs the adjoint kernels
+// (adjoint.cuh) tick by tick in reverse. The replay uses the same kernels on the
+// same inputs, so each tick's tree is the one the recorded run built.
+
+struct Adjoint {
+    uint32_t ticks = 0, every = 1, done = 0;
+    float4 *ckpt = nullptr;  // (ticks / every + 1) x n node records
+    DevState *ckst = nullptr;
+    float4 *segp = nullptr;  // every x n
+    DevState *segst = nullptr;
+    float4 *final_pos = nullptr;
+    DevState *final_st = nullptr;
+    float *lam1 = nullptr, *lam = nullptr, *ub = nullptr, *v = nullptr, *lam_rep = nullptr, *lam_com = nullptr;
+    double *lam_pair = nullptr, *xbar = nullptr, *gce = nullptr, *gs = nullptr, *graw = nullptr, *part = nullptr;
+    AdjScalars *A = nullptr;
+    std::vector<void *> allocs;
+    template <typename T>
+    cudaError_t alloc(T **p, size_t count) {
+        cudaError_t e = cudaMalloc((void **)p, (count ? count : 1) * sizeof(T));
+        if (e == cudaSuccess) allocs.push_back((void *)*p);
+        return e;
+    }
+};
+
+static void adjoint_release(Adjoint *a) {
+    for (void *p : a->allocs) cudaFree(p);
+    delete a;
+}
+
+template <int D>
+static void adjoint_tick(gr_fa2 *h, Adjoint *a, const DevState *before) {
+    const uint32_t n = h->n;
+    cudaStream_t s = h->stream;
+    DevState *st = h->st;
+    // forward recompute up to the forces, with the controller update (no move)
+    enqueue_tick<D>(h, false, PH_TREE | PH_WALK);
+    ForceParams fp;
+    fp.n = n;
+    fp.gravity = (float)h->prm[P_GRAVITY];
+    fp.lin_log = (int)h->prm[P_LINLOG];
+    fp.strong_gravity = (int)h->prm[P_STRONG];
+    fp.dissuade_hubs = (int)h->prm[P_DISSUADE];
+    fp.jitter_tolerance = h->prm[P_JT];
+    if (h->nseg)
+        k_attract_seg<D><<<div_up((uint64_t)h->nseg * GR_WARP, FRC_THREADS), FRC_THREADS, 0, s>>>(
+            h->nseg, fp.lin_log, st, h->pos, h->rp, h->col, h->wt, h->seg_row, h->seg_first, h->seg_out);
+    k_forces<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(fp, st, h->pos, h->rp, h->col, h->wt, h->seg_first,
+                                                                h->seg_out, h->rep, h->U, h->part, 1);
+    const uint32_t gb = div_up(n, FRC_THREADS);
+    k_adj_update<D><<<gb, FRC_THREADS, 0, s>>>(n, h->prm[P_JT], st, before, a->A, h->pos, h->U, a->lam1, a->lam, a->ub,
+                                                a->part);
+    k_adj_node<D><<<gb, FRC_THREADS, 0, s>>>(n, (float)h->prm[P_GRAVITY], (int)h->prm[P_STRONG], st, a->A, h->pos,
+                                              h->U, a->lam, a->ub, a->v, a->part);
+    cudaMemsetAsync(a->xbar, 0, 2 * (size_t)n * D * sizeof(double), s);
+    cudaMemsetAsync(a->lam_pair, 0, (size_t)n * D * sizeof(double), s);
+    WalkParams wp;
+    wp.n = n;
+    wp.kr = (float)h->prm[P_SCALING];
+    wp.theta2 = (float)(h->prm[P_THETA] * h->prm[P_THETA]);
+    wp.seed = (uint32_t)h->prm[P_SEED];
+    k_adj_walk<D><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig, h->uid,
+                                                                    h->leaf_pre, a->ub, a->lam_rep, a->xbar,
+                                                                    a->lam_pair);
+    k_adj_down<D><<<div_up(n, 256), 256, 0, s>>>(st, h->bt, h->leaf_start, h->leaf_pre, h->leaf_body, h->int_body,
+                                                  h->sp, h->sorig, a->xbar, a->lam_pair, a->lam_com);
+    k_adj_final<D><<<gb, FRC_THREADS, 0, s>>>(n, fp.lin_log, fp.dissuade_hubs, a->A, h->pos, h->rp, h->col, h->wt,
+                                               a->lam, a->ub, a->v, a->lam_rep, a->lam_com, a->gce, a->lam1);
+}
+
+extern "C" {
+
+int gr_fa2_adjoint_forward(gr_fa2 *h, uint32_t ticks, uint32_t every) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    if (every == 0) return set_err(GR_INVALID_ARGUMENT, "checkpoint interval must be >= 1");
+    if (h->adj) {
+        adjoint_release(h->adj);
+        h->adj = nullptr;
+    }
+    const uint32_t n = h->n;
+    const int D = h->dim;
+    Adjoint *a = new (std::nothrow) Adjoint();
+    if (!a) return set_err(GR_ALLOC_FAILED, "host allocation failed");
+    a->ticks = ticks;
+    a->every = every;
+    const uint32_t nck = ticks / every + 1;
+    const uint64_t ne = 2 * h->m;
+    cudaError_t e;
+    if ((e = a->alloc(&a->ckpt, (size_t)nck * n)) || (e = a->alloc(&a->ckst, nck)) ||
+        (e = a->alloc(&a->segp, (size_t)every * n)) || (e = a->alloc(&a->segst, every)) ||
+        (e = a->alloc(&a->final_pos, n)) || (e = a->alloc(&a->final_st, 1)) ||
+        (e = a->alloc(&a->lam1, (size_t)n * D)) || (e = a->alloc(&a->lam, (size_t)n * D)) ||
+        (e = a->alloc(&a->ub, (size_t)n * D)) || (e = a->alloc(&a->v, (size_t)n * D)) ||
+        (e = a->alloc(&a->lam_rep, (size_t)n * D)) || (e = a->alloc(&a->lam_com, (size_t)n * D)) ||
+        (e = a->alloc(&a->lam_pair, (size_t)n * D)) || (e = a->alloc(&a->xbar, 2 * (size_t)n * D)) ||
+        (e = a->alloc(&a->gce, ne)) || (e = a->alloc(&a->gs, h->m)) || (e = a->alloc(&a->graw, h->m_raw)) ||
+        (e = a->alloc(&a->part, 3 * (size_t)div_up(n, FRC_THREADS) + 8)) || (e = a->alloc(&a->A, 1))) {
+        adjoint_release(a);
+        return set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+    }
+    if (!h->bt.cell_of) {
+        if ((e = h->alloc(&h->bt.cell_of, n))) {
+            adjoint_release(a);
+            return set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+        }
+        h->drop_graphs();  // the captured tick now also records each cell's node
+    }
+    h->adj = a;
+    DevState s0;
+    if (int c = read_state(h, &s0)) return c;
+    if (n && ticks) {
+        if (int c = build_graph(h)) return c;
+        for (uint32_t t = 0; t < ticks; t++) {
+            if (t % every == 0) {
+                CU(cudaMemcpyAsync(a->ckpt + (size_t)(t / every) * n, h->pos, (size_t)n * sizeof(float4),
+                                   cudaMemcpyDeviceToDevice, h->stream));
+                CU(cudaMemcpyAsync(a->ckst + t / every, h->st, sizeof(DevState), cudaMemcpyDeviceToDevice, h->stream));
+            }
+            CU(cudaGraphLaunch(h->exec, h->stream));
+        }
+    }
+    CU(cudaMemcpyAsync(a->final_pos, h->pos, (size_t)std::max(n, 1u) * sizeof(float4), cudaMemcpyDeviceToDevice,
+                       h->stream));
+    CU(cudaMemcpyAsync(a->final_st, h->st, sizeof(DevState), cudaMemcpyDeviceToDevice, h->stream));
+    DevState s1;
+    if (int c = read_state(h, &s1)) return c;
+    a->done = s1.iter_no - s0.iter_no;
+    if (int c = check_device(h, s1)) return c;
+    return ok();
+}
+
+int gr_fa2_adjoint_backward(gr_fa2 *h, const float *dL_dpT, float *dL_dp0, double *dL_dw) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    Adjoint *a = h->adj;
+    if (!a) return set_err(GR_INVALID_ARGUMENT, "no recorded run: call gr_fa2_adjoint_forward first");
+    if (!dL_dpT || !dL_dp0) return set_err(GR_INVALID_ARGUMENT, "gradient buffers are null");
+    const uint32_t n = h->n;
+    const int D = h->dim;
+    cudaStream_t s = h->stream;
+    CU(cudaMemcpyAsync(a->lam1, dL_dpT, (size_t)n * D * 4, cudaMemcpyHostToDevice, s));
+    CU(cudaMemsetAsync(a->A, 0, sizeof(AdjScalars), s));
+    CU(cudaMemsetAsync(a->gce, 0, std::max<uint64_t>(2 * h->m, 1) * sizeof(double), s));
+    if (n && a->done) {
+        const uint32_t nseg = (a->done + a->every - 1) / a->every;
+        for (uint32_t g = nseg; g-- > 0;) {
+            const uint32_t t0 = g * a->every, t1 = std::min(t0 + a->every, a->done);
+            CU(cudaMemcpyAsync(h->pos, a->ckpt + (size_t)g * n, (size_t)n * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+            CU(cudaMemcpyAsync(h->st, a->ckst + g, sizeof(DevState), cudaMemcpyDeviceToDevice, s));
+            for (uint32_t t = t0; t < t1; t++) {  // replay, keeping each tick's state
+                CU(cudaMemcpyAsync(a->segp + (size_t)(t - t0) * n, h->pos, (size_t)n * sizeof(float4),
+                                   cudaMemcpyDeviceToDevice, s));
+                CU(cudaMemcpyAsync(a->segst + (t - t0), h->st, sizeof(DevState), cudaMemcpyDeviceToDevice, s));
+                enqueue(h, false);
+            }
+            for (uint32_t t = t1; t-- > t0;) {
+                CU(cudaMemcpyAsync(h->pos, a->segp + (size_t)(t - t0) * n, (size_t)n * sizeof(float4),
+                                   cudaMemcpyDeviceToDevice, s));
+                CU(cudaMemcpyAsync(h->st, a->segst + (t - t0), sizeof(DevState), cudaMemcpyDeviceToDevice, s));
+                if (D == 3)
+                    adjoint_tick<3>(h, a, a->segst + (t - t0));
+                else
+                    adjoint_tick<2>(h, a, a->segst + (t - t0));
+            }
+        }
+    }
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(dL_dp0, a->lam1, (size_t)n * D * 4, cudaMemcpyDeviceToHost, s));
+    if (dL_dw && h->m_raw) {
+        CU(cudaMemsetAsync(a->gs, 0, std::max<uint64_t>(h->m, 1) * sizeof(double), s));
+        CU(cudaMemsetAsync(a->graw, 0, h->m_raw * sizeof(double), s));
+        if (h->m) {
+            k_adj_edges<<<div_up(2 * h->m, 256), 256, 0, s>>>((uint32_t)(2 * h->m), h->csr_simple, a->gce, a->gs);
+            k_adj_raw<<<div_up(h->m, 256), 256, 0, s>>>((uint32_t)h->m, a->gs, h->simple_raw, h->simple_dcdw, a->graw);
+        }
+        CU(cudaMemcpyAsync(dL_dw, a->graw, h->m_raw * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    // the handle goes back to the end of the recorded run
+    CU(cudaMemcpyAsync(h->pos, a->final_pos, (size_t)std::max(n, 1u) * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+    CU(cudaMemcpyAsync(h->st, a->final_st, sizeof(DevState), cudaMemcpyDeviceToDevice, s));
+    CU(cudaStreamSynchronize(s));
+    for (size_t i = 0; i < (size_t)n * D; i++)
+        if (!std::isfinite(dL_dp0[i])) return set_err(GR_LAYOUT_FAILED, "non-finite gradient");
     return ok();
 }
 

@@ -39,19 +39,23 @@ __global__ void k_edge_emit(uint32_t m, const uint64_t *__restrict__ keys, const
                             const uint32_t *__restrict__ flag, const uint32_t *__restrict__ excl,
                             const double *__restrict__ w, double influence, float *__restrict__ weff,
                             uint32_t *__restrict__ slo, uint32_t *__restrict__ shi,
-                            uint64_t *__restrict__ dkeys, uint32_t *__restrict__ dvals, uint32_t *err) {
+                            uint64_t *__restrict__ dkeys, uint32_t *__restrict__ dvals, uint32_t *err,
+                            uint32_t *__restrict__ sraw, float *__restrict__ dcdw) {
     uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= m || !flag[q]) return;
     uint32_t s = excl[q];
     uint64_t k = keys[q];
     uint32_t lo = (uint32_t)(k >> 32), hi = (uint32_t)k;
-    double c = 1.0;
+    double c = 1.0, dc = 0.0;
     if (w && influence != 0.0) {
         double x = w[vals[q]];
         if (!(isfinite(x) && x > 0.0)) atomicOr(err, 2u);
         c = influence == 1.0 ? x : pow(x, influence);
+        dc = influence == 1.0 ? 1.0 : influence * c / x;  // d(w^influence)/dw
     }
     weff[s] = (float)c;
+    sraw[s] = vals[q];  // the raw edge that survived (first of its pair)
+    dcdw[s] = (float)dc;
     slo[s] = lo;
     shi[s] = hi;
     dkeys[2 * (uint64_t)s] = ((uint64_t)lo << 32) | hi;

@@ -257,6 +257,7 @@ struct BinTree {
     int32_t *int_parent;  // internal node -> parent (-1 at the root)
     int32_t *leaf_parent; // leaf -> parent (-1 when the tree is one leaf)
     uint32_t *visit;      // bottom-up arrival tickets
+    uint32_t *cell_of;    // internal node -> its cell's preorder index, when it is a cell (nullable)
 };
 
 __device__ __forceinline__ int kdelta(const uint64_t *__restrict__ k, int32_t a, int32_t b, int32_t nu) {
@@ -459,6 +460,7 @@ __device__ __forceinline__ void assign_leaf(uint32_t s, uint32_t nu, uint32_t nc
             uint32_t end = t.last[par] + 1;
             uint32_t skip = end == nu ? ncells : P[end];
             write_cell<D>(cells, idx, int_body[par], t.delta[par] / D, rw, (int32_t)skip, a0);
+            if (t.cell_of) t.cell_of[par] = idx;
         }
         par = t.int_parent[par];
     }

@@ -66,6 +66,7 @@ class Fa2:
         if pos0 is not None:
             p0 = np.ascontiguousarray(pos0, np.float32).reshape(self.n, self.dim)
         h = C.c_void_p()
+        self.m_raw = int(len(src))
         N.check(L.gr_fa2_create(C.byref(h), self.n, len(src), _ptr(src), _ptr(dst), _ptr(w),
                                 C.c_char_p(pb) if pb else None, len(pb), _ptr(p0)))
         self.h = h
@@ -110,6 +111,20 @@ class Fa2:
         N.check(self._L.gr_fa2_tick_timed(self.h, int(ticks), int(l2_flush_bytes), _ptr(out), C.byref(done)))
         return out[:done.value]
 
+    def adjoint_forward(self, ticks: int, every: int = 20) -> None:
+        """Runs `ticks` ticks recording positions and controller every `every`
+        ticks, for adjoint_backward."""
+        N.check(self._L.gr_fa2_adjoint_forward(self.h, int(ticks), int(every)))
+
+    def adjoint_backward(self, dL_dpT) -> tuple:
+        """(dL/d start positions (n x dim), dL/d raw edge weight (m)) for
+        dL_dpT = dL/d final positions of the recorded run."""
+        g = np.ascontiguousarray(dL_dpT, np.float32).reshape(self.n, self.dim)
+        dp0 = np.zeros((self.n, self.dim), np.float32)
+        dw = np.zeros(max(self.m_raw, 1), np.float64)
+        N.check(self._L.gr_fa2_adjoint_backward(self.h, _ptr(g), _ptr(dp0), _ptr(dw)))
+        return dp0, dw[:self.m_raw]
+
     def positions(self) -> np.ndarray:
         out = np.zeros((self.n, self.dim), np.float32)
         N.check(self._L.gr_fa2_positions(self.h, _ptr(out)))
@@ -133,6 +148,15 @@ class Fa2:
         inf = N.Info()
         N.check(self._L.gr_fa2_get_info(self.h, C.byref(inf)))
         return inf.as_dict()
+
+    def controller(self) -> dict:
+        c = N.Controller()
+        N.check(self._L.gr_fa2_get_controller(self.h, C.byref(c)))
+        return {k: getattr(c, k) for k, _ in c._fields_}
+
+    def set_controller(self, swing, traction, speed, speed_efficiency, iter_no, converged=0) -> None:
+        c = N.Controller(swing, traction, speed, speed_efficiency, iter_no, converged)
+        N.check(self._L.gr_fa2_set_controller(self.h, C.byref(c)))
 
     def set_stream(self, stream_ptr: int) -> None:
         N.check(self._L.gr_fa2_set_stream(self.h, C.c_void_p(stream_ptr)))

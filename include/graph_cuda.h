@@ -140,6 +140,28 @@ int gr_fa2_forces(gr_fa2 *h, float *out);
 
 int gr_fa2_get_info(gr_fa2 *h, gr_fa2_info *out);
 
+/* Checkpoint / resume: the FP64 speed controller (state.rs:151-171's swing,
+ * traction, speed, speed_efficiency, iter_no). With gr_fa2_positions /
+ * gr_fa2_set_positions it is the whole state a run carries from tick to tick. */
+typedef struct gr_fa2_controller {
+    double swing, traction, speed, speed_efficiency;
+    uint32_t iter_no, converged;
+} gr_fa2_controller;
+int gr_fa2_get_controller(gr_fa2 *h, gr_fa2_controller *out);
+int gr_fa2_set_controller(gr_fa2 *h, const gr_fa2_controller *in);
+
+/* Adjoint (vector-Jacobian product) of a run, through each tick's tree (its far /
+ * pair decisions held fixed; cell centres move with their points) and the speed
+ * controller's active branch. No counterpart in the reference.
+ * gr_fa2_adjoint_forward runs `ticks` ticks from the current state, recording
+ * positions and controller every `checkpoint_every` ticks; gr_fa2_adjoint_backward
+ * takes dL/d(final positions) (host, n x dim) and returns dL/d(start positions)
+ * (host, n x dim) and, when dL_dw is not NULL, dL/d(raw edge weight) (host, m; 0
+ * for a self-loop or a repeated pair), replaying each segment from its checkpoint.
+ * The handle is left at the end of the recorded run. */
+int gr_fa2_adjoint_forward(gr_fa2 *h, uint32_t ticks, uint32_t checkpoint_every);
+int gr_fa2_adjoint_backward(gr_fa2 *h, const float *dL_dpT, float *dL_dp0, double *dL_dw);
+
 /* The stream every call of this handle enqueues on (default: the handle's own). */
 int gr_fa2_set_stream(gr_fa2 *h, void *cuda_stream);
 

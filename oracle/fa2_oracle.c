@@ -946,3 +946,333 @@ void orc_fa2_repel_delta(const orc_fa2 *s, uint32_t i, uint32_t j, double *out) 
     repel_delta(s, i, j, dl);
     for (int a = 0; a < s->dim; a++) out[a] = dl[a];
 }
+
+/* ------------------------------------------------------------ adjoint --- */
+/*
+ * The vector-Jacobian product of a run of ticks (no counterpart in the
+ * reference, which has no gradient): the exact derivative of iterate()
+ * (state.rs:130-148) with respect to the positions and the attraction
+ * coefficients, through the tree each tick built (its far / pair decisions are
+ * held fixed; cell centres still move with the points) and through the speed
+ * controller on its active branch (estimate_factor's comparisons held fixed).
+ * The coincident-pair jiggle is a constant and contributes nothing.
+ */
+
+typedef struct {
+    double SW, TR, speed, se;
+    uint32_t iter;
+} ctrl;
+
+/* estimate_factor on explicit state, also returning its partial derivatives:
+ * d[0..3] = d speed'/d(SW, TR, speed, se), d[4] = d se'/d se. */
+static void ef_diff(double n, double jt, const ctrl *in, double *speed_out, double *se_out, double *d) {
+    const double SW = in->SW, TR = in->TR;
+    const double opt = 0.05 * sqrt(n), minj = sqrt(opt);
+    const double ratio = opt * TR / (n * n);
+    double other = ratio < 10.0 ? ratio : 10.0;
+    double djit_dTR = 0.0;
+    double jitter;
+    if (minj >= other) {
+        jitter = jt * minj;
+    } else {
+        jitter = jt * other;
+        if (ratio < 10.0) djit_dTR = jt * opt / (n * n);
+    }
+    double se = in->se, k1 = 1.0;
+    if (SW / TR > 2.0) {
+        if (se > 0.05) k1 = 0.5;
+        if (jt > jitter) {
+            jitter = jt;
+            djit_dTR = 0.0;
+        }
+    }
+    const double se1 = se * k1;
+    double target = INFINITY, dt_dSW = 0.0, dt_dTR = 0.0, dt_dse = 0.0;
+    if (SW != 0.0) {
+        target = jitter * se1 * TR / SW;
+        dt_dSW = -target / SW;
+        dt_dTR = jitter * se1 / SW + se1 * TR / SW * djit_dTR;
+        dt_dse = jitter * k1 * TR / SW;
+    }
+    double k2 = 1.0;
+    if (SW > jitter * TR) {
+        if (se1 > 0.05) k2 = 0.7;
+    } else if (in->speed < 1000.0) {
+        k2 = 1.3;
+    }
+    *se_out = se1 * k2;
+    d[4] = k1 * k2;
+    const double sp = in->speed;
+    if (target - sp < 0.5 * sp) {
+        *speed_out = sp + (target - sp);
+        d[0] = dt_dSW;
+        d[1] = dt_dTR;
+        d[2] = 0.0;
+        d[3] = dt_dse;
+    } else {
+        *speed_out = sp + 0.5 * sp;
+        d[0] = d[1] = d[3] = 0.0;
+        d[2] = 1.5;
+    }
+}
+
+/* d (k m_i M d / |d|^2) / d d, applied to v: k m_i M (v/|d|^2 - 2 d (d.v)/|d|^4). */
+static void rep_jac(int dim, double coef, const double *dl, const double *v, double *out) {
+    double d2 = norm2(dl, dim), dv = 0.0;
+    for (int a = 0; a < dim; a++) dv += dl[a] * v[a];
+    for (int a = 0; a < dim; a++) out[a] = coef * (v[a] / d2 - 2.0 * dl[a] * dv / (d2 * d2));
+}
+
+/* Adjoint of one tick at the state's current positions and controller `c`
+ * (the values before the tick). In: lam1 = dL/dp', L1 = adjoint of the
+ * controller after the tick (SW', TR', speed', se'). Out: lam0 = dL/dp,
+ * L0 = adjoint of the controller before, gc += dL/dc per simple edge. */
+static void tick_adjoint(orc_fa2 *s, const ctrl *c, const double *lam1, const double *L1, double *lam0, double *L0,
+                         double *gc) {
+    const int d = s->dim;
+    const uint32_t n = s->n;
+    const double N = (double)n;
+    s->iter_no = c->iter;
+    orc_fa2_accumulate(s, 7); /* u at these positions, and this tick's tree */
+    double sw = 0.0, tr = 0.0;
+    swing_traction(s, &sw, &tr);
+    ctrl after = {c->SW + sw, c->TR + tr, c->speed, c->se, c->iter};
+    double speed1, se1, dd[5];
+    ef_diff(N, s->P.jitter_tolerance, &after, &speed1, &se1, dd);
+    double *ub = (double *)calloc((size_t)n * MAXD, sizeof(double));
+    /* update: p' = p + f u, f = speed1 / (1 + sqrt(speed1 m |u|)) */
+    double Lsp = L1[2];
+    for (uint32_t i = 0; i < n; i++) {
+        const double *u = s->u + (size_t)i * MAXD, *l = lam1 + (size_t)i * d;
+        double un = sqrt(norm2(u, d)), m = s->mass[i];
+        double q = sqrt(speed1 * m * un), f = speed1 / (1.0 + q);
+        double lu = 0.0;
+        for (int a = 0; a < d; a++) lu += l[a] * u[a];
+        double dfds = q > 0.0 ? (1.0 + 0.5 * q) / ((1.0 + q) * (1.0 + q)) : 1.0;
+        Lsp += lu * dfds;
+        for (int a = 0; a < d; a++) {
+            lam0[(size_t)i * d + a] = l[a];
+            ub[(size_t)i * MAXD + a] = f * l[a];
+        }
+        if (q > 0.0) { /* grad_u f = -speed1/(1+q)^2 * speed1 m u / (2 q |u|) */
+            double g = -speed1 / ((1.0 + q) * (1.0 + q)) * speed1 * m / (2.0 * q * un);
+            for (int a = 0; a < d; a++) ub[(size_t)i * MAXD + a] += lu * g * u[a];
+        }
+    }
+    /* controller: speed1 = EF(SW', TR', speed, se), se1 likewise */
+    const double Lse = L1[3];
+    double LSW = L1[0] + Lsp * dd[0], LTR = L1[1] + Lsp * dd[1];
+    L0[2] = Lsp * dd[2];
+    L0[3] = Lsp * dd[3] + Lse * dd[4];
+    L0[0] = LSW;
+    L0[1] = LTR;
+    /* swing = sum m |p - u|, traction = sum 0.5 m |p + u| */
+    for (uint32_t i = 0; i < n; i++) {
+        const double *p = s->p + (size_t)i * MAXD, *u = s->u + (size_t)i * MAXD;
+        double b[MAXD], g[MAXD], m = s->mass[i];
+        for (int a = 0; a < d; a++) {
+            b[a] = p[a] - u[a];
+            g[a] = p[a] + u[a];
+        }
+        double bn = sqrt(norm2(b, d)), gn = sqrt(norm2(g, d));
+        for (int a = 0; a < d; a++) {
+            double tb = bn > 0.0 ? LSW * m * b[a] / bn : 0.0;
+            double tg = gn > 0.0 ? LTR * 0.5 * m * g[a] / gn : 0.0;
+            lam0[(size_t)i * d + a] += tb + tg;
+            ub[(size_t)i * MAXD + a] += -tb + tg;
+        }
+    }
+    /* gravity: g_i = -gm c/|c| (or -gm c), c = p - mean */
+    {
+        double vmean[MAXD] = {0, 0, 0};
+        double *v = (double *)calloc((size_t)n * MAXD, sizeof(double));
+        double mean[MAXD];
+        pos_mean(s, mean);
+        for (uint32_t i = 0; i < n; i++) {
+            double cc[MAXD], gm = s->P.gravity * s->mass[i];
+            const double *ui = ub + (size_t)i * MAXD;
+            for (int a = 0; a < d; a++) cc[a] = s->p[(size_t)i * MAXD + a] - mean[a];
+            double *vi = v + (size_t)i * MAXD;
+            if (s->P.strong_gravity) {
+                for (int a = 0; a < d; a++) vi[a] = -gm * ui[a];
+            } else {
+                double cn = sqrt(norm2(cc, d));
+                if (cn > 0.0) {
+                    double cu = 0.0;
+                    for (int a = 0; a < d; a++) cu += cc[a] * ui[a];
+                    for (int a = 0; a < d; a++) vi[a] = -gm * (ui[a] - cc[a] * cu / (cn * cn)) / cn;
+                }
+            }
+            for (int a = 0; a < d; a++) vmean[a] += vi[a];
+        }
+        for (int a = 0; a < d; a++) vmean[a] /= N;
+        for (uint32_t i = 0; i < n; i++)
+            for (int a = 0; a < d; a++) lam0[(size_t)i * d + a] += v[(size_t)i * MAXD + a] - vmean[a];
+        free(v);
+    }
+    /* attraction: a_i = sum_j c phi(|delta|) delta, delta = p_j - p_i; u_i += a_i (/ m_i) */
+    for (int64_t e = 0; e < s->m; e++) {
+        uint32_t i = s->lo[e], j = s->hi[e];
+        double dl[MAXD], ai[MAXD], aj[MAXD];
+        double mi = s->P.dissuade_hubs ? s->mass[i] : 1.0, mj = s->P.dissuade_hubs ? s->mass[j] : 1.0;
+        for (int a = 0; a < d; a++) {
+            dl[a] = s->p[(size_t)j * MAXD + a] - s->p[(size_t)i * MAXD + a];
+            ai[a] = ub[(size_t)i * MAXD + a] / mi;
+            aj[a] = ub[(size_t)j * MAXD + a] / mj;
+        }
+        double dist = sqrt(norm2(dl, d));
+        double phi = 1.0, dphi = 0.0;
+        if (s->P.lin_log) {
+            if (dist > 0.0) {
+                phi = log(1.0 + dist) / dist;
+                dphi = (dist / (1.0 + dist) - log(1.0 + dist)) / (dist * dist);
+            } else {
+                phi = 0.0; /* the forward's zero-distance convention */
+            }
+        }
+        double cw = s->w[e];
+        double diff[MAXD], ddot = 0.0;
+        for (int a = 0; a < d; a++) {
+            diff[a] = aj[a] - ai[a];
+            ddot += dl[a] * diff[a];
+        }
+        /* lam_j += J (a_j - a_i)... J = c (phi I + dphi delta delta^T / dist) */
+        for (int a = 0; a < d; a++) {
+            double jv = cw * (phi * diff[a] + (dist > 0.0 ? dphi * dl[a] * ddot / dist : 0.0));
+            lam0[(size_t)j * d + a] -= jv;
+            lam0[(size_t)i * d + a] += jv;
+        }
+        double g = 0.0;
+        for (int a = 0; a < d; a++) g += phi * (ai[a] - aj[a]) * dl[a];
+        gc[e] += g;
+    }
+    /* repulsion */
+    const double kr = s->P.scaling_ratio;
+    if (s->P.theta < 0.0) {
+        for (uint32_t i = 0; i < n; i++)
+            for (uint32_t j = i + 1; j < n; j++) {
+                double dl[MAXD], v[MAXD], out[MAXD];
+                int zero = 1;
+                for (int a = 0; a < d; a++) {
+                    dl[a] = s->p[(size_t)i * MAXD + a] - s->p[(size_t)j * MAXD + a];
+                    if (dl[a] != 0.0) zero = 0;
+                    v[a] = ub[(size_t)i * MAXD + a] - ub[(size_t)j * MAXD + a];
+                }
+                if (zero) continue;
+                rep_jac(d, kr * s->mass[i] * s->mass[j], dl, v, out);
+                for (int a = 0; a < d; a++) {
+                    lam0[(size_t)i * d + a] += out[a];
+                    lam0[(size_t)j * d + a] -= out[a];
+                }
+            }
+    } else {
+        ttree *t = &s->tree;
+        double th2 = s->P.theta * s->P.theta;
+        double *cbar = (double *)calloc(t->ncells * MAXD + 1, sizeof(double));
+        for (size_t p = 0; p < t->norder; p++) {
+            uint32_t i = t->order[p];
+            const double *xi = s->p + (size_t)i * MAXD, *ui = ub + (size_t)i * MAXD;
+            double mi = s->mass[i];
+            size_t k = 0;
+            while (k < t->ncells) {
+                const tcell *cl = &t->cells[k];
+                int holds = cl->start <= p && p < cl->end;
+                const tbody *b = &t->bodies[k];
+                double dl[MAXD];
+                for (int a = 0; a < d; a++) dl[a] = xi[a] - b->c[a];
+                double d2 = norm2(dl, d), w = cl->b1[0] - cl->b0[0];
+                if (!holds && d2 > 0.0 && w * w < th2 * d2) {
+                    double out[MAXD];
+                    rep_jac(d, kr * mi * b->mass, dl, ui, out);
+                    for (int a = 0; a < d; a++) {
+                        lam0[(size_t)i * d + a] += out[a];
+                        cbar[k * MAXD + a] -= out[a];
+                    }
+                    k = cl->skip;
+                } else if (cl->skip == k + 1) {
+                    for (uint32_t q = cl->start; q < cl->end; q++) {
+                        uint32_t j = t->order[q];
+                        if (j == i) continue;
+                        double dj[MAXD], out[MAXD];
+                        int zero = 1;
+                        for (int a = 0; a < d; a++) {
+                            dj[a] = xi[a] - s->p[(size_t)j * MAXD + a];
+                            if (dj[a] != 0.0) zero = 0;
+                        }
+                        if (zero) continue;
+                        rep_jac(d, kr * mi * s->mass[j], dj, ui, out);
+                        for (int a = 0; a < d; a++) {
+                            lam0[(size_t)i * d + a] += out[a];
+                            lam0[(size_t)j * d + a] -= out[a];
+                        }
+                    }
+                    k++;
+                } else {
+                    k++;
+                }
+            }
+        }
+        /* a cell centre is sum m_j p_j / M over its points */
+        for (size_t k = 0; k < t->ncells; k++) {
+            const tcell *cl = &t->cells[k];
+            double M = t->bodies[k].mass;
+            for (uint32_t q = cl->start; q < cl->end; q++) {
+                uint32_t j = t->order[q];
+                for (int a = 0; a < d; a++) lam0[(size_t)j * d + a] += s->mass[j] / M * cbar[k * MAXD + a];
+            }
+        }
+        free(cbar);
+    }
+    free(ub);
+}
+
+/* Runs `ticks` ticks from the current state, recording each tick's positions
+ * and controller, then pulls lamT = dL/d(final positions) (n x dim) back:
+ * lam0 = dL/d(start positions) (n x dim), gc = dL/d(attraction coefficient) per
+ * simple edge (the caller multiplies by dc/dw). The state ends at the final
+ * positions. */
+void orc_fa2_adjoint(orc_fa2 *s, uint32_t ticks, const double *lamT, double *lam0, double *gc) {
+    const int d = s->dim;
+    const uint32_t n = s->n;
+    double *hist = (double *)malloc(((size_t)ticks + 1) * n * MAXD * sizeof(double) + 8);
+    ctrl *cs = (ctrl *)malloc(((size_t)ticks + 1) * sizeof(ctrl));
+    for (uint32_t t = 0; t < ticks; t++) {
+        memcpy(hist + (size_t)t * n * MAXD, s->p, (size_t)n * MAXD * sizeof(double));
+        cs[t] = (ctrl){s->swing, s->traction, s->speed, s->speed_efficiency, s->iter_no};
+        orc_fa2_iterate(s);
+    }
+    double *lam = (double *)malloc((size_t)n * d * sizeof(double) + 8);
+    double *nxt = (double *)malloc((size_t)n * d * sizeof(double) + 8);
+    memcpy(lam, lamT, (size_t)n * d * sizeof(double));
+    double L1[4] = {0, 0, 0, 0}, L0[4];
+    for (int64_t e = 0; e < s->m; e++) gc[e] = 0.0;
+    double *keep = (double *)malloc((size_t)n * MAXD * sizeof(double) + 8);
+    memcpy(keep, s->p, (size_t)n * MAXD * sizeof(double));
+    ctrl last = {s->swing, s->traction, s->speed, s->speed_efficiency, s->iter_no};
+    for (uint32_t t = ticks; t-- > 0;) {
+        memcpy(s->p, hist + (size_t)t * n * MAXD, (size_t)n * MAXD * sizeof(double));
+        tick_adjoint(s, &cs[t], lam, L1, nxt, L0, gc);
+        memcpy(lam, nxt, (size_t)n * d * sizeof(double));
+        memcpy(L1, L0, sizeof L1);
+    }
+    memcpy(lam0, lam, (size_t)n * d * sizeof(double));
+    memcpy(s->p, keep, (size_t)n * MAXD * sizeof(double));
+    s->swing = last.SW;
+    s->traction = last.TR;
+    s->speed = last.speed;
+    s->speed_efficiency = last.se;
+    s->iter_no = last.iter;
+    free(keep);
+    free(lam);
+    free(nxt);
+    free(hist);
+    free(cs);
+}
+
+/* The simple edges' attraction coefficients (w^influence), in / out. */
+void orc_fa2_get_coef(const orc_fa2 *s, double *out) {
+    for (int64_t e = 0; e < s->m; e++) out[e] = s->w[e];
+}
+void orc_fa2_set_coef(orc_fa2 *s, const double *in) {
+    for (int64_t e = 0; e < s->m; e++) s->w[e] = in[e];
+}

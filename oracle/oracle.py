@@ -219,3 +219,40 @@ class State:
         return dict(width=width[:k], skip=skip[:k], start=start[:k], end=end[:k],
                     mass=mass[:k], com=com[:k * self.dim].reshape(-1, self.dim),
                     order=order[:self.n])
+
+
+def _adjoint_lib():
+    L = lib()
+    if not getattr(L, "_adj", False):
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+        L.orc_fa2_adjoint.argtypes = [C.c_void_p, C.c_uint32, f64p, f64p, f64p]
+        L.orc_fa2_get_coef.argtypes = [C.c_void_p, f64p]
+        L.orc_fa2_set_coef.argtypes = [C.c_void_p, f64p]
+        L._adj = True
+    return L
+
+
+def adjoint(state: "State", ticks: int, lam_T) -> tuple:
+    """VJP of `ticks` ticks from the state's current positions: (dL/dp0, dL/dc per
+    simple edge) for lam_T = dL/dp_T. The state ends at the final positions."""
+    L = _adjoint_lib()
+    lam_T = np.ascontiguousarray(lam_T, np.float64).reshape(-1)
+    lam0 = np.zeros(state.n * state.dim, np.float64)
+    gc = np.zeros(max(len(state._lo), 1), np.float64)
+    L.orc_fa2_adjoint(state.h, ticks, lam_T, lam0, gc)
+    return lam0.reshape(state.n, state.dim), gc[:len(state._lo)]
+
+
+def coef(state: "State") -> np.ndarray:
+    L = _adjoint_lib()
+    out = np.zeros(max(len(state._lo), 1), np.float64)
+    L.orc_fa2_get_coef(state.h, out)
+    return out[:len(state._lo)]
+
+
+def set_coef(state: "State", c) -> None:
+    L = _adjoint_lib()
+    c = np.ascontiguousarray(c, np.float64)
+    if len(c) == 0:
+        c = np.zeros(1)
+    L.orc_fa2_set_coef(state.h, c)
