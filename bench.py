@@ -317,6 +317,8 @@ def run_gpu(args, dist: Dist):
     wl = workload(args.workload, args.n)
     dim = int(wl.params.get("dim", 2))
     eng = Fa2(wl.n, wl.src, wl.dst, wl.weight, params=wl.params, pos0=wl.pos0)
+    eng.tick(1)
+    schedule, schedule_ms = eng.tune(3)  # walk schedule autotuner (state restored)
     eng.tick(max(args.warmup, 3))
     torch.cuda.synchronize()
     info0 = eng.info()
@@ -403,11 +405,14 @@ def run_gpu(args, dist: Dist):
                        "l2": f"{FLUSH_BYTES >> 20} MiB buffer overwritten before every timed tick "
                              "(outside the events)",
                        "parallelism": f"{dist.world} independent replicas" if dist.world > 1 else "1 GPU",
-                       "phase_ms": {"tree": tree_ms, "walk": walk_ms, "finish": fin_ms}},
+                       "phase_ms": {"tree": tree_ms, "walk": walk_ms, "finish": fin_ms},
+                       "walk_schedule": {"chosen": ["warp-union", "per-lane"][schedule],
+                                         "tuned_walk_ms": {"warp-union": schedule_ms[0],
+                                                           "per-lane": schedule_ms[1]}}},
             "clocks": clocks,
             "e2e": e2e,
             "gpu_launches": int(info1["graph_kernels"]) * done,
-            "roofline": {"kernel": "k_walk", "bound": "fp32", "achieved": achieved / 1e12,
+            "roofline": {"kernel": "k_walk_s", "bound": "fp32", "achieved": achieved / 1e12,
                          "peak": fp32_peak / 1e12, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                          "traffic": None,
                          "peak_source": "nominal FP32 FMA rate, 148 SM x 128 lanes x 2 x sm_max_mhz "

@@ -143,6 +143,7 @@ struct gr_fa2 {
     float4 *sp = nullptr;
     BinTree bt{};
     Body *leaf_body = nullptr, *int_body = nullptr;
+    BodyDD *dd_prefix = nullptr, *dd_bsum = nullptr;
     uint8_t *leaf_coinc = nullptr;
     Cells cells{};
     float *rep = nullptr, *U = nullptr;
@@ -154,6 +155,7 @@ struct gr_fa2 {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint32_t graph_kernels = 0;
+    int walk_schedule = 1;  // 0: warp-cooperative union walk, 1: per-lane walk
     // the same tick as three graphs (tree, walk, forces+update) for per-phase timing
     cudaGraph_t pgraph[3] = {nullptr, nullptr, nullptr};
     cudaGraphExec_t pexec[3] = {nullptr, nullptr, nullptr};
@@ -223,6 +225,8 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
     A(h->leaf_body, n);
     A(h->int_body, n);
     A(h->leaf_coinc, n);
+    A(h->dd_prefix, (size_t)n + 1);
+    A(h->dd_bsum, div_up(n, AG_TILE) + 1);
     A(h->cells.A, 2 * (size_t)n);
     A(h->cells.B, 2 * (size_t)n);
     if (D == 3) A(h->cells.C, 2 * (size_t)n);
@@ -253,8 +257,12 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
         h->scanner.scan(h->flag, h->excl, n, nullptr, 0, &st->n_unique, nullptr, s, conv);
         k_leaves<<<gn, 256, 0, s>>>(n, st, h->keys, h->flag, h->excl, h->leaf_start, h->ukey, h->uid);
         k_karras<<<gn, 256, 0, s>>>(st, h->ukey, h->bt);
-        k_aggregate<D><<<gn, 256, 0, s>>>(st, h->sp, h->leaf_start, h->bt, h->leaf_body, h->int_body,
-                                          h->leaf_coinc);
+        k_leaf_body<D><<<gn, 256, 0, s>>>(st, h->sp, h->leaf_start, h->leaf_body, h->leaf_coinc);
+        const uint32_t ab = div_up(n, AG_TILE);
+        k_dd_reduce<<<ab, AG_T, 0, s>>>(st, h->leaf_body, h->dd_bsum);
+        k_dd_blocks<<<1, AG_T, 0, s>>>(st, h->dd_bsum, h->dd_prefix);
+        k_dd_down<<<ab, AG_T, 0, s>>>(st, h->leaf_body, h->dd_bsum, h->dd_prefix);
+        k_node_body<<<gn, 256, 0, s>>>(st, h->bt, h->dd_prefix, h->int_body);
         k_count<D><<<gn, 256, 0, s>>>(st, h->bt, h->cells_at);
         h->scanner.scan(h->cells_at, h->P, n, &st->n_unique, 0, &st->n_cells, nullptr, s, conv);
         k_assign<D><<<gn, 256, 0, s>>>(st, h->bt, h->sp, h->P, h->cells_at, h->leaf_start, h->leaf_body, h->int_body,
@@ -266,8 +274,12 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
         wp.kr = (float)h->prm[P_SCALING];
         wp.theta2 = (float)(h->prm[P_THETA] * h->prm[P_THETA]);
         wp.seed = (uint32_t)h->prm[P_SEED];
-        k_walk<D><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig, h->uid,
-                                                                    h->leaf_pre, h->rep, st);
+        if (h->walk_schedule == 1)
+            k_walk_s<D, true><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig,
+                                                                                h->uid, h->leaf_pre, h->rep, st);
+        else
+            k_walk_s<D, false><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig,
+                                                                                 h->uid, h->leaf_pre, h->rep, st);
     }
     if (phases & PH_FINISH) {
         ForceParams fp;
@@ -768,6 +780,57 @@ int gr_fa2_get_info(gr_fa2 *h, gr_fa2_info *out) {
     return ok();
 }
 
+int gr_fa2_set_walk_schedule(gr_fa2 *h, int schedule) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    if (schedule != 0 && schedule != 1) return set_err(GR_INVALID_ARGUMENT, "walk schedule must be 0 or 1");
+    if (schedule != h->walk_schedule) {
+        h->walk_schedule = schedule;
+        h->drop_graphs();
+    }
+    return ok();
+}
+
+int gr_fa2_tune(gr_fa2 *h, uint32_t sample_ticks, int *chosen, float *walk_ms_each) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    if (h->n == 0) return ok();
+    if (sample_ticks == 0) sample_ticks = 1;
+    // time each walk schedule over the same ticks from the same state, then restore it
+    float4 *save_p = nullptr;
+    DevState save_s;
+    CU(cudaMalloc(&save_p, (size_t)h->n * sizeof(float4)));
+    CU(cudaMemcpyAsync(save_p, h->pos, (size_t)h->n * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream));
+    if (int c = read_state(h, &save_s)) {
+        cudaFree(save_p);
+        return c;
+    }
+    std::vector<float> ms(4 * (size_t)sample_ticks);
+    float best = 1e30f;
+    int pick = h->walk_schedule, rc = GR_OK;
+    for (int sch = 0; sch < 2 && rc == GR_OK; sch++) {
+        h->walk_schedule = sch;
+        h->drop_graphs();
+        uint32_t done = 0;
+        rc = gr_fa2_tick_timed(h, sample_ticks, 0, ms.data(), &done);
+        float w = 0.f;
+        for (uint32_t t = 0; t < done; t++) w += ms[4 * t + 1];
+        w /= std::max(done, 1u);
+        if (walk_ms_each) walk_ms_each[sch] = w;
+        if (rc == GR_OK && done && w < best) {
+            best = w;
+            pick = sch;
+        }
+        cudaMemcpyAsync(h->pos, save_p, (size_t)h->n * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream);
+        cudaMemcpyAsync(h->st, &save_s, sizeof save_s, cudaMemcpyHostToDevice, h->stream);
+        cudaStreamSynchronize(h->stream);
+    }
+    cudaFree(save_p);
+    h->walk_schedule = pick;
+    h->drop_graphs();
+    if (chosen) *chosen = pick;
+    if (rc) return rc;
+    return ok();
+}
+
 int gr_fa2_get_controller(gr_fa2 *h, gr_fa2_controller *out) {
     if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
     if (!out) return set_err(GR_INVALID_ARGUMENT, "out is null");
@@ -845,7 +908,7 @@ int gr_run(const char *layout_id, uint32_t n, uint64_t m, const uint32_t *src, c
 // cudaFree or any allocating routine.
 
 constexpr uint32_t STATIC_MAX_N = GR_FORCES_STATIC_MAX_N;
-constexpr size_t STATIC_BYTES_PER_NODE = 320;
+constexpr size_t STATIC_BYTES_PER_NODE = 400;
 constexpr size_t STATIC_BYTES = STATIC_BYTES_PER_NODE * STATIC_MAX_N + (1u << 20);
 
 static __device__ __align__(256) unsigned char g_static_scratch[STATIC_BYTES];
@@ -926,6 +989,8 @@ static int forces_static(uint32_t n, const float4 *nodes, const uint32_t *rp, co
     h.leaf_body = cv.take<Body>(n);
     h.int_body = cv.take<Body>(n);
     h.leaf_coinc = cv.take<uint8_t>(n);
+    h.dd_prefix = cv.take<BodyDD>((size_t)n + 1);
+    h.dd_bsum = cv.take<BodyDD>(div_up(n, AG_TILE) + 1);
     h.cells.A = cv.take<float4>(2 * (size_t)n);
     h.cells.B = cv.take<float4>(2 * (size_t)n);
     h.cells.C = D == 3 ? cv.take<int2>(2 * (size_t)n) : nullptr;

@@ -367,6 +367,173 @@ __global__ void k_aggregate(DevState *st, const float4 *__restrict__ sp,
     aggregate_leaf<D>(s, sp, leaf_start, t, leaf_body, int_body, leaf_coinc, &st->error);
 }
 
+// ---- bodies without atomics: leaf sums, a double-double prefix over the
+// leaves in key order, and every internal node's body as the difference of the
+// prefixes at its range ends. The prefix is exact to ~1e-32 of its magnitude,
+// so a node's sums are as exact as a direct FP64 sum; the scan's decomposition
+// is fixed, so the result is the same every run.
+
+struct DD {
+    double hi, lo;
+};
+
+__device__ __forceinline__ DD dd_add(DD a, DD b) {  // Knuth's two-sum, renormalised
+    const double s = a.hi + b.hi;
+    const double bb = s - a.hi;
+    double e = (a.hi - (s - bb)) + (b.hi - bb);
+    e += a.lo + b.lo;
+    const double hi = s + e;
+    return DD{hi, e - (hi - s)};
+}
+
+struct BodyDD {
+    DD m, c0, c1, c2;
+};
+
+__device__ __forceinline__ BodyDD bdd_add(const BodyDD &a, const BodyDD &b) {
+    return BodyDD{dd_add(a.m, b.m), dd_add(a.c0, b.c0), dd_add(a.c1, b.c1), dd_add(a.c2, b.c2)};
+}
+
+__device__ __forceinline__ BodyDD bdd_of(const Body &b) {
+    return BodyDD{{b.m, 0.0}, {b.c0, 0.0}, {b.c1, 0.0}, {b.c2, 0.0}};
+}
+
+__device__ __forceinline__ double dd_diff(DD a, DD b) { return dd_add(a, DD{-b.hi, -b.lo}).hi; }
+
+constexpr int AG_T = 256, AG_I = 4, AG_TILE = AG_T * AG_I, AG_W = AG_T / GR_WARP;
+
+template <int D>
+__global__ void k_leaf_body(const DevState *st, const float4 *__restrict__ sp, const uint32_t *__restrict__ leaf_start,
+                            Body *__restrict__ leaf_body, uint8_t *__restrict__ leaf_coinc) {
+    if (st->converged) return;
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= st->n_unique) return;
+    const uint32_t a0 = leaf_start[s], a1 = leaf_start[s + 1];
+    Body b{0.0, 0.0, 0.0, 0.0};
+    const float4 f0 = sp[a0];
+    bool coinc = true;
+    for (uint32_t q = a0; q < a1; q++) {
+        const float4 p = sp[q];
+        const double m = (double)p.w;
+        b.m += m;
+        b.c0 += m * (double)p.x;
+        b.c1 += m * (double)p.y;
+        if (D == 3) b.c2 += m * (double)p.z;
+        coinc = coinc && p.x == f0.x && p.y == f0.y && (D == 2 || p.z == f0.z);
+    }
+    body_store(&leaf_body[s], b);
+    leaf_coinc[s] = coinc ? 1 : 0;
+}
+
+__device__ __forceinline__ DD dd_shfl_up(DD v, int o) {
+    return DD{__shfl_up_sync(GR_FULL, v.hi, o), __shfl_up_sync(GR_FULL, v.lo, o)};
+}
+
+// Inclusive warp scan of BodyDD, a fixed Hillis-Steele shape.
+__device__ __forceinline__ BodyDD warp_scan_bdd(BodyDD v) {
+    const int lane = threadIdx.x % GR_WARP;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const BodyDD u{dd_shfl_up(v.m, o), dd_shfl_up(v.c0, o), dd_shfl_up(v.c1, o), dd_shfl_up(v.c2, o)};
+        if (lane >= o) v = bdd_add(u, v);
+    }
+    return v;
+}
+
+// Exclusive block scan (AG_T threads) of one BodyDD per thread, offset by
+// `carry`; returns this thread's exclusive prefix and the block total.
+__device__ __forceinline__ BodyDD block_scan_bdd(const BodyDD &x, const BodyDD &carry, BodyDD &total,
+                                                 BodyDD *s_w) {
+    const int lane = threadIdx.x % GR_WARP, w = threadIdx.x / GR_WARP;
+    const BodyDD inc = warp_scan_bdd(x);
+    if (lane == 31) s_w[w] = inc;
+    __syncthreads();
+    if (w == 0) {  // scan the warp totals (one per lane < AG_W)
+        BodyDD t = lane < AG_W ? s_w[lane] : BodyDD{};
+        t = warp_scan_bdd(t);
+        if (lane < AG_W) s_w[AG_W + lane] = t;
+    }
+    __syncthreads();
+    const BodyDD before = w > 0 ? s_w[AG_W + w - 1] : BodyDD{};
+    total = bdd_add(carry, s_w[AG_W + AG_W - 1]);
+    // exclusive prefix: carry + warps before + lanes before (inc - x recomputed as a shifted scan)
+    BodyDD lanes_before{dd_shfl_up(inc.m, 1), dd_shfl_up(inc.c0, 1), dd_shfl_up(inc.c1, 1), dd_shfl_up(inc.c2, 1)};
+    if (lane == 0) lanes_before = BodyDD{};
+    __syncthreads();
+    return bdd_add(bdd_add(carry, before), lanes_before);
+}
+
+// Sequential double-double sum of this thread's AG_I leaves.
+__device__ __forceinline__ BodyDD thread_chunk(const Body *__restrict__ lb, uint32_t base, uint32_t nu) {
+    BodyDD acc{};
+    for (int r = 0; r < AG_I; r++) {
+        const uint32_t s = base + r;
+        if (s < nu) acc = bdd_add(acc, bdd_of(lb[s]));
+    }
+    return acc;
+}
+
+__global__ void __launch_bounds__(AG_T) k_dd_reduce(const DevState *st, const Body *__restrict__ lb,
+                                                    BodyDD *__restrict__ bsum) {
+    if (st->converged) return;
+    __shared__ BodyDD s_w[2 * AG_W];
+    const uint32_t nu = st->n_unique;
+    const uint32_t base = blockIdx.x * AG_TILE;
+    if (base >= nu) return;
+    BodyDD total;
+    block_scan_bdd(thread_chunk(lb, base + threadIdx.x * AG_I, nu), BodyDD{}, total, s_w);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+// One block: exclusive prefix of the block sums in block order (in place); the
+// total is the prefix at nu.
+__global__ void __launch_bounds__(AG_T) k_dd_blocks(const DevState *st, BodyDD *__restrict__ bsum,
+                                                    BodyDD *__restrict__ prefix) {
+    if (st->converged) return;
+    __shared__ BodyDD s_w[2 * AG_W];
+    const uint32_t nu = st->n_unique;
+    const uint32_t nb = (nu + AG_TILE - 1) / AG_TILE;
+    BodyDD carry{};
+    for (uint32_t off = 0; off < nb; off += AG_T) {
+        const uint32_t b = off + threadIdx.x;
+        const BodyDD x = b < nb ? bsum[b] : BodyDD{};
+        BodyDD total;
+        const BodyDD ex = block_scan_bdd(x, carry, total, s_w);
+        if (b < nb) bsum[b] = ex;
+        carry = total;
+    }
+    if (threadIdx.x == 0) prefix[nu] = carry;
+}
+
+__global__ void __launch_bounds__(AG_T) k_dd_down(const DevState *st, const Body *__restrict__ lb,
+                                                  const BodyDD *__restrict__ bsum, BodyDD *__restrict__ prefix) {
+    if (st->converged) return;
+    __shared__ BodyDD s_w[2 * AG_W];
+    const uint32_t nu = st->n_unique;
+    const uint32_t base = blockIdx.x * AG_TILE;
+    if (base >= nu) return;
+    const uint32_t mine = base + threadIdx.x * AG_I;
+    BodyDD total;
+    BodyDD run = block_scan_bdd(thread_chunk(lb, mine, nu), bsum[blockIdx.x], total, s_w);
+    for (int r = 0; r < AG_I; r++) {
+        const uint32_t s = mine + r;
+        if (s >= nu) break;
+        prefix[s] = run;
+        run = bdd_add(run, bdd_of(lb[s]));
+    }
+}
+
+// Internal node i covers leaves [first, last]: its sums are prefix[last + 1] -
+// prefix[first].
+__global__ void k_node_body(const DevState *st, BinTree t, const BodyDD *__restrict__ prefix,
+                            Body *__restrict__ int_body) {
+    if (st->converged) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i + 1 >= st->n_unique) return;
+    const BodyDD a = prefix[t.first[i]], b = prefix[t.last[i] + 1];
+    body_store(&int_body[i], Body{dd_diff(b.m, a.m), dd_diff(b.c0, a.c0), dd_diff(b.c1, a.c1), dd_diff(b.c2, a.c2)});
+}
+
 template <int D>
 __device__ __forceinline__ bool is_cell(const BinTree &t, int32_t node) {
     int32_t par = t.int_parent[node];

@@ -157,6 +157,139 @@ __device__ __forceinline__ void walk_group(const WalkView &V, uint32_t p, float 
     }
 }
 
+// The same per-node walk with every lane on its own cell index (gathered cell
+// loads, no warp vote): the warp runs as long as its longest path instead of
+// the union of its 32 paths. Each lane meets its cells in the same preorder and
+// adds the same terms in the same order as walk_group, so the forces are
+// bit-identical; only the schedule differs.
+template <int D>
+__device__ __forceinline__ void walk_lane(const WalkView &V, uint32_t p, float &f0, float &f1, float &f2,
+                                          uint32_t &nfar, uint32_t &npair) {
+    const Cells cells = V.cells;
+    const float4 *__restrict__ sp = V.sp;
+    const uint32_t n = V.n, ncells = V.ncells, iter = V.iter;
+    const bool valid = p < n;
+    const float4 me = valid ? sp[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t mylp = valid ? V.leaf_pre[V.uid[p]] : 0u;
+    const uint32_t oi = valid ? V.sorig[p] : 0u;
+    f0 = f1 = f2 = 0.f;
+    nfar = npair = 0;
+    const float kr = V.kr, th2 = V.th2;
+    uint32_t k = valid ? 0u : ncells;
+    while (k < ncells) {
+        const float4 A = __ldg(&cells.A[k]);
+        const float4 B = __ldg(&cells.B[k]);
+        int32_t sk;
+        uint32_t start;
+        float cx, cy, cz, cm, w2, lx, ly, lz;
+        if (D == 2) {
+            cx = A.x; cy = A.y; cz = 0.f; cm = A.z; w2 = A.w;
+            lx = B.x; ly = B.y; lz = 0.f;
+            sk = __float_as_int(B.z);
+            start = __float_as_uint(B.w);
+        } else {
+            const int2 Cc = __ldg(&cells.C[k]);
+            cx = A.x; cy = A.y; cz = A.z; cm = A.w;
+            lx = B.x; ly = B.y; lz = B.z; w2 = B.w;
+            sk = Cc.x;
+            start = (uint32_t)Cc.y;
+        }
+        const bool leaf = sk < 0;
+        uint32_t skip = leaf ? k + 1 : (uint32_t)sk;
+        if (skip <= k || skip > ncells) {  // malformed cell: record it, keep the walk finite
+            atomicOr(V.err, (uint32_t)ERR_TREE);
+            skip = k + 1;
+        }
+        const bool holds = (k <= mylp) && (mylp < skip);
+        const float dx = (me.x - cx) - lx;
+        const float dy = (me.y - cy) - ly;
+        const float dz = (D == 3) ? (me.z - cz) - lz : 0.f;
+        const float d2 = (D == 3) ? dx * dx + dy * dy + dz * dz : dx * dx + dy * dy;
+        const bool far = !holds && d2 > 0.f && w2 < th2 * d2;
+        if (far || (sk == -1 && !holds && d2 > 0.f)) {  // a body: far cell, or a one-point leaf's pair
+            const float f = __fdividef(me.w * cm, d2) * kr;
+            f0 += dx * f;
+            f1 += dy * f;
+            if (D == 3) f2 += dz * f;
+            if (far)
+                nfar++;
+            else
+                npair++;
+            k = skip;
+        } else if (leaf && !holds && sk == -1) {  // coincident one-point leaf: the jiggle
+            const uint32_t oj = __ldg(&V.sorig[start]);
+            const float sg = oi < oj ? 1.f : -1.f;
+            const float ex = sg * (float)jiggle(V.seed, iter, 0, oi, oj);
+            const float ey = sg * (float)jiggle(V.seed, iter, 1, oi, oj);
+            const float ez = (D == 3) ? sg * (float)jiggle(V.seed, iter, 2, oi, oj) : 0.f;
+            const float e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
+            const float f = __fdividef(me.w * cm, e2) * kr;
+            f0 += ex * f;
+            f1 += ey * f;
+            if (D == 3) f2 += ez * f;
+            npair++;
+            k = k + 1;
+        } else if (leaf) {  // several points (or this node's own leaf): exact pairs
+            int32_t cnt = -sk;
+            if (start >= n || (uint32_t)cnt > n - start) {
+                atomicOr(V.err, (uint32_t)ERR_TREE);
+                cnt = 0;
+            }
+            for (int32_t q = 0; q < cnt; q++) {
+                const uint32_t jp = start + (uint32_t)q;
+                if (jp == p) continue;
+                const float4 o = __ldg(&sp[jp]);
+                float ex = me.x - o.x, ey = me.y - o.y, ez = (D == 3) ? me.z - o.z : 0.f;
+                if (ex == 0.f && ey == 0.f && (D == 2 || ez == 0.f)) {
+                    const uint32_t oj = __ldg(&V.sorig[jp]);
+                    const float sg = oi < oj ? 1.f : -1.f;
+                    ex = sg * (float)jiggle(V.seed, iter, 0, oi, oj);
+                    ey = sg * (float)jiggle(V.seed, iter, 1, oi, oj);
+                    if (D == 3) ez = sg * (float)jiggle(V.seed, iter, 2, oi, oj);
+                }
+                const float e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
+                const float f = __fdividef(me.w * o.w, e2) * kr;
+                f0 += ex * f;
+                f1 += ey * f;
+                if (D == 3) f2 += ez * f;
+                npair++;
+            }
+            k = k + 1;
+        } else {
+            k = k + 1;
+        }
+    }
+}
+
+template <int D, bool LANE>
+__global__ void __launch_bounds__(WALK_THREADS)
+k_walk_s(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 *__restrict__ sp,
+         const uint32_t *__restrict__ sorig, const uint32_t *__restrict__ uid,
+         const uint32_t *__restrict__ leaf_pre, float *__restrict__ rep, DevState *stw) {
+    if (st->converged) return;
+    const uint32_t p = blockIdx.x * WALK_THREADS + threadIdx.x;
+    if (__all_sync(GR_FULL, p >= P.n)) return;
+    WalkView V{cells, sp, sorig, uid, leaf_pre, P.n, st->n_cells, st->iter_no, P.seed, P.kr, P.theta2, &stw->error};
+    float f0, f1, f2;
+    uint32_t nfar, npair;
+    if (LANE)
+        walk_lane<D>(V, p, f0, f1, f2, nfar, npair);
+    else
+        walk_group<D>(V, p, f0, f1, f2, nfar, npair);
+    if (p < P.n) {
+        const uint32_t oi = sorig[p];
+        rep[(size_t)oi * D + 0] = f0;
+        rep[(size_t)oi * D + 1] = f1;
+        if (D == 3) rep[(size_t)oi * D + 2] = f2;
+    }
+    nfar = __reduce_add_sync(GR_FULL, nfar);
+    npair = __reduce_add_sync(GR_FULL, npair);
+    if ((threadIdx.x % GR_WARP) == 0) {
+        atomicAdd(&stw->far_count, (unsigned long long)nfar);
+        atomicAdd(&stw->pair_count, (unsigned long long)npair);
+    }
+}
+
 template <int D>
 __global__ void __launch_bounds__(WALK_THREADS)
 k_walk(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 *__restrict__ sp,

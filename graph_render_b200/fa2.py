@@ -149,6 +149,16 @@ class Fa2:
         N.check(self._L.gr_fa2_get_info(self.h, C.byref(inf)))
         return inf.as_dict()
 
+    def set_walk_schedule(self, schedule: int) -> None:
+        N.check(self._L.gr_fa2_set_walk_schedule(self.h, int(schedule)))
+
+    def tune(self, sample_ticks: int = 3):
+        """Autotunes the walk schedule; returns (chosen, {schedule: mean walk ms})."""
+        chosen = C.c_int()
+        ms = np.zeros(2, np.float32)
+        N.check(self._L.gr_fa2_tune(self.h, int(sample_ticks), C.byref(chosen), _ptr(ms)))
+        return chosen.value, {0: float(ms[0]), 1: float(ms[1])}
+
     def controller(self) -> dict:
         c = N.Controller()
         N.check(self._L.gr_fa2_get_controller(self.h, C.byref(c)))

@@ -124,6 +124,15 @@ int gr_fa2_tick_record(gr_fa2 *h, uint32_t ticks, float *dev_out, uint32_t *done
  * cold L2. No counterpart in the reference (which has no clock, stage.rs:4-8). */
 int gr_fa2_tick_timed(gr_fa2 *h, uint32_t ticks, size_t l2_flush_bytes, float *ms_out, uint32_t *done);
 
+/* Repulsion walk schedule: 0 = warp-cooperative (a warp visits the union of its 32
+ * nodes' paths, one broadcast load per cell), 1 = per lane (each lane its own
+ * path, gathered loads; the default). Both give bit-identical forces.
+ * gr_fa2_tune times sample_ticks ticks with each from the current state (restored
+ * afterwards) and keeps the faster; walk_ms_each (nullable, 2 floats) gets the
+ * mean walk time of each. */
+int gr_fa2_set_walk_schedule(gr_fa2 *h, int schedule);
+int gr_fa2_tune(gr_fa2 *h, uint32_t sample_ticks, int *chosen, float *walk_ms_each);
+
 /* Current positions to a host buffer (n x dim), refusing non-finite ones as
  * `settle` does (crates/graph-core/src/layout/forceatlas2.rs:82-91). */
 int gr_fa2_positions(gr_fa2 *h, float *out);
@@ -174,7 +183,7 @@ int gr_fa2_set_stream(gr_fa2 *h, void *cuda_stream);
  * repulsion - gravity at the given positions; the same tree build and walk) but
  * takes every input and output as device memory and keeps its scratch in a
  * fixed array compiled into this library, sized for GR_FORCES_STATIC_MAX_N
- * nodes (about 11.5 MB, held on every GPU that loads the library until the
+ * nodes (about 14 MB, held on every GPU that loads the library until the
  * process exits). It calls no cudaMalloc, cudaFree or other allocating routine.
  *
  *   nodes    device, n x float4 {x, y, z (0 in 2D), mass}; FA2's mass is degree + 1

@@ -134,3 +134,19 @@ def test_trajectory_tracks_the_oracle_for_a_few_ticks():
     r = st.positions()
     ext = (r.max(0) - r.min(0)).max()
     assert np.abs(g - r).max() / ext < 1e-4
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_walk_schedules_give_bit_identical_forces_and_tuning_keeps_the_state(dim):
+    wl = synth.powerlaw_1m(n=200_000, dim=dim)
+    outs = []
+    with Fa2(wl.n, wl.src, wl.dst, params=wl.params, pos0=wl.pos0) as eng:
+        eng.tick(3)
+        pos = eng.positions()
+        for sch in (0, 1):
+            eng.set_walk_schedule(sch)
+            outs.append((eng.forces(), eng.info()["far_count"]))
+        chosen, ms = eng.tune(2)
+        assert chosen in (0, 1) and ms[0] > 0 and ms[1] > 0
+        assert np.array_equal(eng.positions(), pos)
+    assert np.array_equal(outs[0][0], outs[1][0])
