@@ -56,6 +56,16 @@ def parse():
     return ap.parse_args()
 
 
+def walk_traffic_per_node():
+    """DRAM bytes per node of one walk launch, from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "k_walk_traffic.txt")
+    try:
+        kv = dict(line.strip().split("=", 1) for line in open(path) if "=" in line and not line.startswith("#"))
+        return float(kv["dram_read_bytes_per_node"]) + float(kv["dram_write_bytes_per_node"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 def workload(name: str, n: int = 0):
     from graph_render_b200 import synth
 
@@ -414,7 +424,9 @@ def run_gpu(args, dist: Dist):
             "gpu_launches": int(info1["graph_kernels"]) * done,
             "roofline": {"kernel": "k_walk_s", "bound": "fp32", "achieved": achieved / 1e12,
                          "peak": fp32_peak / 1e12, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                         "traffic": None,
+                         "traffic": (walk_traffic_per_node() * wl.n if walk_traffic_per_node() and dim == 2
+                                     else None),
+                         "traffic_source": "ncu dram__bytes_read+write of k_walk_s at 2M nodes, scaled by nodes",
                          "peak_source": "nominal FP32 FMA rate, 148 SM x 128 lanes x 2 x sm_max_mhz "
                                         "(MEASURED_PEAKS.json has no non-tensor FP32 figure)",
                          "interactions_per_tick": {"far": far, "pair": pair},

@@ -138,6 +138,8 @@ struct gr_fa2 {
 
     // per-tick buffers
     uint64_t *keys = nullptr, *ukey = nullptr;
+    uint32_t *too_long = nullptr;  // count of runs of equal high key words longer than 64
+    uint2 *long_runs = nullptr;    // those runs (start, length)
     uint32_t *vals = nullptr, *sorig = nullptr, *flag = nullptr, *excl = nullptr, *uid = nullptr;
     uint32_t *leaf_start = nullptr, *cells_at = nullptr, *P = nullptr, *leaf_pre = nullptr;
     float4 *sp = nullptr;
@@ -203,6 +205,8 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
     cudaError_t e;
 #define A(p, c) if ((e = h->alloc(&(p), (c)))) return e
     A(h->keys, n);
+    A(h->too_long, 1);
+    A(h->long_runs, (size_t)n / 64 + 2);
     A(h->vals, n);
     A(h->ukey, n);
     A(h->sorig, n);
@@ -242,6 +246,36 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
 
 enum Phase { PH_TREE = 1, PH_WALK = 2, PH_FINISH = 4, PH_ALL = 7 };
 
+// Runs of equal high key words longer than the in-place fix-up takes: one CTA
+// each, a stable block radix sort of the run in place (scratch: the sorter's
+// ping-pong buffers at the run's own offsets, free after an even pass count).
+__global__ void __launch_bounds__(256) k_fix_long_runs(uint64_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                                                       uint64_t *__restrict__ kalt, uint32_t *__restrict__ valt,
+                                                       const uint32_t *long_count, const uint2 *__restrict__ runs,
+                                                       const uint32_t *skip) {
+    if (skip && *skip) return;
+    __shared__ uint32_t s_cnt[8][256];
+    __shared__ uint32_t s_tot[256];
+    const uint32_t count = *long_count;
+    for (uint32_t q = blockIdx.x; q < count; q += gridDim.x) {
+        const uint2 r = runs[q];
+        block_sort<256>(keys + r.x, vals + r.x, kalt + r.x, valt + r.x, r.y, s_cnt, s_tot);
+    }
+}
+
+// Sort on the high 32 key bits (4 passes, stable), then put every run of equal
+// high words in full-key order: runs of up to 64 in place by one thread, longer
+// ones by one CTA each. The order is exactly the full stable 64-bit sort's.
+static void sort_fast(gr_fa2 *h, cudaStream_t s) {
+    const uint32_t n = h->n;
+    const uint32_t *conv = &h->st->converged;
+    cudaMemsetAsync(h->too_long, 0, 4, s);
+    h->sorter.sort_digits(h->keys, h->vals, n, 4, 4, s, conv);
+    rs_fix_runs<<<div_up(n, 256), 256, 0, s>>>(h->keys, h->vals, n, 64, h->too_long, h->long_runs, conv);
+    k_fix_long_runs<<<148, 256, 0, s>>>(h->keys, h->vals, h->sorter.k_alt, h->sorter.v_alt, h->too_long,
+                                        h->long_runs, conv);
+}
+
 template <int D>
 static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
     const uint32_t n = h->n;
@@ -252,7 +286,10 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
     if (phases & PH_TREE) {
         k_bounds<D><<<h->bnd_blocks(), BND_THREADS, 0, s>>>(h->pos, n, st, h->part);
         k_keys<D><<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals);
-        h->sorter.sort(h->keys, h->vals, n, 64, s, conv);
+        if (h->long_runs)
+            sort_fast(h, s);
+        else
+            h->sorter.sort(h->keys, h->vals, n, 64, s, conv);
         k_gather<<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals, h->sp, h->sorig, h->flag);
         h->scanner.scan(h->flag, h->excl, n, nullptr, 0, &st->n_unique, nullptr, s, conv);
         k_leaves<<<gn, 256, 0, s>>>(n, st, h->keys, h->flag, h->excl, h->leaf_start, h->ukey, h->uid);

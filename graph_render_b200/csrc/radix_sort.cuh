@@ -141,6 +141,46 @@ rs_downsweep(const uint64_t *__restrict__ kin, const V *__restrict__ vin, uint64
     }
 }
 
+__global__ void rs_zero(uint32_t *__restrict__ totals) { totals[blockIdx.x * RS_BINS + threadIdx.x] = 0; }
+
+// After a stable sort on the high 32 key bits: every run of equal high words
+// is put in full-key order by a stable insertion sort in place, which makes the
+// result identical to a stable sort of the whole key. A run longer than
+// max_run is left alone and raises *too_long instead.
+__global__ void rs_fix_runs(uint64_t *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t n, uint32_t max_run,
+                            uint32_t *long_count, uint2 *__restrict__ long_runs, const uint32_t *skip) {
+    if (skip && *skip) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i + 1 >= n) return;
+    const uint32_t hi = (uint32_t)(keys[i] >> 32);
+    if ((uint32_t)(keys[i + 1] >> 32) != hi) return;  // not a run of two or more
+    if (i > 0 && (uint32_t)(keys[i - 1] >> 32) == hi) return;  // not the run's first element
+    uint32_t len = 2;
+    while (i + len < n && (uint32_t)(keys[i + len] >> 32) == hi) len++;
+    if (len > max_run) {  // one CTA sorts it (rs_fix_long_runs)
+        const uint32_t q = atomicAdd(long_count, 1u);
+        long_runs[q] = make_uint2(i, len);
+        return;
+    }
+    for (uint32_t a = i + 1; a < i + len; a++) {
+        const uint64_t k = keys[a];
+        const uint32_t v = vals[a];
+        uint32_t b = a;
+        while (b > i && keys[b - 1] > k) {  // strictly greater: equal keys keep their order
+            keys[b] = keys[b - 1];
+            vals[b] = vals[b - 1];
+            b--;
+        }
+        keys[b] = k;
+        vals[b] = v;
+    }
+}
+
+// The pieces the fix-up of long runs needs: the block-level stable sort.
+template <int BT>
+__device__ void block_sort(uint64_t *keys, uint32_t *vals, uint64_t *kalt, uint32_t *valt, uint32_t n,
+                           uint32_t (*s_cnt)[256], uint32_t *s_tot);
+
 // Device buffers for sorting up to `cap` pairs. keys/vals are sorted in place
 // (the scratch pair is the ping-pong partner; an even pass count ends in the
 // caller's buffers).
@@ -179,15 +219,22 @@ struct RadixSorter {
     // their values, in place. Kernel launches only: graph-capturable.
     void sort(uint64_t *keys, uint32_t *vals, uint32_t n, int bits, cudaStream_t s,
               const uint32_t *skip = nullptr) {
-        if (n == 0) return;
-        uint32_t nt = div_up(n, RS_TILE);
         int passes = (bits + 7) / 8;
         passes += passes & 1;  // even, so the result lands back in keys/vals
-        cudaMemsetAsync(totals, 0, (size_t)8 * RS_BINS * sizeof(uint32_t), s);
+        sort_digits(keys, vals, n, 0, passes, s, skip);
+    }
+
+    // The passes for digits first_digit .. first_digit + passes - 1 (an even
+    // count, so the result lands back in keys/vals).
+    void sort_digits(uint64_t *keys, uint32_t *vals, uint32_t n, int first_digit, int passes, cudaStream_t s,
+                     const uint32_t *skip = nullptr) {
+        if (n == 0) return;
+        uint32_t nt = div_up(n, RS_TILE);
+        rs_zero<<<8, RS_BINS, 0, s>>>(totals);  // a kernel, so the sort also fits graph bodies that take kernels only
         uint64_t *ka = keys, *kb = k_alt;
         uint32_t *va = vals, *vb = v_alt;
         for (int p = 0; p < passes; p++) {
-            int shift = 8 * p;
+            int shift = 8 * (first_digit + p);
             uint32_t *tot = totals + (size_t)p * RS_BINS;
             rs_upsweep<<<nt, RS_THREADS, 0, s>>>(ka, n, shift, hist, tot, nt, skip);
             rs_scan<<<RS_BINS, RS_THREADS, 0, s>>>(hist, tot, nt, skip);

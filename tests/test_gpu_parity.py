@@ -150,3 +150,45 @@ def test_walk_schedules_give_bit_identical_forces_and_tuning_keeps_the_state(dim
         assert chosen in (0, 1) and ms[0] > 0 and ms[1] > 0
         assert np.array_equal(eng.positions(), pos)
     assert np.array_equal(outs[0][0], outs[1][0])
+
+
+def _full_sort_forces(n, src, dst, pos, prm):
+    """Forces through gr_fa2_forces_static, which sorts the whole 64-bit key
+    (8 passes) where a handle sorts the high word and fixes the runs."""
+    import ctypes as C
+
+    import torch
+
+    from graph_render_b200 import _native as N, params_bytes
+    from tests.test_zz_no_alloc import csr
+
+    rp, col, wts, mass = csr(n, src, dst, None)
+    nodes = np.zeros((n, 4), np.float32)
+    nodes[:, :2] = pos
+    nodes[:, 3] = mass
+    dev = torch.device("cuda", 0)
+    t = [torch.from_numpy(a).to(dev) for a in (nodes, rp, col, np.ones(len(col), np.float32))]
+    out = torch.zeros((n, 2), dtype=torch.float32, device=dev)
+    pb = params_bytes(prm)
+    N.check(N.lib().gr_fa2_forces_static(n, *[C.c_void_p(x.data_ptr()) for x in t], C.c_char_p(pb), len(pb), 0,
+                                         C.c_void_p(out.data_ptr()),
+                                         C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
+    torch.cuda.synchronize(dev)
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize("cluster", [0, 300])
+def test_high_word_sort_with_run_fixup_equals_the_full_sort(cluster):
+    """A handle sorts the keys' high 32 bits and then orders each run of equal
+    high words in place (runs > 64, here a cluster of 300 coincident nodes, by
+    one CTA each); the result must be the full 64-bit sort's, so forces on a
+    graph whose rows all take the same attraction path are bit-identical."""
+    wl = synth.sbm_1500()
+    pos = wl.pos0.copy()
+    if cluster:
+        pos[:cluster] = pos[0]
+    prm = dict(wl.params)
+    with Fa2(wl.n, wl.src, wl.dst, params=prm, pos0=pos) as eng:
+        fast = eng.forces()
+    full = _full_sort_forces(wl.n, wl.src, wl.dst, pos, prm)
+    assert np.array_equal(fast, full)
