@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--e2e-ticks", type=int, default=100)
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-3d", action="store_true")
     ap.add_argument("--batched-graphs", type=int, default=4096, help="graphs per GPU")
     ap.add_argument("--batched-ticks", type=int, default=200)
     ap.add_argument("--batched-sample", type=int, default=48, help="graphs timed one launch sequence each")
@@ -315,6 +317,59 @@ def run_batched(args, dist: Dist):
     }
 
 
+# ---------------------------------------------------------- adjoint arm --
+
+def run_adjoint(args, dist: Dist):
+    """The differentiated workload: SBM 50,000 nodes in 16 blocks, edge weights 1,
+    200 ticks with positions checkpointed every 20, loss = sampled stress-1
+    against hop distance over ~1M node pairs; gradients for start positions
+    and edge weights through the adjoint ticks."""
+    import torch
+
+    from graph_render_b200 import Fa2, stress, synth
+
+    wl = synth.sbm_50k()
+    t0 = time.perf_counter()
+    a, b, h = stress.sample_pairs(wl.n, wl.src, wl.dst, 1_000_000, 5)
+    pairs_s = time.perf_counter() - t0
+    with Fa2(wl.n, wl.src, wl.dst, wl.weight, params=wl.params, pos0=wl.pos0) as eng:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.adjoint_forward(200, 20)
+        torch.cuda.synchronize()
+        fwd = time.perf_counter() - t0
+        pT = eng.positions()
+        L, g = stress.stress(pT, a, b, h)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gp, gw = eng.adjoint_backward(g)
+        torch.cuda.synchronize()
+        bwd = time.perf_counter() - t0
+    return {"workload": "sbm50000-16blocks-2d", "ticks": 200, "checkpoint_every": 20, "pairs": int(len(a)),
+            "stress": L, "forward_ms": 1e3 * fwd, "backward_ms": 1e3 * bwd,
+            "backward_node_ticks_per_s": wl.n * 200 / bwd, "pair_sampling_s": pairs_s,
+            "grad_pos_norm": float(np.linalg.norm(gp)), "grad_w_norm": float(np.linalg.norm(gw)),
+            "finite": bool(np.isfinite(gp).all() and np.isfinite(gw).all())}
+
+
+def run_3d(args, dist: Dist):
+    """The 1M-node configuration-model graph in 3D (octree), strong gravity, theta 1.2."""
+    from graph_render_b200 import Fa2
+
+    wl = workload("powerlaw-3d", 0)
+    with Fa2(wl.n, wl.src, wl.dst, wl.weight, params=wl.params, pos0=wl.pos0) as eng:
+        eng.tick(1)
+        eng.tune(2)
+        eng.tick(3)
+        ms = eng.tick_timed(10, l2_flush_bytes=FLUSH_BYTES)
+        inf = eng.info()
+    t = float(ms[:, 3].sum())
+    return {"workload": wl.name, "n": wl.n, "node_ticks_per_s": wl.n * len(ms) / (t / 1e3),
+            "ms_per_tick": t / len(ms), "phase_ms": {"tree": float(ms[:, 0].mean()), "walk": float(ms[:, 1].mean()),
+                                                    "finish": float(ms[:, 2].mean())},
+            "n_cells": inf["n_cells"]}
+
+
 # --------------------------------------------------------------- GPU arm --
 
 def run_gpu(args, dist: Dist):
@@ -395,6 +450,12 @@ def run_gpu(args, dist: Dist):
     batched = None
     if not args.no_batched:
         batched = run_batched(args, dist)
+    adjoint = None
+    if not args.no_adjoint and dist.rank == 0:
+        adjoint = run_adjoint(args, dist)
+    three_d = None
+    if not args.no_3d and dist.rank == 0:
+        three_d = run_3d(args, dist)
 
     if dist.rank == 0:
         line = {
@@ -433,6 +494,8 @@ def run_gpu(args, dist: Dist):
                          "flops_per_interaction": FLOPS_PER_INTERACTION[dim]},
             "cpu_baseline": cpu,
             "batched": batched,
+            "adjoint": adjoint,
+            "powerlaw_1m_3d": three_d,
             "vs_baseline_basis": "reference's own 1M-node FA2-BH run, 1 thread, other host "
                                  "(perf-fa2bh.md:60-63; theta 0.8, its gate-model graph)",
         }

@@ -23,6 +23,9 @@ struct AdjScalars {
     double Lsw_cur, Ltr_cur;    // this tick's adjoints of sw, tr
     double vsum[3];             // sum of the gravity VJP terms
     uint32_t counters[4];
+    uint32_t absmax;            // bit pattern of max |lam'| (a non-negative float orders as its bits)
+    int shift;                  // this tick's rescale exponent
+    long long exponent;         // lam' and the accumulated dL/dc are the true values times 2^-exponent
 };
 
 // estimate_factor's partial derivatives on its active branch: d[0..3] =
@@ -394,6 +397,45 @@ k_adj_final(uint32_t n, int lin_log, int dissuade, const AdjScalars *A, const fl
         lam_out[k] = (float)((double)lam[k] + ((double)v[k] - A->vsum[a] / (double)n) + (double)lam_rep[k] +
                              (double)lam_com[k] + acc[a]);
     }
+}
+
+// The adjoint of a run grows by orders of magnitude per tick (FA2's speed
+// controller and repulsion make the map expansive: the FP64 oracle's
+// dL/dp0 on a 2,000-node SBM has norm ~1e5 after 5 ticks and ~1e37 after
+// 200), beyond FP32. Between ticks the carried adjoints (lam', the controller
+// adjoints and the accumulated dL/dc) are multiplied by 2^-k so that max |lam'|
+// lies in [0.5, 1). The VJP is linear in what it carries and a power-of-two
+// scale is exact, so this changes no value's significand; the host multiplies
+// the results by 2^exponent at the end.
+__global__ void k_adj_absmax(uint32_t count, const float *__restrict__ lam, AdjScalars *A) {
+    float m = 0.f;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(lam[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(&A->absmax, __float_as_uint(m));
+}
+
+__global__ void k_adj_shift(AdjScalars *A) {
+    const float m = __uint_as_float(A->absmax);
+    int k = 0;
+    if (m > 0.f && isfinite(m)) frexpf(m, &k);  // m = f 2^k, f in [0.5, 1)
+    A->shift = k;
+    A->exponent += k;
+    A->absmax = 0u;
+    A->LSW = ldexp(A->LSW, -k);
+    A->LTR = ldexp(A->LTR, -k);
+    A->Lsp = ldexp(A->Lsp, -k);
+    A->Lse = ldexp(A->Lse, -k);
+}
+
+__global__ void k_adj_rescale(uint32_t count, float *__restrict__ lam, uint64_t ne, double *__restrict__ gce,
+                              const AdjScalars *A) {
+    const int k = A->shift;
+    if (k == 0) return;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride)
+        lam[i] = ldexpf(lam[i], -k);
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += stride) gce[e] = ldexp(gce[e], -k);
 }
 
 // dL/dc per simple edge (its two CSR entries), times dc/dw, onto the raw edge

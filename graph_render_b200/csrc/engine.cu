@@ -296,9 +296,9 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
         k_karras<<<gn, 256, 0, s>>>(st, h->ukey, h->bt);
         k_leaf_body<D><<<gn, 256, 0, s>>>(st, h->sp, h->leaf_start, h->leaf_body, h->leaf_coinc);
         const uint32_t ab = div_up(n, AG_TILE);
-        k_dd_reduce<<<ab, AG_T, 0, s>>>(st, h->leaf_body, h->dd_bsum);
-        k_dd_blocks<<<1, AG_T, 0, s>>>(st, h->dd_bsum, h->dd_prefix);
-        k_dd_down<<<ab, AG_T, 0, s>>>(st, h->leaf_body, h->dd_bsum, h->dd_prefix);
+        k_dd_reduce<D><<<ab, AG_T, 0, s>>>(st, h->leaf_body, h->dd_bsum);
+        k_dd_blocks<D><<<1, AG_T, 0, s>>>(st, h->dd_bsum, h->dd_prefix);
+        k_dd_down<D><<<ab, AG_T, 0, s>>>(st, h->leaf_body, h->dd_bsum, h->dd_prefix);
         k_node_body<<<gn, 256, 0, s>>>(st, h->bt, h->dd_prefix, h->int_body);
         k_count<D><<<gn, 256, 0, s>>>(st, h->bt, h->cells_at);
         h->scanner.scan(h->cells_at, h->P, n, &st->n_unique, 0, &st->n_cells, nullptr, s, conv);
@@ -1495,6 +1495,11 @@ static void adjoint_tick(gr_fa2 *h, Adjoint *a, const DevState *before) {
     const uint32_t n = h->n;
     cudaStream_t s = h->stream;
     DevState *st = h->st;
+    // bring max |lam'| into [0.5, 1) by a power of two (k_adj_shift)
+    const uint32_t rb = std::min<uint32_t>(div_up((uint64_t)n * D, 256), 4 * 148);
+    k_adj_absmax<<<rb, 256, 0, s>>>(n * D, a->lam1, a->A);
+    k_adj_shift<<<1, 1, 0, s>>>(a->A);
+    k_adj_rescale<<<rb, 256, 0, s>>>(n * D, a->lam1, 2 * h->m, a->gce, a->A);
     // forward recompute up to the forces, with the controller update (no move)
     enqueue_tick<D>(h, false, PH_TREE | PH_WALK);
     ForceParams fp;
@@ -1591,7 +1596,7 @@ int gr_fa2_adjoint_forward(gr_fa2 *h, uint32_t ticks, uint32_t every) {
     return ok();
 }
 
-int gr_fa2_adjoint_backward(gr_fa2 *h, const float *dL_dpT, float *dL_dp0, double *dL_dw) {
+int gr_fa2_adjoint_backward(gr_fa2 *h, const float *dL_dpT, double *dL_dp0, double *dL_dw) {
     if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
     Adjoint *a = h->adj;
     if (!a) return set_err(GR_INVALID_ARGUMENT, "no recorded run: call gr_fa2_adjoint_forward first");
@@ -1626,7 +1631,10 @@ int gr_fa2_adjoint_backward(gr_fa2 *h, const float *dL_dpT, float *dL_dp0, doubl
         }
     }
     CU(cudaGetLastError());
-    CU(cudaMemcpyAsync(dL_dp0, a->lam1, (size_t)n * D * 4, cudaMemcpyDeviceToHost, s));
+    std::vector<float> lam0((size_t)n * D);
+    AdjScalars Ah;
+    if (n) CU(cudaMemcpyAsync(lam0.data(), a->lam1, (size_t)n * D * 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(&Ah, a->A, sizeof(AdjScalars), cudaMemcpyDeviceToHost, s));
     if (dL_dw && h->m_raw) {
         CU(cudaMemsetAsync(a->gs, 0, std::max<uint64_t>(h->m, 1) * sizeof(double), s));
         CU(cudaMemsetAsync(a->graw, 0, h->m_raw * sizeof(double), s));
@@ -1640,8 +1648,17 @@ int gr_fa2_adjoint_backward(gr_fa2 *h, const float *dL_dpT, float *dL_dp0, doubl
     CU(cudaMemcpyAsync(h->pos, a->final_pos, (size_t)std::max(n, 1u) * sizeof(float4), cudaMemcpyDeviceToDevice, s));
     CU(cudaMemcpyAsync(h->st, a->final_st, sizeof(DevState), cudaMemcpyDeviceToDevice, s));
     CU(cudaStreamSynchronize(s));
-    for (size_t i = 0; i < (size_t)n * D; i++)
+    // undo the running power-of-two scale (k_adj_shift); beyond FP64's range is non-finite
+    const int ex = (int)std::max<long long>(-4096, std::min<long long>(4096, Ah.exponent));
+    for (size_t i = 0; i < (size_t)n * D; i++) {
+        dL_dp0[i] = std::ldexp((double)lam0[i], ex);
         if (!std::isfinite(dL_dp0[i])) return set_err(GR_LAYOUT_FAILED, "non-finite gradient");
+    }
+    if (dL_dw)
+        for (uint64_t e = 0; e < h->m_raw; e++) {
+            dL_dw[e] = std::ldexp(dL_dw[e], ex);
+            if (!std::isfinite(dL_dw[e])) return set_err(GR_LAYOUT_FAILED, "non-finite gradient");
+        }
     return ok();
 }
 

@@ -390,8 +390,10 @@ struct BodyDD {
     DD m, c0, c1, c2;
 };
 
+template <int D>
 __device__ __forceinline__ BodyDD bdd_add(const BodyDD &a, const BodyDD &b) {
-    return BodyDD{dd_add(a.m, b.m), dd_add(a.c0, b.c0), dd_add(a.c1, b.c1), dd_add(a.c2, b.c2)};
+    return BodyDD{dd_add(a.m, b.m), dd_add(a.c0, b.c0), dd_add(a.c1, b.c1),
+                  D == 3 ? dd_add(a.c2, b.c2) : DD{0.0, 0.0}};
 }
 
 __device__ __forceinline__ BodyDD bdd_of(const Body &b) {
@@ -430,49 +432,55 @@ __device__ __forceinline__ DD dd_shfl_up(DD v, int o) {
 }
 
 // Inclusive warp scan of BodyDD, a fixed Hillis-Steele shape.
+template <int D>
 __device__ __forceinline__ BodyDD warp_scan_bdd(BodyDD v) {
     const int lane = threadIdx.x % GR_WARP;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const BodyDD u{dd_shfl_up(v.m, o), dd_shfl_up(v.c0, o), dd_shfl_up(v.c1, o), dd_shfl_up(v.c2, o)};
-        if (lane >= o) v = bdd_add(u, v);
+        const BodyDD u{dd_shfl_up(v.m, o), dd_shfl_up(v.c0, o), dd_shfl_up(v.c1, o),
+                       D == 3 ? dd_shfl_up(v.c2, o) : DD{0.0, 0.0}};
+        if (lane >= o) v = bdd_add<D>(u, v);
     }
     return v;
 }
 
 // Exclusive block scan (AG_T threads) of one BodyDD per thread, offset by
 // `carry`; returns this thread's exclusive prefix and the block total.
+template <int D>
 __device__ __forceinline__ BodyDD block_scan_bdd(const BodyDD &x, const BodyDD &carry, BodyDD &total,
                                                  BodyDD *s_w) {
     const int lane = threadIdx.x % GR_WARP, w = threadIdx.x / GR_WARP;
-    const BodyDD inc = warp_scan_bdd(x);
+    const BodyDD inc = warp_scan_bdd<D>(x);
     if (lane == 31) s_w[w] = inc;
     __syncthreads();
     if (w == 0) {  // scan the warp totals (one per lane < AG_W)
         BodyDD t = lane < AG_W ? s_w[lane] : BodyDD{};
-        t = warp_scan_bdd(t);
+        t = warp_scan_bdd<D>(t);
         if (lane < AG_W) s_w[AG_W + lane] = t;
     }
     __syncthreads();
     const BodyDD before = w > 0 ? s_w[AG_W + w - 1] : BodyDD{};
-    total = bdd_add(carry, s_w[AG_W + AG_W - 1]);
+    total = bdd_add<D>(carry, s_w[AG_W + AG_W - 1]);
     // exclusive prefix: carry + warps before + lanes before (inc - x recomputed as a shifted scan)
-    BodyDD lanes_before{dd_shfl_up(inc.m, 1), dd_shfl_up(inc.c0, 1), dd_shfl_up(inc.c1, 1), dd_shfl_up(inc.c2, 1)};
+    BodyDD lanes_before{dd_shfl_up(inc.m, 1), dd_shfl_up(inc.c0, 1), dd_shfl_up(inc.c1, 1),
+                        D == 3 ? dd_shfl_up(inc.c2, 1) : DD{0.0, 0.0}};
     if (lane == 0) lanes_before = BodyDD{};
     __syncthreads();
-    return bdd_add(bdd_add(carry, before), lanes_before);
+    return bdd_add<D>(bdd_add<D>(carry, before), lanes_before);
 }
 
 // Sequential double-double sum of this thread's AG_I leaves.
+template <int D>
 __device__ __forceinline__ BodyDD thread_chunk(const Body *__restrict__ lb, uint32_t base, uint32_t nu) {
     BodyDD acc{};
     for (int r = 0; r < AG_I; r++) {
         const uint32_t s = base + r;
-        if (s < nu) acc = bdd_add(acc, bdd_of(lb[s]));
+        if (s < nu) acc = bdd_add<D>(acc, bdd_of(lb[s]));
     }
     return acc;
 }
 
+template <int D>
 __global__ void __launch_bounds__(AG_T) k_dd_reduce(const DevState *st, const Body *__restrict__ lb,
                                                     BodyDD *__restrict__ bsum) {
     if (st->converged) return;
@@ -481,12 +489,13 @@ __global__ void __launch_bounds__(AG_T) k_dd_reduce(const DevState *st, const Bo
     const uint32_t base = blockIdx.x * AG_TILE;
     if (base >= nu) return;
     BodyDD total;
-    block_scan_bdd(thread_chunk(lb, base + threadIdx.x * AG_I, nu), BodyDD{}, total, s_w);
+    block_scan_bdd<D>(thread_chunk<D>(lb, base + threadIdx.x * AG_I, nu), BodyDD{}, total, s_w);
     if (threadIdx.x == 0) bsum[blockIdx.x] = total;
 }
 
 // One block: exclusive prefix of the block sums in block order (in place); the
 // total is the prefix at nu.
+template <int D>
 __global__ void __launch_bounds__(AG_T) k_dd_blocks(const DevState *st, BodyDD *__restrict__ bsum,
                                                     BodyDD *__restrict__ prefix) {
     if (st->converged) return;
@@ -498,13 +507,14 @@ __global__ void __launch_bounds__(AG_T) k_dd_blocks(const DevState *st, BodyDD *
         const uint32_t b = off + threadIdx.x;
         const BodyDD x = b < nb ? bsum[b] : BodyDD{};
         BodyDD total;
-        const BodyDD ex = block_scan_bdd(x, carry, total, s_w);
+        const BodyDD ex = block_scan_bdd<D>(x, carry, total, s_w);
         if (b < nb) bsum[b] = ex;
         carry = total;
     }
     if (threadIdx.x == 0) prefix[nu] = carry;
 }
 
+template <int D>
 __global__ void __launch_bounds__(AG_T) k_dd_down(const DevState *st, const Body *__restrict__ lb,
                                                   const BodyDD *__restrict__ bsum, BodyDD *__restrict__ prefix) {
     if (st->converged) return;
@@ -514,12 +524,12 @@ __global__ void __launch_bounds__(AG_T) k_dd_down(const DevState *st, const Body
     if (base >= nu) return;
     const uint32_t mine = base + threadIdx.x * AG_I;
     BodyDD total;
-    BodyDD run = block_scan_bdd(thread_chunk(lb, mine, nu), bsum[blockIdx.x], total, s_w);
+    BodyDD run = block_scan_bdd<D>(thread_chunk<D>(lb, mine, nu), bsum[blockIdx.x], total, s_w);
     for (int r = 0; r < AG_I; r++) {
         const uint32_t s = mine + r;
         if (s >= nu) break;
         prefix[s] = run;
-        run = bdd_add(run, bdd_of(lb[s]));
+        run = bdd_add<D>(run, bdd_of(lb[s]));
     }
 }
 

@@ -56,7 +56,7 @@ __device__ __forceinline__ void walk_group(const WalkView &V, uint32_t p, float 
     uint32_t resume = valid ? 0u : 0xffffffffu;
     f0 = f1 = f2 = 0.f;
     nfar = npair = 0;
-    const float kr = V.kr, th2 = V.th2;
+    const float th2 = V.th2, mk = me.w * V.kr;
     const uint32_t lane = threadIdx.x % GR_WARP;
 
     uint32_t k = 0;
@@ -92,7 +92,7 @@ __device__ __forceinline__ void walk_group(const WalkView &V, uint32_t p, float 
         const float d2 = (D == 3) ? dx * dx + dy * dy + dz * dz : dx * dx + dy * dy;
         const bool far = active && !holds && d2 > 0.f && w2 < th2 * d2;
         if (far) {
-            const float f = __fdividef(me.w * cm, d2) * kr;
+            const float f = __fdividef(mk * cm, d2);
             f0 += dx * f;
             f1 += dy * f;
             if (D == 3) f2 += dz * f;
@@ -114,7 +114,7 @@ __device__ __forceinline__ void walk_group(const WalkView &V, uint32_t p, float 
                     if (D == 3) ez = sg * (float)jiggle(V.seed, iter, 2, oi, oj);
                     e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
                 }
-                const float f = __fdividef(me.w * cm, e2) * kr;
+                const float f = __fdividef(mk * cm, e2);
                 f0 += ex * f;
                 f1 += ey * f;
                 if (D == 3) f2 += ez * f;
@@ -142,7 +142,7 @@ __device__ __forceinline__ void walk_group(const WalkView &V, uint32_t p, float 
                             if (D == 3) ez = sg * (float)jiggle(V.seed, iter, 2, oi, oj);
                         }
                         const float e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
-                        const float f = __fdividef(me.w * o.w, e2) * kr;
+                        const float f = __fdividef(mk * o.w, e2);
                         f0 += ex * f;
                         f1 += ey * f;
                         if (D == 3) f2 += ez * f;
@@ -174,7 +174,7 @@ __device__ __forceinline__ void walk_lane(const WalkView &V, uint32_t p, float &
     const uint32_t oi = valid ? V.sorig[p] : 0u;
     f0 = f1 = f2 = 0.f;
     nfar = npair = 0;
-    const float kr = V.kr, th2 = V.th2;
+    const float th2 = V.th2, mk = me.w * V.kr;
     uint32_t k = valid ? 0u : ncells;
     while (k < ncells) {
         const float4 A = __ldg(&cells.A[k]);
@@ -196,18 +196,15 @@ __device__ __forceinline__ void walk_lane(const WalkView &V, uint32_t p, float &
         }
         const bool leaf = sk < 0;
         uint32_t skip = leaf ? k + 1 : (uint32_t)sk;
-        if (skip <= k || skip > ncells) {  // malformed cell: record it, keep the walk finite
-            atomicOr(V.err, (uint32_t)ERR_TREE);
-            skip = k + 1;
-        }
+        skip = max(skip, k + 1);  // every step moves forward, whatever a cell holds
         const bool holds = (k <= mylp) && (mylp < skip);
         const float dx = (me.x - cx) - lx;
         const float dy = (me.y - cy) - ly;
         const float dz = (D == 3) ? (me.z - cz) - lz : 0.f;
         const float d2 = (D == 3) ? dx * dx + dy * dy + dz * dz : dx * dx + dy * dy;
-        const bool far = !holds && d2 > 0.f && w2 < th2 * d2;
+        const bool far = !holds && w2 < th2 * d2;  // w2 > 0, so this is false at d2 == 0
         if (far || (sk == -1 && !holds && d2 > 0.f)) {  // a body: far cell, or a one-point leaf's pair
-            const float f = __fdividef(me.w * cm, d2) * kr;
+            const float f = __fdividef(mk * cm, d2);
             f0 += dx * f;
             f1 += dy * f;
             if (D == 3) f2 += dz * f;
@@ -223,7 +220,7 @@ __device__ __forceinline__ void walk_lane(const WalkView &V, uint32_t p, float &
             const float ey = sg * (float)jiggle(V.seed, iter, 1, oi, oj);
             const float ez = (D == 3) ? sg * (float)jiggle(V.seed, iter, 2, oi, oj) : 0.f;
             const float e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
-            const float f = __fdividef(me.w * cm, e2) * kr;
+            const float f = __fdividef(mk * cm, e2);
             f0 += ex * f;
             f1 += ey * f;
             if (D == 3) f2 += ez * f;
@@ -248,7 +245,7 @@ __device__ __forceinline__ void walk_lane(const WalkView &V, uint32_t p, float &
                     if (D == 3) ez = sg * (float)jiggle(V.seed, iter, 2, oi, oj);
                 }
                 const float e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
-                const float f = __fdividef(me.w * o.w, e2) * kr;
+                const float f = __fdividef(mk * o.w, e2);
                 f0 += ex * f;
                 f1 += ey * f;
                 if (D == 3) f2 += ez * f;

@@ -120,7 +120,7 @@ class Fa2:
         """(dL/d start positions (n x dim), dL/d raw edge weight (m)) for
         dL_dpT = dL/d final positions of the recorded run."""
         g = np.ascontiguousarray(dL_dpT, np.float32).reshape(self.n, self.dim)
-        dp0 = np.zeros((self.n, self.dim), np.float32)
+        dp0 = np.zeros((self.n, self.dim), np.float64)
         dw = np.zeros(max(self.m_raw, 1), np.float64)
         N.check(self._L.gr_fa2_adjoint_backward(self.h, _ptr(g), _ptr(dp0), _ptr(dw)))
         return dp0, dw[:self.m_raw]

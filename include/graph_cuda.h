@@ -165,11 +165,14 @@ int gr_fa2_set_controller(gr_fa2 *h, const gr_fa2_controller *in);
  * gr_fa2_adjoint_forward runs `ticks` ticks from the current state, recording
  * positions and controller every `checkpoint_every` ticks; gr_fa2_adjoint_backward
  * takes dL/d(final positions) (host, n x dim) and returns dL/d(start positions)
- * (host, n x dim) and, when dL_dw is not NULL, dL/d(raw edge weight) (host, m; 0
- * for a self-loop or a repeated pair), replaying each segment from its checkpoint.
+ * (host, n x dim, FP64) and, when dL_dw is not NULL, dL/d(raw edge weight) (host,
+ * m; 0 for a self-loop or a repeated pair), replaying each segment from its
+ * checkpoint. The carried adjoint is FP32 under a running power-of-two scale, so
+ * gradients that outgrow FP32 over a long run (they grow by orders of magnitude
+ * per tick) come back in FP64; GR_LAYOUT_FAILED if they outgrow FP64.
  * The handle is left at the end of the recorded run. */
 int gr_fa2_adjoint_forward(gr_fa2 *h, uint32_t ticks, uint32_t checkpoint_every);
-int gr_fa2_adjoint_backward(gr_fa2 *h, const float *dL_dpT, float *dL_dp0, double *dL_dw);
+int gr_fa2_adjoint_backward(gr_fa2 *h, const float *dL_dpT, double *dL_dp0, double *dL_dw);
 
 /* The stream every call of this handle enqueues on (default: the handle's own). */
 int gr_fa2_set_stream(gr_fa2 *h, void *cuda_stream);

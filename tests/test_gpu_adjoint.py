@@ -145,3 +145,21 @@ def test_3d_adjoint_matches_the_oracle():
     st = oracle_state(wl.n, wl.src, wl.dst, None, wl.pos0, prm, dense=True)
     op, _ = O.adjoint(st, 3, R)
     assert rel(gp, op) < TOL
+
+
+def test_long_run_adjoint_outgrows_fp32_and_stays_exactly_linear():
+    """200 ticks with checkpoints every 20 (the differentiated workload's
+    schedule) on the 2,000-node instance: the true dL/dp0 grows far beyond
+    FP32 (the FP64 oracle's has norm ~1e37 here), so the engine carries the
+    adjoint under a power-of-two scale. Scaling dL/dpT by 2^-40 must scale
+    both gradients by exactly 2^-40."""
+    wl, w, prm = instance(n=2000, theta=1.2)
+    R = np.random.default_rng(2).normal(size=(wl.n, 2)).astype(np.float32)
+    with Fa2(wl.n, wl.src, wl.dst, w, params=prm, pos0=wl.pos0) as eng:
+        eng.adjoint_forward(200, 20)
+        gp, gw = eng.adjoint_backward(R)
+        gp2, gw2 = eng.adjoint_backward(np.ldexp(R, -40))
+    assert np.isfinite(gp).all() and np.isfinite(gw).all()
+    assert np.linalg.norm(gp) > 1e10
+    assert np.array_equal(np.ldexp(gp, -40), gp2)
+    assert np.array_equal(np.ldexp(gw, -40), gw2)
