@@ -147,7 +147,7 @@ __device__ void block_sort(uint64_t *keys, uint32_t *vals, uint64_t *kalt, uint3
             const uint32_t i = b + lane;
             const bool ok = i < c1;
             const uint32_t dgt = ok ? (uint32_t)(ka[i] >> shift) & 0xffu : 256u + lane;
-            const uint32_t peers = __match_any_sync(GR_FULL, dgt);
+            const uint32_t peers = warp_digit_peers(dgt, ok);
             if (ok && (peers & lt) == 0) s_cnt[w][dgt] += __popc(peers);
             __syncwarp();
         }
@@ -196,7 +196,7 @@ __device__ void block_sort(uint64_t *keys, uint32_t *vals, uint64_t *kalt, uint3
             const bool ok = i < c1;
             const uint64_t key = ok ? ka[i] : 0ull;
             const uint32_t dgt = ok ? (uint32_t)(key >> shift) & 0xffu : 256u + lane;
-            const uint32_t peers = __match_any_sync(GR_FULL, dgt);
+            const uint32_t peers = warp_digit_peers(dgt, ok);
             const uint32_t base = ok ? s_cnt[w][dgt] : 0u;
             __syncwarp();
             if (ok) {

@@ -50,6 +50,7 @@ enum DevError : uint32_t {
     ERR_NONFINITE = 1u,
     ERR_TREE = 2u,
     ERR_BOUNDS = 4u,
+    ERR_WAIT = 8u,  // a bounded wait on another block gave up
 };
 
 struct Body {  // FP64 cell sums: mass and mass-weighted coordinate sums

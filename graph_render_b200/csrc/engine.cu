@@ -270,7 +270,10 @@ static void sort_fast(gr_fa2 *h, cudaStream_t s) {
     const uint32_t n = h->n;
     const uint32_t *conv = &h->st->converged;
     cudaMemsetAsync(h->too_long, 0, 4, s);
-    h->sorter.sort_digits(h->keys, h->vals, n, 4, 4, s, conv);
+    if (n < (1u << 30))
+        h->sorter.sort_onesweep(h->keys, h->vals, n, 4, 4, s, &h->st->error, conv);
+    else
+        h->sorter.sort_digits(h->keys, h->vals, n, 4, 4, s, conv);
     rs_fix_runs<<<div_up(n, 256), 256, 0, s>>>(h->keys, h->vals, n, 64, h->too_long, h->long_runs, conv);
     k_fix_long_runs<<<148, 256, 0, s>>>(h->keys, h->vals, h->sorter.k_alt, h->sorter.v_alt, h->too_long,
                                         h->long_runs, conv);
