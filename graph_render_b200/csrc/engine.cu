@@ -297,16 +297,17 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
         h->scanner.scan(h->flag, h->excl, n, nullptr, 0, &st->n_unique, nullptr, s, conv);
         k_leaves<<<gn, 256, 0, s>>>(n, st, h->keys, h->flag, h->excl, h->leaf_start, h->ukey, h->uid);
         k_karras<<<gn, 256, 0, s>>>(st, h->ukey, h->bt);
-        k_leaf_body<D><<<gn, 256, 0, s>>>(st, h->sp, h->leaf_start, h->leaf_body, h->leaf_coinc);
+        const bool adjoint = h->bt.cell_of != nullptr;  // the adjoint reads leaf and node bodies as arrays
+        if (adjoint) k_leaf_body<D><<<gn, 256, 0, s>>>(st, h->sp, h->leaf_start, h->leaf_body, h->leaf_coinc);
         const uint32_t ab = div_up(n, AG_TILE);
-        k_dd_reduce<D><<<ab, AG_T, 0, s>>>(st, h->leaf_body, h->dd_bsum);
+        k_dd_reduce<D><<<ab, AG_T, 0, s>>>(st, h->sp, h->leaf_start, h->dd_bsum);
         k_dd_blocks<D><<<1, AG_T, 0, s>>>(st, h->dd_bsum, h->dd_prefix);
-        k_dd_down<D><<<ab, AG_T, 0, s>>>(st, h->leaf_body, h->dd_bsum, h->dd_prefix);
-        k_node_body<<<gn, 256, 0, s>>>(st, h->bt, h->dd_prefix, h->int_body);
+        k_dd_down<D><<<ab, AG_T, 0, s>>>(st, h->sp, h->leaf_start, h->dd_bsum, h->dd_prefix, h->leaf_coinc);
+        if (adjoint) k_node_body<<<gn, 256, 0, s>>>(st, h->bt, h->dd_prefix, h->int_body);
         k_count<D><<<gn, 256, 0, s>>>(st, h->bt, h->cells_at);
         h->scanner.scan(h->cells_at, h->P, n, &st->n_unique, 0, &st->n_cells, nullptr, s, conv);
-        k_assign<D><<<gn, 256, 0, s>>>(st, h->bt, h->sp, h->P, h->cells_at, h->leaf_start, h->leaf_body, h->int_body,
-                                       h->leaf_coinc, h->cells, h->leaf_pre, st);
+        k_assign_dd<D><<<gn, 256, 0, s>>>(st, h->bt, h->sp, h->P, h->cells_at, h->leaf_start, h->dd_prefix,
+                                          h->leaf_coinc, h->cells, h->leaf_pre, st);
     }
     if (phases & PH_WALK) {
         WalkParams wp;

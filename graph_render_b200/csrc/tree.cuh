@@ -404,18 +404,15 @@ __device__ __forceinline__ double dd_diff(DD a, DD b) { return dd_add(a, DD{-b.h
 
 constexpr int AG_T = 256, AG_I = 4, AG_TILE = AG_T * AG_I, AG_W = AG_T / GR_WARP;
 
+// FP64 sums of the sorted points [a0, a1) of one leaf, in order; coinc = all
+// points are the same point.
 template <int D>
-__global__ void k_leaf_body(const DevState *st, const float4 *__restrict__ sp, const uint32_t *__restrict__ leaf_start,
-                            Body *__restrict__ leaf_body, uint8_t *__restrict__ leaf_coinc) {
-    if (st->converged) return;
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= st->n_unique) return;
-    const uint32_t a0 = leaf_start[s], a1 = leaf_start[s + 1];
+__device__ __forceinline__ Body leaf_sum(const float4 *__restrict__ sp, uint32_t a0, uint32_t a1, bool &coinc) {
     Body b{0.0, 0.0, 0.0, 0.0};
     const float4 f0 = sp[a0];
-    bool coinc = true;
+    coinc = true;
     for (uint32_t q = a0; q < a1; q++) {
-        const float4 p = sp[q];
+        const float4 p = q == a0 ? f0 : sp[q];
         const double m = (double)p.w;
         b.m += m;
         b.c0 += m * (double)p.x;
@@ -423,7 +420,19 @@ __global__ void k_leaf_body(const DevState *st, const float4 *__restrict__ sp, c
         if (D == 3) b.c2 += m * (double)p.z;
         coinc = coinc && p.x == f0.x && p.y == f0.y && (D == 2 || p.z == f0.z);
     }
-    body_store(&leaf_body[s], b);
+    return b;
+}
+
+// Leaf bodies as an array (the adjoint reads them; the tick's own cell writer
+// recomputes them with the same leaf_sum).
+template <int D>
+__global__ void k_leaf_body(const DevState *st, const float4 *__restrict__ sp, const uint32_t *__restrict__ leaf_start,
+                            Body *__restrict__ leaf_body, uint8_t *__restrict__ leaf_coinc) {
+    if (st->converged) return;
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= st->n_unique) return;
+    bool coinc;
+    body_store(&leaf_body[s], leaf_sum<D>(sp, leaf_start[s], leaf_start[s + 1], coinc));
     leaf_coinc[s] = coinc ? 1 : 0;
 }
 
@@ -469,19 +478,29 @@ __device__ __forceinline__ BodyDD block_scan_bdd(const BodyDD &x, const BodyDD &
     return bdd_add<D>(bdd_add<D>(carry, before), lanes_before);
 }
 
-// Sequential double-double sum of this thread's AG_I leaves.
+// This thread's AG_I leaf bodies (leaf_sum over the sorted points) and their
+// sequential double-double sum.
 template <int D>
-__device__ __forceinline__ BodyDD thread_chunk(const Body *__restrict__ lb, uint32_t base, uint32_t nu) {
+__device__ __forceinline__ BodyDD thread_chunk(const float4 *__restrict__ sp, const uint32_t *__restrict__ leaf_start,
+                                               uint32_t base, uint32_t nu, Body *lb, uint32_t &coinc_bits) {
     BodyDD acc{};
+    coinc_bits = 0;
+#pragma unroll
     for (int r = 0; r < AG_I; r++) {
         const uint32_t s = base + r;
-        if (s < nu) acc = bdd_add<D>(acc, bdd_of(lb[s]));
+        if (s < nu) {
+            bool c;
+            lb[r] = leaf_sum<D>(sp, leaf_start[s], leaf_start[s + 1], c);
+            coinc_bits |= (c ? 1u : 0u) << r;
+            acc = bdd_add<D>(acc, bdd_of(lb[r]));
+        }
     }
     return acc;
 }
 
 template <int D>
-__global__ void __launch_bounds__(AG_T) k_dd_reduce(const DevState *st, const Body *__restrict__ lb,
+__global__ void __launch_bounds__(AG_T) k_dd_reduce(const DevState *st, const float4 *__restrict__ sp,
+                                                    const uint32_t *__restrict__ leaf_start,
                                                     BodyDD *__restrict__ bsum) {
     if (st->converged) return;
     __shared__ BodyDD s_w[2 * AG_W];
@@ -489,7 +508,9 @@ __global__ void __launch_bounds__(AG_T) k_dd_reduce(const DevState *st, const Bo
     const uint32_t base = blockIdx.x * AG_TILE;
     if (base >= nu) return;
     BodyDD total;
-    block_scan_bdd<D>(thread_chunk<D>(lb, base + threadIdx.x * AG_I, nu), BodyDD{}, total, s_w);
+    Body lb[AG_I];
+    uint32_t cb;
+    block_scan_bdd<D>(thread_chunk<D>(sp, leaf_start, base + threadIdx.x * AG_I, nu, lb, cb), BodyDD{}, total, s_w);
     if (threadIdx.x == 0) bsum[blockIdx.x] = total;
 }
 
@@ -514,9 +535,12 @@ __global__ void __launch_bounds__(AG_T) k_dd_blocks(const DevState *st, BodyDD *
     if (threadIdx.x == 0) prefix[nu] = carry;
 }
 
+// The exclusive prefix at every leaf, and every leaf's coincidence flag.
 template <int D>
-__global__ void __launch_bounds__(AG_T) k_dd_down(const DevState *st, const Body *__restrict__ lb,
-                                                  const BodyDD *__restrict__ bsum, BodyDD *__restrict__ prefix) {
+__global__ void __launch_bounds__(AG_T) k_dd_down(const DevState *st, const float4 *__restrict__ sp,
+                                                  const uint32_t *__restrict__ leaf_start,
+                                                  const BodyDD *__restrict__ bsum, BodyDD *__restrict__ prefix,
+                                                  uint8_t *__restrict__ leaf_coinc) {
     if (st->converged) return;
     __shared__ BodyDD s_w[2 * AG_W];
     const uint32_t nu = st->n_unique;
@@ -524,24 +548,34 @@ __global__ void __launch_bounds__(AG_T) k_dd_down(const DevState *st, const Body
     if (base >= nu) return;
     const uint32_t mine = base + threadIdx.x * AG_I;
     BodyDD total;
-    BodyDD run = block_scan_bdd<D>(thread_chunk<D>(lb, mine, nu), bsum[blockIdx.x], total, s_w);
+    Body lb[AG_I];
+    uint32_t cb;
+    BodyDD run = block_scan_bdd<D>(thread_chunk<D>(sp, leaf_start, mine, nu, lb, cb), bsum[blockIdx.x], total, s_w);
+#pragma unroll
     for (int r = 0; r < AG_I; r++) {
         const uint32_t s = mine + r;
-        if (s >= nu) break;
-        prefix[s] = run;
-        run = bdd_add<D>(run, bdd_of(lb[s]));
+        if (s < nu) {
+            prefix[s] = run;
+            leaf_coinc[s] = (cb >> r) & 1u;
+            run = bdd_add<D>(run, bdd_of(lb[r]));
+        }
     }
 }
 
 // Internal node i covers leaves [first, last]: its sums are prefix[last + 1] -
 // prefix[first].
+__device__ __forceinline__ Body range_body(const BodyDD &a, const BodyDD &b) {
+    return Body{dd_diff(b.m, a.m), dd_diff(b.c0, a.c0), dd_diff(b.c1, a.c1), dd_diff(b.c2, a.c2)};
+}
+
+// Every internal node's body as an array (the adjoint reads them; the tick's
+// own cell writer takes range_body of the cells only).
 __global__ void k_node_body(const DevState *st, BinTree t, const BodyDD *__restrict__ prefix,
                             Body *__restrict__ int_body) {
     if (st->converged) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i + 1 >= st->n_unique) return;
-    const BodyDD a = prefix[t.first[i]], b = prefix[t.last[i] + 1];
-    body_store(&int_body[i], Body{dd_diff(b.m, a.m), dd_diff(b.c0, a.c0), dd_diff(b.c1, a.c1), dd_diff(b.c2, a.c2)});
+    body_store(&int_body[i], range_body(prefix[t.first[i]], prefix[t.last[i] + 1]));
 }
 
 template <int D>
@@ -644,18 +678,46 @@ __device__ __forceinline__ void assign_leaf(uint32_t s, uint32_t nu, uint32_t nc
     if (idx != P[s]) atomicOr(err, (uint32_t)ERR_TREE);
 }
 
+// assign_leaf with the bodies computed on the spot: the leaf's from its points
+// (leaf_sum), each cell ancestor's from the prefix at its range ends
+// (range_body) — the values k_leaf_body and k_node_body store.
 template <int D>
-__global__ void k_assign(const DevState *st, BinTree t, const float4 *__restrict__ sp, const uint32_t *__restrict__ P,
-                         const uint32_t *__restrict__ cells_at, const uint32_t *__restrict__ leaf_start,
-                         const Body *__restrict__ leaf_body, const Body *__restrict__ int_body,
-                         const uint8_t *__restrict__ leaf_coinc, Cells cells,
-                         uint32_t *__restrict__ leaf_pre, DevState *stw) {
+__global__ void k_assign_dd(const DevState *st, BinTree t, const float4 *__restrict__ sp,
+                            const uint32_t *__restrict__ P, const uint32_t *__restrict__ cells_at,
+                            const uint32_t *__restrict__ leaf_start, const BodyDD *__restrict__ prefix,
+                            const uint8_t *__restrict__ leaf_coinc, Cells cells, uint32_t *__restrict__ leaf_pre,
+                            DevState *stw) {
     if (st->converged) return;
+    constexpr int L = Levels<D>::L;
     const uint32_t nu = st->n_unique;
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nu) return;
-    assign_leaf<D>(s, nu, st->n_cells, st->root_w, t, sp, P, cells_at, leaf_start, leaf_body, int_body, leaf_coinc,
-                   cells, leaf_pre, &stw->error);
+    const uint32_t ncells = st->n_cells;
+    const double rw = st->root_w;
+    uint32_t idx = P[s] + cells_at[s] - 1;
+    int32_t par = t.leaf_parent[s];
+    int level = 0;
+    if (par >= 0) level = leaf_coinc[s] ? t.delta[par] / D + 1 : L;
+    const uint32_t a0 = leaf_start[s], a1 = leaf_start[s + 1];
+    const float4 one = sp[a0];
+    bool coinc;
+    write_cell<D>(cells, idx, leaf_sum<D>(sp, a0, a1, coinc), level, rw, -(int32_t)(a1 - a0), a0,
+                  a1 - a0 == 1 ? &one : nullptr);
+    leaf_pre[s] = idx;
+    if (par >= 0 && t.first[par] == s) {
+        const BodyDD ps = prefix[s];
+        for (int depth = 0; par >= 0 && t.first[par] == s && depth <= 66; depth++) {
+            if (is_cell<D>(t, par)) {
+                idx--;
+                const uint32_t end = t.last[par] + 1;
+                const uint32_t skip = end == nu ? ncells : P[end];
+                write_cell<D>(cells, idx, range_body(ps, prefix[end]), t.delta[par] / D, rw, (int32_t)skip, a0);
+                if (t.cell_of) t.cell_of[par] = idx;
+            }
+            par = t.int_parent[par];
+        }
+    }
+    if (idx != P[s]) atomicOr(&stw->error, (uint32_t)ERR_TREE);
 }
 
 }  // namespace gr
