@@ -226,6 +226,7 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
     A(h->bt.int_parent, n);
     A(h->bt.leaf_parent, n);
     A(h->bt.visit, n);
+    A(h->bt.rec, n);
     A(h->leaf_body, n);
     A(h->int_body, n);
     A(h->leaf_coinc, n);
@@ -1027,6 +1028,7 @@ static int forces_static(uint32_t n, const float4 *nodes, const uint32_t *rp, co
     h.bt.int_parent = cv.take<int32_t>(n);
     h.bt.leaf_parent = cv.take<int32_t>(n);
     h.bt.visit = cv.take<uint32_t>(n);
+    h.bt.rec = cv.take<int4>(n);
     h.leaf_body = cv.take<Body>(n);
     h.int_body = cv.take<Body>(n);
     h.leaf_coinc = cv.take<uint8_t>(n);

@@ -258,6 +258,7 @@ struct BinTree {
     int32_t *leaf_parent; // leaf -> parent (-1 when the tree is one leaf)
     uint32_t *visit;      // bottom-up arrival tickets
     uint32_t *cell_of;    // internal node -> its cell's preorder index, when it is a cell (nullable)
+    int4 *rec;            // internal node -> {first, last, parent, delta} in one load (nullable)
 };
 
 __device__ __forceinline__ int kdelta(const uint64_t *__restrict__ k, int32_t a, int32_t b, int32_t nu) {
@@ -288,12 +289,19 @@ __device__ __forceinline__ void karras_node(int32_t i, int32_t nu, const uint64_
     t.last[i] = (uint32_t)last;
     t.delta[i] = dnode;
     t.visit[i] = 0;
+    if (t.rec) {  // z (parent) is written by the parent
+        int *r = (int *)&t.rec[i];
+        r[0] = first;
+        r[1] = last;
+        r[3] = dnode;
+    }
     if (first == gamma) {
         t.left[i] = (uint32_t)gamma | LEAF_BIT;
         t.leaf_parent[gamma] = i;
     } else {
         t.left[i] = (uint32_t)gamma;
         t.int_parent[gamma] = i;
+        if (t.rec) ((int *)&t.rec[gamma])[2] = i;
     }
     if (last == gamma + 1) {
         t.right[i] = (uint32_t)(gamma + 1) | LEAF_BIT;
@@ -301,8 +309,12 @@ __device__ __forceinline__ void karras_node(int32_t i, int32_t nu, const uint64_
     } else {
         t.right[i] = (uint32_t)(gamma + 1);
         t.int_parent[gamma + 1] = i;
+        if (t.rec) ((int *)&t.rec[gamma + 1])[2] = i;
     }
-    if (i == 0) t.int_parent[0] = -1;
+    if (i == 0) {
+        t.int_parent[0] = -1;
+        if (t.rec) ((int *)&t.rec[0])[2] = -1;
+    }
 }
 
 __global__ void k_karras(const DevState *st, const uint64_t *__restrict__ k, BinTree t) {
@@ -597,13 +609,30 @@ __device__ __forceinline__ uint32_t count_leaf(uint32_t s, const BinTree &t) {
     return c;
 }
 
+// count_leaf over the packed records: one dependent load per level (the
+// parent's record tells whether this node is a cell and is the next level).
+template <int D>
+__device__ __forceinline__ uint32_t count_leaf_rec(uint32_t s, const BinTree &t) {
+    uint32_t c = 1;
+    const int32_t par = t.leaf_parent[s];
+    if (par < 0) return c;
+    int4 R = t.rec[par];
+    for (int depth = 0; R.x == (int)s && depth <= 66; depth++) {
+        if (R.z < 0) return c + 1;  // the root is a cell
+        const int4 Q = t.rec[R.z];
+        if (R.w / D != Q.w / D) c++;
+        R = Q;
+    }
+    return c;
+}
+
 template <int D>
 __global__ void k_count(const DevState *st, BinTree t, uint32_t *__restrict__ cells_at) {
     if (st->converged) return;
     const uint32_t nu = st->n_unique;
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nu) return;
-    cells_at[s] = count_leaf<D>(s, t);
+    cells_at[s] = t.rec ? count_leaf_rec<D>(s, t) : count_leaf<D>(s, t);
 }
 
 // Cell record, 2D: A = {cx, cy, mass, w^2}, B = {cx_lo, cy_lo, skip | -count, start}.
@@ -696,25 +725,29 @@ __global__ void k_assign_dd(const DevState *st, BinTree t, const float4 *__restr
     const double rw = st->root_w;
     uint32_t idx = P[s] + cells_at[s] - 1;
     int32_t par = t.leaf_parent[s];
+    int4 R = par >= 0 ? t.rec[par] : make_int4(-1, -1, -1, 0);
     int level = 0;
-    if (par >= 0) level = leaf_coinc[s] ? t.delta[par] / D + 1 : L;
+    if (par >= 0) level = leaf_coinc[s] ? R.w / D + 1 : L;
     const uint32_t a0 = leaf_start[s], a1 = leaf_start[s + 1];
     const float4 one = sp[a0];
     bool coinc;
     write_cell<D>(cells, idx, leaf_sum<D>(sp, a0, a1, coinc), level, rw, -(int32_t)(a1 - a0), a0,
                   a1 - a0 == 1 ? &one : nullptr);
     leaf_pre[s] = idx;
-    if (par >= 0 && t.first[par] == s) {
+    if (par >= 0 && R.x == (int)s) {
         const BodyDD ps = prefix[s];
-        for (int depth = 0; par >= 0 && t.first[par] == s && depth <= 66; depth++) {
-            if (is_cell<D>(t, par)) {
+        for (int depth = 0; depth <= 66; depth++) {
+            const int4 Q = R.z >= 0 ? t.rec[R.z] : make_int4(-1, -1, -1, 0);
+            if (R.z < 0 || R.w / D != Q.w / D) {  // par is a cell
                 idx--;
-                const uint32_t end = t.last[par] + 1;
+                const uint32_t end = (uint32_t)R.y + 1;
                 const uint32_t skip = end == nu ? ncells : P[end];
-                write_cell<D>(cells, idx, range_body(ps, prefix[end]), t.delta[par] / D, rw, (int32_t)skip, a0);
+                write_cell<D>(cells, idx, range_body(ps, prefix[end]), R.w / D, rw, (int32_t)skip, a0);
                 if (t.cell_of) t.cell_of[par] = idx;
             }
-            par = t.int_parent[par];
+            if (R.z < 0 || Q.x != (int)s) break;
+            par = R.z;
+            R = Q;
         }
     }
     if (idx != P[s]) atomicOr(&stw->error, (uint32_t)ERR_TREE);
