@@ -203,17 +203,21 @@ __device__ __forceinline__ void walk_lane(const WalkView &V, uint32_t p, float &
         const float dz = (D == 3) ? (me.z - cz) - lz : 0.f;
         const float d2 = (D == 3) ? dx * dx + dy * dy + dz * dz : dx * dx + dy * dy;
         const bool far = !holds && w2 < th2 * d2;  // w2 > 0, so this is false at d2 == 0
-        if (far || (sk == -1 && !holds && d2 > 0.f)) {  // a body: far cell, or a one-point leaf's pair
-            const float f = __fdividef(mk * cm, d2);
-            f0 += dx * f;
-            f1 += dy * f;
-            if (D == 3) f2 += dz * f;
-            if (far)
-                nfar++;
-            else
-                npair++;
-            k = skip;
-        } else if (leaf && !holds && sk == -1) {  // coincident one-point leaf: the jiggle
+        // The common outcomes without a branch: a body term (far cell, or a
+        // one-point leaf's pair) is added, anything else adds +-0 (an exact no-op:
+        // the sums start at +0 and never hold -0); the walk moves to skip or k + 1.
+        const bool body = far || (sk == -1 && !holds && d2 > 0.f);
+        const float fb = __fdividef(mk * cm, d2);
+        const float f = body ? fb : 0.f;
+        f0 += dx * f;
+        f1 += dy * f;
+        if (D == 3) f2 += dz * f;
+        nfar += far ? 1u : 0u;
+        npair += (body && !far) ? 1u : 0u;
+        const uint32_t kn = body ? skip : k + 1;
+        if (!leaf || body) {
+            k = kn;
+        } else if (!holds && sk == -1) {  // coincident one-point leaf: the jiggle
             const uint32_t oj = __ldg(&V.sorig[start]);
             const float sg = oi < oj ? 1.f : -1.f;
             const float ex = sg * (float)jiggle(V.seed, iter, 0, oi, oj);
@@ -226,7 +230,7 @@ __device__ __forceinline__ void walk_lane(const WalkView &V, uint32_t p, float &
             if (D == 3) f2 += ez * f;
             npair++;
             k = k + 1;
-        } else if (leaf) {  // several points (or this node's own leaf): exact pairs
+        } else {  // several points (or this node's own leaf): exact pairs
             int32_t cnt = -sk;
             if (start >= n || (uint32_t)cnt > n - start) {
                 atomicOr(V.err, (uint32_t)ERR_TREE);
@@ -251,8 +255,6 @@ __device__ __forceinline__ void walk_lane(const WalkView &V, uint32_t p, float &
                 if (D == 3) f2 += ez * f;
                 npair++;
             }
-            k = k + 1;
-        } else {
             k = k + 1;
         }
     }
