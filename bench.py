@@ -355,11 +355,12 @@ def run_adjoint(args, dist: Dist):
 def run_3d(args, dist: Dist):
     """The 1M-node configuration-model graph in 3D (octree), strong gravity, theta 1.2."""
     from graph_render_b200 import Fa2
+    from graph_render_b200.fa2 import WALK_SCHEDULE_NAMES
 
     wl = workload("powerlaw-3d", 0)
     with Fa2(wl.n, wl.src, wl.dst, wl.weight, params=wl.params, pos0=wl.pos0) as eng:
         eng.tick(1)
-        eng.tune(2)
+        chosen, tuned = eng.tune(2)
         eng.tick(3)
         ms = eng.tick_timed(10, l2_flush_bytes=FLUSH_BYTES)
         inf = eng.info()
@@ -367,7 +368,9 @@ def run_3d(args, dist: Dist):
     return {"workload": wl.name, "n": wl.n, "node_ticks_per_s": wl.n * len(ms) / (t / 1e3),
             "ms_per_tick": t / len(ms), "phase_ms": {"tree": float(ms[:, 0].mean()), "walk": float(ms[:, 1].mean()),
                                                     "finish": float(ms[:, 2].mean())},
-            "n_cells": inf["n_cells"]}
+            "n_cells": inf["n_cells"],
+            "walk_schedule": {"chosen": WALK_SCHEDULE_NAMES[chosen],
+                              "tuned_walk_ms": {WALK_SCHEDULE_NAMES[i]: v for i, v in tuned.items()}}}
 
 
 # --------------------------------------------------------------- GPU arm --
@@ -376,6 +379,7 @@ def run_gpu(args, dist: Dist):
     import torch
 
     from graph_render_b200 import Fa2
+    from graph_render_b200.fa2 import WALK_SCHEDULE_NAMES
 
     dev = dist.local if dist.world > 1 else 0
     torch.cuda.set_device(dev)
@@ -477,9 +481,9 @@ def run_gpu(args, dist: Dist):
                              "(outside the events)",
                        "parallelism": f"{dist.world} independent replicas" if dist.world > 1 else "1 GPU",
                        "phase_ms": {"tree": tree_ms, "walk": walk_ms, "finish": fin_ms},
-                       "walk_schedule": {"chosen": ["warp-union", "per-lane"][schedule],
-                                         "tuned_walk_ms": {"warp-union": schedule_ms[0],
-                                                           "per-lane": schedule_ms[1]}}},
+                       "walk_schedule": {"chosen": WALK_SCHEDULE_NAMES[schedule],
+                                         "tuned_walk_ms": {WALK_SCHEDULE_NAMES[i]: schedule_ms[i]
+                                                           for i in range(len(WALK_SCHEDULE_NAMES))}}},
             "clocks": clocks,
             "e2e": e2e,
             "gpu_launches": int(info1["graph_kernels"]) * done,

@@ -157,7 +157,7 @@ struct gr_fa2 {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint32_t graph_kernels = 0;
-    int walk_schedule = 1;  // 0: warp-cooperative union walk, 1: per-lane walk
+    int walk_schedule = 1;  // 0: warp-cooperative union walk, 1: per-lane walk, 2: two nodes per lane
     // the same tick as three graphs (tree, walk, forces+update) for per-phase timing
     cudaGraph_t pgraph[3] = {nullptr, nullptr, nullptr};
     cudaGraphExec_t pexec[3] = {nullptr, nullptr, nullptr};
@@ -316,12 +316,15 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
         wp.kr = (float)h->prm[P_SCALING];
         wp.theta2 = (float)(h->prm[P_THETA] * h->prm[P_THETA]);
         wp.seed = (uint32_t)h->prm[P_SEED];
-        if (h->walk_schedule == 1)
-            k_walk_s<D, true><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig,
-                                                                                h->uid, h->leaf_pre, h->rep, st);
+        if (h->walk_schedule == 2)
+            k_walk_s<D, 2><<<div_up(div_up(n, 2), WALK_THREADS), WALK_THREADS, 0, s>>>(
+                wp, st, h->cells, h->sp, h->sorig, h->uid, h->leaf_pre, h->rep, st);
+        else if (h->walk_schedule == 1)
+            k_walk_s<D, 1><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig, h->uid,
+                                                                           h->leaf_pre, h->rep, st);
         else
-            k_walk_s<D, false><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig,
-                                                                                 h->uid, h->leaf_pre, h->rep, st);
+            k_walk_s<D, 0><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig, h->uid,
+                                                                           h->leaf_pre, h->rep, st);
     }
     if (phases & PH_FINISH) {
         ForceParams fp;
@@ -824,7 +827,8 @@ int gr_fa2_get_info(gr_fa2 *h, gr_fa2_info *out) {
 
 int gr_fa2_set_walk_schedule(gr_fa2 *h, int schedule) {
     if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
-    if (schedule != 0 && schedule != 1) return set_err(GR_INVALID_ARGUMENT, "walk schedule must be 0 or 1");
+    if (schedule < 0 || schedule >= GR_WALK_SCHEDULES)
+        return set_err(GR_INVALID_ARGUMENT, "walk schedule must be 0, 1 or 2");
     if (schedule != h->walk_schedule) {
         h->walk_schedule = schedule;
         h->drop_graphs();
@@ -848,7 +852,7 @@ int gr_fa2_tune(gr_fa2 *h, uint32_t sample_ticks, int *chosen, float *walk_ms_ea
     std::vector<float> ms(4 * (size_t)sample_ticks);
     float best = 1e30f;
     int pick = h->walk_schedule, rc = GR_OK;
-    for (int sch = 0; sch < 2 && rc == GR_OK; sch++) {
+    for (int sch = 0; sch < GR_WALK_SCHEDULES && rc == GR_OK; sch++) {
         h->walk_schedule = sch;
         h->drop_graphs();
         uint32_t done = 0;

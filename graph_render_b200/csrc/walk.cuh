@@ -260,52 +260,169 @@ __device__ __forceinline__ void walk_lane(const WalkView &V, uint32_t p, float &
     }
 }
 
-template <int D, bool LANE>
+// One node of a two-node walk (walk_pair): its own state and its visit of
+// cell k when k >= resume, with walk_lane's arithmetic.
+struct PairNode {
+    float4 me;
+    uint32_t p, mylp, oi, resume;
+    float mk, f0, f1, f2;
+    uint32_t nfar, npair;
+};
+
+template <int D>
+__device__ __forceinline__ void pair_init(const WalkView &V, uint32_t p, PairNode &X) {
+    const bool valid = p < V.n;
+    X.p = p;
+    X.me = valid ? V.sp[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+    X.mylp = valid ? V.leaf_pre[V.uid[p]] : 0u;
+    X.oi = valid ? V.sorig[p] : 0u;
+    X.resume = valid ? 0u : 0xffffffffu;
+    X.mk = X.me.w * V.kr;
+    X.f0 = X.f1 = X.f2 = 0.f;
+    X.nfar = X.npair = 0;
+}
+
+template <int D>
+__device__ __forceinline__ void pair_visit(const WalkView &V, PairNode &X, uint32_t k, float cx, float cy, float cz,
+                                           float lx, float ly, float lz, float cm, float w2, int32_t sk,
+                                           uint32_t start, uint32_t skip, bool leaf) {
+    if (k < X.resume) return;  // inside a subtree this node approximated
+    const bool holds = (k <= X.mylp) && (X.mylp < skip);
+    const float dx = (X.me.x - cx) - lx;
+    const float dy = (X.me.y - cy) - ly;
+    const float dz = (D == 3) ? (X.me.z - cz) - lz : 0.f;
+    const float d2 = (D == 3) ? dx * dx + dy * dy + dz * dz : dx * dx + dy * dy;
+    const bool far = !holds && w2 < V.th2 * d2;
+    const bool body = far || (sk == -1 && !holds && d2 > 0.f);
+    const float fb = __fdividef(X.mk * cm, d2);
+    const float f = body ? fb : 0.f;
+    X.f0 += dx * f;
+    X.f1 += dy * f;
+    if (D == 3) X.f2 += dz * f;
+    X.nfar += far ? 1u : 0u;
+    X.npair += (body && !far) ? 1u : 0u;
+    X.resume = body ? skip : k + 1;
+    if (!leaf || body) return;
+    const float4 *__restrict__ sp = V.sp;
+    const uint32_t n = V.n, iter = V.iter;
+    if (!holds && sk == -1) {  // coincident one-point leaf: the jiggle
+        const uint32_t oj = __ldg(&V.sorig[start]);
+        const float sg = X.oi < oj ? 1.f : -1.f;
+        const float ex = sg * (float)jiggle(V.seed, iter, 0, X.oi, oj);
+        const float ey = sg * (float)jiggle(V.seed, iter, 1, X.oi, oj);
+        const float ez = (D == 3) ? sg * (float)jiggle(V.seed, iter, 2, X.oi, oj) : 0.f;
+        const float e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
+        const float g = __fdividef(X.mk * cm, e2);
+        X.f0 += ex * g;
+        X.f1 += ey * g;
+        if (D == 3) X.f2 += ez * g;
+        X.npair++;
+        return;
+    }
+    int32_t cnt = -sk;  // several points (or this node's own leaf): exact pairs
+    if (start >= n || (uint32_t)cnt > n - start) {
+        atomicOr(V.err, (uint32_t)ERR_TREE);
+        cnt = 0;
+    }
+    for (int32_t q = 0; q < cnt; q++) {
+        const uint32_t jp = start + (uint32_t)q;
+        if (jp == X.p) continue;
+        const float4 o = __ldg(&sp[jp]);
+        float ex = X.me.x - o.x, ey = X.me.y - o.y, ez = (D == 3) ? X.me.z - o.z : 0.f;
+        if (ex == 0.f && ey == 0.f && (D == 2 || ez == 0.f)) {
+            const uint32_t oj = __ldg(&V.sorig[jp]);
+            const float sg = X.oi < oj ? 1.f : -1.f;
+            ex = sg * (float)jiggle(V.seed, iter, 0, X.oi, oj);
+            ey = sg * (float)jiggle(V.seed, iter, 1, X.oi, oj);
+            if (D == 3) ez = sg * (float)jiggle(V.seed, iter, 2, X.oi, oj);
+        }
+        const float e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
+        const float g = __fdividef(X.mk * o.w, e2);
+        X.f0 += ex * g;
+        X.f1 += ey * g;
+        if (D == 3) X.f2 += ez * g;
+        X.npair++;
+    }
+}
+
+// Two adjacent Morton-sorted nodes per thread over the union of their walks:
+// one cell load and one loop step serve both, and each node acts only at the
+// cells of its own walk (k >= its resume), in the same order, so its forces are
+// walk_lane's bit for bit. Adjacent nodes' walks nearly coincide, so the union
+// is little longer than either.
+template <int D>
+__device__ __forceinline__ void walk_pair(const WalkView &V, PairNode &a, PairNode &b) {
+    const Cells cells = V.cells;
+    const uint32_t ncells = V.ncells;
+    uint32_t k = min(a.resume, b.resume);
+    while (k < ncells) {
+        const float4 A = __ldg(&cells.A[k]);
+        const float4 B = __ldg(&cells.B[k]);
+        int32_t sk;
+        uint32_t start;
+        float cx, cy, cz, cm, w2, lx, ly, lz;
+        if (D == 2) {
+            cx = A.x; cy = A.y; cz = 0.f; cm = A.z; w2 = A.w;
+            lx = B.x; ly = B.y; lz = 0.f;
+            sk = __float_as_int(B.z);
+            start = __float_as_uint(B.w);
+        } else {
+            const int2 Cc = __ldg(&cells.C[k]);
+            cx = A.x; cy = A.y; cz = A.z; cm = A.w;
+            lx = B.x; ly = B.y; lz = B.z; w2 = B.w;
+            sk = Cc.x;
+            start = (uint32_t)Cc.y;
+        }
+        const bool leaf = sk < 0;
+        uint32_t skip = leaf ? k + 1 : (uint32_t)sk;
+        skip = max(skip, k + 1);  // every step moves forward, whatever a cell holds
+        pair_visit<D>(V, a, k, cx, cy, cz, lx, ly, lz, cm, w2, sk, start, skip, leaf);
+        pair_visit<D>(V, b, k, cx, cy, cz, lx, ly, lz, cm, w2, sk, start, skip, leaf);
+        k = min(a.resume, b.resume);
+    }
+}
+
+// Walk schedules: 0 = walk_group (a warp over the union of its 32 nodes),
+// 1 = walk_lane (one node per lane), 2 = walk_pair (two adjacent nodes per lane).
+template <int D, int SCHED>
 __global__ void __launch_bounds__(WALK_THREADS)
 k_walk_s(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 *__restrict__ sp,
          const uint32_t *__restrict__ sorig, const uint32_t *__restrict__ uid,
          const uint32_t *__restrict__ leaf_pre, float *__restrict__ rep, DevState *stw) {
     if (st->converged) return;
-    const uint32_t p = blockIdx.x * WALK_THREADS + threadIdx.x;
+    const uint32_t g = blockIdx.x * WALK_THREADS + threadIdx.x;
+    const uint32_t p = SCHED == 2 ? 2 * g : g;
     if (__all_sync(GR_FULL, p >= P.n)) return;
     WalkView V{cells, sp, sorig, uid, leaf_pre, P.n, st->n_cells, st->iter_no, P.seed, P.kr, P.theta2, &stw->error};
-    float f0, f1, f2;
     uint32_t nfar, npair;
-    if (LANE)
-        walk_lane<D>(V, p, f0, f1, f2, nfar, npair);
-    else
-        walk_group<D>(V, p, f0, f1, f2, nfar, npair);
-    if (p < P.n) {
-        const uint32_t oi = sorig[p];
-        rep[(size_t)oi * D + 0] = f0;
-        rep[(size_t)oi * D + 1] = f1;
-        if (D == 3) rep[(size_t)oi * D + 2] = f2;
-    }
-    nfar = __reduce_add_sync(GR_FULL, nfar);
-    npair = __reduce_add_sync(GR_FULL, npair);
-    if ((threadIdx.x % GR_WARP) == 0) {
-        atomicAdd(&stw->far_count, (unsigned long long)nfar);
-        atomicAdd(&stw->pair_count, (unsigned long long)npair);
-    }
-}
-
-template <int D>
-__global__ void __launch_bounds__(WALK_THREADS)
-k_walk(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 *__restrict__ sp,
-       const uint32_t *__restrict__ sorig, const uint32_t *__restrict__ uid,
-       const uint32_t *__restrict__ leaf_pre, float *__restrict__ rep, DevState *stw) {
-    if (st->converged) return;
-    const uint32_t p = blockIdx.x * WALK_THREADS + threadIdx.x;
-    if (__all_sync(GR_FULL, p >= P.n)) return;
-    WalkView V{cells, sp, sorig, uid, leaf_pre, P.n, st->n_cells, st->iter_no, P.seed, P.kr, P.theta2, &stw->error};
-    float f0, f1, f2;
-    uint32_t nfar, npair;
-    walk_group<D>(V, p, f0, f1, f2, nfar, npair);
-    if (p < P.n) {
-        const uint32_t oi = sorig[p];
-        rep[(size_t)oi * D + 0] = f0;
-        rep[(size_t)oi * D + 1] = f1;
-        if (D == 3) rep[(size_t)oi * D + 2] = f2;
+    if (SCHED == 2) {
+        PairNode a, b;
+        pair_init<D>(V, p, a);
+        pair_init<D>(V, p + 1, b);
+        walk_pair<D>(V, a, b);
+        const PairNode *X[2] = {&a, &b};
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+            if (X[j]->p < P.n) {
+                const uint32_t oi = X[j]->oi;
+                rep[(size_t)oi * D + 0] = X[j]->f0;
+                rep[(size_t)oi * D + 1] = X[j]->f1;
+                if (D == 3) rep[(size_t)oi * D + 2] = X[j]->f2;
+            }
+        nfar = a.nfar + b.nfar;
+        npair = a.npair + b.npair;
+    } else {
+        float f0, f1, f2;
+        if (SCHED == 1)
+            walk_lane<D>(V, p, f0, f1, f2, nfar, npair);
+        else
+            walk_group<D>(V, p, f0, f1, f2, nfar, npair);
+        if (p < P.n) {
+            const uint32_t oi = sorig[p];
+            rep[(size_t)oi * D + 0] = f0;
+            rep[(size_t)oi * D + 1] = f1;
+            if (D == 3) rep[(size_t)oi * D + 2] = f2;
+        }
     }
     nfar = __reduce_add_sync(GR_FULL, nfar);
     npair = __reduce_add_sync(GR_FULL, npair);

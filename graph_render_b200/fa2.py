@@ -23,6 +23,10 @@ PARAM_NAMES = ("max_iter", "jitter_tolerance", "scaling_ratio", "gravity", "seed
 DEFAULTS = dict(max_iter=100, jitter_tolerance=1.0, scaling_ratio=2.0, gravity=1.0, seed=0, dim=2,
                 theta=0.8, lin_log=0, strong_gravity=0, dissuade_hubs=0, edge_weight_influence=0.0)
 
+# walk schedules (include/graph_cuda.h GR_WALK_SCHEDULES): warp-union, per-lane, two nodes per lane
+WALK_SCHEDULES = 3
+WALK_SCHEDULE_NAMES = ("warp-union", "per-lane", "pair-per-lane")
+
 
 def params_bytes(params: Union[None, bytes, Dict[str, float], Sequence[float]] = None, **kw) -> bytes:
     """A parameter buffer from a dict / keywords (unnamed ones at their defaults)."""
@@ -155,9 +159,9 @@ class Fa2:
     def tune(self, sample_ticks: int = 3):
         """Autotunes the walk schedule; returns (chosen, {schedule: mean walk ms})."""
         chosen = C.c_int()
-        ms = np.zeros(2, np.float32)
+        ms = np.zeros(WALK_SCHEDULES, np.float32)
         N.check(self._L.gr_fa2_tune(self.h, int(sample_ticks), C.byref(chosen), _ptr(ms)))
-        return chosen.value, {0: float(ms[0]), 1: float(ms[1])}
+        return chosen.value, {i: float(ms[i]) for i in range(WALK_SCHEDULES)}
 
     def controller(self) -> dict:
         c = N.Controller()

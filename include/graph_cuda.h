@@ -126,10 +126,12 @@ int gr_fa2_tick_timed(gr_fa2 *h, uint32_t ticks, size_t l2_flush_bytes, float *m
 
 /* Repulsion walk schedule: 0 = warp-cooperative (a warp visits the union of its 32
  * nodes' paths, one broadcast load per cell), 1 = per lane (each lane its own
- * path, gathered loads; the default). Both give bit-identical forces.
+ * path, gathered loads; the default), 2 = two adjacent nodes per lane over the
+ * union of their two paths. All give bit-identical forces.
  * gr_fa2_tune times sample_ticks ticks with each from the current state (restored
- * afterwards) and keeps the faster; walk_ms_each (nullable, 2 floats) gets the
- * mean walk time of each. */
+ * afterwards) and keeps the fastest; walk_ms_each (nullable, GR_WALK_SCHEDULES
+ * floats) gets the mean walk time of each. */
+#define GR_WALK_SCHEDULES 3
 int gr_fa2_set_walk_schedule(gr_fa2 *h, int schedule);
 int gr_fa2_tune(gr_fa2 *h, uint32_t sample_ticks, int *chosen, float *walk_ms_each);
 

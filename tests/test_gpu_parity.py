@@ -143,13 +143,14 @@ def test_walk_schedules_give_bit_identical_forces_and_tuning_keeps_the_state(dim
     with Fa2(wl.n, wl.src, wl.dst, params=wl.params, pos0=wl.pos0) as eng:
         eng.tick(3)
         pos = eng.positions()
-        for sch in (0, 1):
+        for sch in (0, 1, 2):
             eng.set_walk_schedule(sch)
             outs.append((eng.forces(), eng.info()["far_count"]))
         chosen, ms = eng.tune(2)
-        assert chosen in (0, 1) and ms[0] > 0 and ms[1] > 0
+        assert chosen in (0, 1, 2) and all(ms[i] > 0 for i in (0, 1, 2))
         assert np.array_equal(eng.positions(), pos)
     assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][0], outs[2][0])
 
 
 def _full_sort_forces(n, src, dst, pos, prm):
