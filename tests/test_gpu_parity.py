@@ -193,3 +193,25 @@ def test_high_word_sort_with_run_fixup_equals_the_full_sort(cluster):
         fast = eng.forces()
     full = _full_sort_forces(wl.n, wl.src, wl.dst, pos, prm)
     assert np.array_equal(fast, full)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_engine_result_flows_through_the_snapshot_encoder(dim):
+    """run_params (the registry face) -> Geometry -> the snapshot's binary face ->
+    decode: the f32 columns come back bit for bit, in the topology's order."""
+    from graph_render_b200 import Topology, find, params_bytes
+    from graph_render_b200 import snapshot as S
+
+    n = 300
+    src, dst, st = O.gate_edges(n)
+    topo = Topology(n, src, dst, st)
+    geom = find("layout.forceatlas2.barnes_hut.cuda").run_params(topo, params_bytes(dim=dim, max_iter=50))
+    node_ids, edge_ids = S.gate_ids(n, len(src))
+    snap = S.of_geometry(node_ids, edge_ids, topo, geom)
+    b = snap.to_bytes()
+    back = S.from_bytes(b)
+    assert back.to_bytes() == b and back.dim == dim
+    assert np.array_equal(back.x.view(np.uint32), np.asarray(geom.x, np.float32).view(np.uint32))
+    assert np.array_equal(back.y.view(np.uint32), np.asarray(geom.y, np.float32).view(np.uint32))
+    assert np.array_equal(back.source, src) and np.array_equal(back.target, dst)
+    assert b[8:12] == (b"\x04\0\0\0" if dim == 3 else b"\x03\0\0\0")
