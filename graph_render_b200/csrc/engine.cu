@@ -29,6 +29,7 @@
 #include "walk.cuh"
 #include "batch.cuh"
 #include "adjoint.cuh"
+#include "stress.cuh"
 
 using namespace gr;
 
@@ -1669,6 +1670,152 @@ int gr_fa2_adjoint_backward(gr_fa2 *h, const float *dL_dpT, double *dL_dp0, doub
             dL_dw[e] = std::ldexp(dL_dw[e], ex);
             if (!std::isfinite(dL_dw[e])) return set_err(GR_LAYOUT_FAILED, "non-finite gradient");
         }
+    return ok();
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ stress / BFS --
+//
+// Multi-source BFS and Kruskal stress-1 on the device (stress.cuh). The
+// adjacency of the raw edges (both directions, self-loops dropped) is counted
+// and filled on the host, O(m), and copied once per call.
+
+namespace {
+
+struct DevBufs {  // device allocations released on every return path
+    std::vector<void *> p;
+    template <typename T>
+    cudaError_t get(T **out, size_t count) {
+        cudaError_t e = cudaMalloc((void **)out, (count ? count : 1) * sizeof(T));
+        if (e == cudaSuccess) p.push_back((void *)*out);
+        return e;
+    }
+    ~DevBufs() {
+        for (void *q : p) cudaFree(q);
+    }
+};
+
+struct StreamGuard {
+    cudaStream_t s = nullptr;
+    ~StreamGuard() {
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
+constexpr uint64_t kMaxHopTableBytes = 16ull << 30;
+
+// Hop counts from the k sources (device) to every node into hops (device, k x n,
+// HOP_NONE when unreachable), 64 sources per level-synchronous pull.
+int bfs_on_device(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst, uint32_t k,
+                  const uint32_t *sources_dev, uint32_t *hops, cudaStream_t s, DevBufs &B) {
+    std::vector<uint64_t> rp((size_t)n + 1, 0);
+    for (uint64_t e = 0; e < m; e++) {
+        if (src[e] >= n || dst[e] >= n) return set_err(GR_INDEX_OUT_OF_RANGE, "edge endpoint out of range", (int)e);
+        if (src[e] == dst[e]) continue;
+        rp[src[e] + 1]++;
+        rp[dst[e] + 1]++;
+    }
+    for (uint32_t i = 0; i < n; i++) rp[i + 1] += rp[i];
+    std::vector<uint32_t> col(std::max<uint64_t>(rp[n], 1));
+    std::vector<uint64_t> fill(rp.begin(), rp.end() - 1);
+    for (uint64_t e = 0; e < m; e++) {
+        if (src[e] == dst[e]) continue;
+        col[fill[src[e]]++] = dst[e];
+        col[fill[dst[e]]++] = src[e];
+    }
+    uint64_t *d_rp;
+    uint32_t *d_col, *d_changed;
+    unsigned long long *vis, *fa, *fb;
+    cudaError_t e;
+    if ((e = B.get(&d_rp, (size_t)n + 1)) || (e = B.get(&d_col, col.size())) || (e = B.get(&d_changed, 1)) ||
+        (e = B.get(&vis, n)) || (e = B.get(&fa, n)) || (e = B.get(&fb, n)))
+        return set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+    CU(cudaMemcpyAsync(d_rp, rp.data(), rp.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(d_col, col.data(), col.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    CU(cudaMemsetAsync(hops, 0xff, (size_t)k * n * sizeof(uint32_t), s));
+    const uint32_t grid = div_up(n, BFS_T);
+    for (uint32_t k0 = 0; k0 < k; k0 += 64) {
+        const uint32_t kb = std::min<uint32_t>(64, k - k0);
+        const unsigned long long all = kb == 64 ? ~0ull : ((1ull << kb) - 1ull);
+        CU(cudaMemsetAsync(vis, 0, (size_t)n * 8, s));
+        CU(cudaMemsetAsync(fa, 0, (size_t)n * 8, s));
+        k_msbfs_seed<<<1, 64, 0, s>>>(n, k0, kb, sources_dev, vis, fa, hops);
+        unsigned long long *cur = fa, *nxt = fb;
+        for (uint32_t level = 1; level < n; level++) {  // a BFS is at most n - 1 levels deep
+            uint32_t changed = 0;
+            CU(cudaMemsetAsync(d_changed, 0, 4, s));
+            k_msbfs_level<<<grid, BFS_T, 0, s>>>(n, d_rp, d_col, all, cur, vis, nxt, hops, k0, level, d_changed);
+            CU(cudaMemcpyAsync(&changed, d_changed, 4, cudaMemcpyDeviceToHost, s));
+            CU(cudaStreamSynchronize(s));
+            if (!changed) break;
+            std::swap(cur, nxt);
+        }
+    }
+    CU(cudaGetLastError());
+    return GR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gr_bfs_hops(uint32_t n, uint64_t m, const uint32_t *source, const uint32_t *target, uint32_t k,
+                const uint32_t *sources, uint32_t *hops_out) {
+    if ((m && (!source || !target)) || (k && (!sources || !hops_out)))
+        return set_err(GR_INVALID_ARGUMENT, "null buffer");
+    if ((uint64_t)k * n * 4 > kMaxHopTableBytes) return set_err(GR_INVALID_ARGUMENT, "hop table above 16 GiB");
+    for (uint32_t i = 0; i < k; i++)
+        if (sources[i] >= n) return set_err(GR_INDEX_OUT_OF_RANGE, "source out of range", (int)i);
+    if (k == 0 || n == 0) return ok();
+    DevBufs B;
+    StreamGuard g;
+    CU(cudaStreamCreateWithFlags(&g.s, cudaStreamNonBlocking));
+    uint32_t *d_src, *hops;
+    cudaError_t e;
+    if ((e = B.get(&d_src, k)) || (e = B.get(&hops, (size_t)k * n))) return set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+    CU(cudaMemcpyAsync(d_src, sources, (size_t)k * 4, cudaMemcpyHostToDevice, g.s));
+    if (int c = bfs_on_device(n, m, source, target, k, d_src, hops, g.s, B)) return c;
+    CU(cudaMemcpyAsync(hops_out, hops, (size_t)k * n * 4, cudaMemcpyDeviceToHost, g.s));
+    CU(cudaStreamSynchronize(g.s));
+    return ok();
+}
+
+int gr_stress(uint32_t n, uint64_t m, const uint32_t *source, const uint32_t *target, const float *x, const float *y,
+              uint32_t sources, double *out) {
+    if (!out || (m && (!source || !target)) || (n && (!x || !y))) return set_err(GR_INVALID_ARGUMENT, "null buffer");
+    if (sources == 0) return set_err(GR_INVALID_ARGUMENT, "sources must be >= 1");
+    *out = 1.0;
+    if (n == 0) return ok();
+    // the reference's sources: every max(n / sources, 1)-th node from 0 (bench.rs:266)
+    const uint32_t step = std::max<uint32_t>(n / sources, 1u);
+    std::vector<uint32_t> from;
+    for (uint64_t v = 0; v < n; v += step) from.push_back((uint32_t)v);
+    const uint32_t k = (uint32_t)from.size();
+    if ((uint64_t)k * n * 4 > kMaxHopTableBytes) return set_err(GR_INVALID_ARGUMENT, "hop table above 16 GiB");
+    DevBufs B;
+    StreamGuard g;
+    CU(cudaStreamCreateWithFlags(&g.s, cudaStreamNonBlocking));
+    uint32_t *d_src, *hops, *ticket;
+    float *dx, *dy;
+    double *part, *d_out;
+    const uint32_t G = 4 * 148;
+    cudaError_t e;
+    if ((e = B.get(&d_src, k)) || (e = B.get(&hops, (size_t)k * n)) || (e = B.get(&dx, n)) || (e = B.get(&dy, n)) ||
+        (e = B.get(&part, 3 * (size_t)G)) || (e = B.get(&d_out, 3)) || (e = B.get(&ticket, 1)))
+        return set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+    CU(cudaMemcpyAsync(d_src, from.data(), (size_t)k * 4, cudaMemcpyHostToDevice, g.s));
+    CU(cudaMemcpyAsync(dx, x, (size_t)n * 4, cudaMemcpyHostToDevice, g.s));
+    CU(cudaMemcpyAsync(dy, y, (size_t)n * 4, cudaMemcpyHostToDevice, g.s));
+    CU(cudaMemsetAsync(ticket, 0, 4, g.s));
+    if (int c = bfs_on_device(n, m, source, target, k, d_src, hops, g.s, B)) return c;
+    k_stress_sums<<<G, STRESS_T, 0, g.s>>>(n, k, d_src, hops, dx, dy, part, d_out, ticket);
+    double sums[3];
+    CU(cudaMemcpyAsync(sums, d_out, sizeof sums, cudaMemcpyDeviceToHost, g.s));
+    CU(cudaStreamSynchronize(g.s));
+    const double de = sums[0], ee = sums[1], dd = sums[2];
+    if (ee == 0.0 || dd == 0.0) return ok();
+    *out = std::sqrt(std::max((dd - de / ee * de) / dd, 0.0));
     return ok();
 }
 

@@ -218,47 +218,3 @@ void syn_unit(uint64_t count, uint64_t seed, double *out) {
     sm64 r = {seed};
     for (uint64_t i = 0; i < count; i++) out[i] = sm_unit(&r);
 }
-
-/* Hop distances by breadth-first search over the undirected raw edges, from
- * each of `nsrc` sources to every node: out[s * n + v] (UINT32_MAX when
- * unreachable). */
-void syn_bfs(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst, uint32_t nsrc,
-             const uint32_t *sources, uint32_t *out) {
-    uint64_t *rp = (uint64_t *)calloc((size_t)n + 1, sizeof(uint64_t));
-    for (uint64_t e = 0; e < m; e++) {
-        if (src[e] == dst[e]) continue;
-        rp[src[e] + 1]++;
-        rp[dst[e] + 1]++;
-    }
-    for (uint32_t i = 0; i < n; i++) rp[i + 1] += rp[i];
-    uint32_t *adj = (uint32_t *)malloc((size_t)(rp[n] ? rp[n] : 1) * sizeof(uint32_t));
-    uint64_t *fill = (uint64_t *)malloc((size_t)(n ? n : 1) * sizeof(uint64_t));
-    for (uint32_t i = 0; i < n; i++) fill[i] = rp[i];
-    for (uint64_t e = 0; e < m; e++) {
-        if (src[e] == dst[e]) continue;
-        adj[fill[src[e]]++] = dst[e];
-        adj[fill[dst[e]]++] = src[e];
-    }
-    uint32_t *queue = (uint32_t *)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
-    for (uint32_t k = 0; k < nsrc; k++) {
-        uint32_t *hop = out + (size_t)k * n;
-        for (uint32_t i = 0; i < n; i++) hop[i] = UINT32_MAX;
-        uint32_t head = 0, tail = 0, s = sources[k];
-        hop[s] = 0;
-        queue[tail++] = s;
-        while (head < tail) {
-            uint32_t v = queue[head++];
-            for (uint64_t e = rp[v]; e < rp[v + 1]; e++) {
-                uint32_t w = adj[e];
-                if (hop[w] == UINT32_MAX) {
-                    hop[w] = hop[v] + 1;
-                    queue[tail++] = w;
-                }
-            }
-        }
-    }
-    free(queue);
-    free(fill);
-    free(adj);
-    free(rp);
-}

@@ -3,9 +3,10 @@
 The reference's quality measure (crates/graph-cli/src/bench.rs:256-295):
 stress-1 with the optimal scale, sqrt((DD - DE^2/EE) / DD) over node pairs,
 DE = sum d e, EE = sum e^2, DD = sum d^2, d the hop distance and e the
-Euclidean distance. The reference sums over every target of a few BFS sources;
-here the pairs are sampled from a seed (`sample_pairs`), unreachable pairs are
-dropped, and `stress` also returns dL/dpositions for the adjoint.
+Euclidean distance. `kruskal_stress` is that measure (every target of the
+evenly spaced BFS sources), on the device. For the differentiated workload the
+pairs are sampled from a seed (`sample_pairs`, hop counts from the device BFS),
+unreachable pairs are dropped, and `stress` also returns dL/dpositions.
 """
 
 from __future__ import annotations
@@ -14,22 +15,36 @@ import ctypes as C
 
 import numpy as np
 
+from . import _native as N
 from . import synth
 
 
 def bfs_hops(n: int, src, dst, sources) -> np.ndarray:
-    """Hop distances from each source to every node (uint32, MAX if unreachable)."""
+    """Hop distances from each source to every node (uint32, MAX if unreachable),
+    by the device's multi-source BFS (gr_bfs_hops)."""
     src = np.ascontiguousarray(src, np.uint32)
     dst = np.ascontiguousarray(dst, np.uint32)
     sources = np.ascontiguousarray(sources, np.uint32)
     out = np.zeros((len(sources), n), np.uint32)
-    L = synth.lib()
-    if not getattr(L, "_bfs", False):
-        L.syn_bfs.argtypes = [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
-        L._bfs = True
-    L.syn_bfs(n, len(src), src.ctypes.data_as(C.c_void_p), dst.ctypes.data_as(C.c_void_p), len(sources),
-              sources.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p))
+    N.check(N.lib().gr_bfs_hops(n, len(src), _p(src), _p(dst), len(sources), _p(sources), _p(out)))
     return out
+
+
+def kruskal_stress(x, y, src, dst, sources: int = 16) -> float:
+    """The reference's quality measure (graph-cli/src/bench.rs:255-295 `stress`):
+    Kruskal stress-1 of (x, y) against hop distance from every max(n / sources,
+    1)-th node, on the device (gr_stress)."""
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    src = np.ascontiguousarray(src, np.uint32)
+    dst = np.ascontiguousarray(dst, np.uint32)
+    out = C.c_double()
+    N.check(N.lib().gr_stress(len(x), len(src), _p(src), _p(dst), _p(x), _p(y), sources, C.byref(out)))
+    return out.value
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p) if a.size else None
 
 
 def sample_pairs(n: int, src, dst, pairs: int, seed: int, sources: int = 1000):

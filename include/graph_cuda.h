@@ -176,6 +176,21 @@ int gr_fa2_set_controller(gr_fa2 *h, const gr_fa2_controller *in);
 int gr_fa2_adjoint_forward(gr_fa2 *h, uint32_t ticks, uint32_t checkpoint_every);
 int gr_fa2_adjoint_backward(gr_fa2 *h, const float *dL_dpT, double *dL_dp0, double *dL_dw);
 
+/* Multi-source BFS on the device: hop counts from k source nodes to every node
+ * (host out, k x n, UINT32_MAX when unreachable) over the raw edges (source,
+ * target), undirected, self-loops ignored. No counterpart in the reference, whose
+ * stress runs one queue BFS per source on the host (graph-cli/src/bench.rs:264-277). */
+int gr_bfs_hops(uint32_t n, uint64_t m, const uint32_t *source, const uint32_t *target, uint32_t k,
+                const uint32_t *sources, uint32_t *hops_out);
+
+/* Kruskal stress-1 of positions (x, y) against hop distance, the reference's
+ * quality measure (graph-cli/src/bench.rs:255-295 `stress`, called with its
+ * SOURCES = 16): BFS from every max(n / sources, 1)-th node, FP64 sums over every
+ * reachable (source, target) pair, stress = sqrt(max((DD - DE/EE*DE) / DD, 0)), and
+ * 1.0 for a collapsed layout or an edgeless graph. */
+int gr_stress(uint32_t n, uint64_t m, const uint32_t *source, const uint32_t *target, const float *x, const float *y,
+              uint32_t sources, double *out);
+
 /* The stream every call of this handle enqueues on (default: the handle's own). */
 int gr_fa2_set_stream(gr_fa2 *h, void *cuda_stream);
 

@@ -1276,3 +1276,99 @@ void orc_fa2_get_coef(const orc_fa2 *s, double *out) {
 void orc_fa2_set_coef(orc_fa2 *s, const double *in) {
     for (int64_t e = 0; e < s->m; e++) s->w[e] = in[e];
 }
+
+
+/* ------------------------------------------------------------- stress ------ */
+
+/* Adjacency of the raw edges as graph-cli/src/bench.rs:258-262 builds it: for
+ * edge (s, t) in edge order, t is pushed to s's list and s to t's (a self-loop
+ * appears twice in its own list). */
+static void stress_adjacency(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst, uint64_t **rp_out,
+                             uint32_t **adj_out) {
+    uint64_t *rp = (uint64_t *)calloc((size_t)n + 1, sizeof(uint64_t));
+    for (uint64_t e = 0; e < m; e++) {
+        rp[src[e] + 1]++;
+        rp[dst[e] + 1]++;
+    }
+    for (uint32_t i = 0; i < n; i++) rp[i + 1] += rp[i];
+    uint32_t *adj = (uint32_t *)malloc((size_t)(rp[n] ? rp[n] : 1) * sizeof(uint32_t));
+    uint64_t *fill = (uint64_t *)malloc((size_t)(n ? n : 1) * sizeof(uint64_t));
+    for (uint32_t i = 0; i < n; i++) fill[i] = rp[i];
+    for (uint64_t e = 0; e < m; e++) {
+        adj[fill[src[e]]++] = dst[e];
+        adj[fill[dst[e]]++] = src[e];
+    }
+    free(fill);
+    *rp_out = rp;
+    *adj_out = adj;
+}
+
+/* One FIFO BFS (bench.rs:267-277): hop[v] = UINT32_MAX when unreachable. */
+static void stress_bfs(uint32_t n, const uint64_t *rp, const uint32_t *adj, uint32_t from, uint32_t *hop,
+                       uint32_t *queue) {
+    for (uint32_t i = 0; i < n; i++) hop[i] = UINT32_MAX;
+    uint32_t head = 0, tail = 0;
+    hop[from] = 0;
+    queue[tail++] = from;
+    while (head < tail) {
+        uint32_t v = queue[head++];
+        for (uint64_t e = rp[v]; e < rp[v + 1]; e++) {
+            uint32_t w = adj[e];
+            if (hop[w] == UINT32_MAX) {
+                hop[w] = hop[v] + 1;
+                queue[tail++] = w;
+            }
+        }
+    }
+}
+
+/* graph-cli/src/bench.rs:255-295 `stress`: BFS from every max(n / sources, 1)-th
+ * node; per reachable target in ascending order d = hops, e = hypot((f64)(x[to] -
+ * x[from]), (f64)(y[to] - y[from])) with the difference taken in f32; DE, EE, DD
+ * summed in that order; sqrt(max((DD - DE / EE * DE) / DD, 0)), or 1 when EE or DD
+ * is 0. */
+double orc_stress(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst, const float *x, const float *y,
+                  uint32_t sources) {
+    if (n == 0) return 1.0;
+    uint64_t *rp;
+    uint32_t *adj;
+    stress_adjacency(n, m, src, dst, &rp, &adj);
+    uint32_t *hop = (uint32_t *)malloc((size_t)n * sizeof(uint32_t));
+    uint32_t *queue = (uint32_t *)malloc((size_t)n * sizeof(uint32_t));
+    double de = 0.0, ee = 0.0, dd = 0.0;
+    uint32_t step = n / sources;
+    if (step < 1) step = 1;
+    for (uint64_t from = 0; from < n; from += step) {
+        stress_bfs(n, rp, adj, (uint32_t)from, hop, queue);
+        for (uint32_t to = 0; to < n; to++) {
+            if (to == from || hop[to] == UINT32_MAX) continue;
+            double dist = (double)hop[to];
+            double dx = (double)(x[to] - x[from]), dy = (double)(y[to] - y[from]);
+            double euclid = hypot(dx, dy);
+            de += dist * euclid;
+            ee += euclid * euclid;
+            dd += dist * dist;
+        }
+    }
+    free(queue);
+    free(hop);
+    free(adj);
+    free(rp);
+    if (ee == 0.0 || dd == 0.0) return 1.0;
+    double r = (dd - de / ee * de) / dd;
+    return sqrt(r > 0.0 ? r : 0.0);
+}
+
+/* Hop counts from each of k sources by the same BFS (out: k x n). */
+void orc_bfs(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst, uint32_t k, const uint32_t *sources,
+             uint32_t *out) {
+    if (n == 0) return;
+    uint64_t *rp;
+    uint32_t *adj;
+    stress_adjacency(n, m, src, dst, &rp, &adj);
+    uint32_t *queue = (uint32_t *)malloc((size_t)n * sizeof(uint32_t));
+    for (uint32_t j = 0; j < k; j++) stress_bfs(n, rp, adj, sources[j], out + (size_t)j * n, queue);
+    free(queue);
+    free(adj);
+    free(rp);
+}

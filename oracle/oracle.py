@@ -64,10 +64,14 @@ def lib():
     L = C.CDLL(_LIB_PATH)
     P = C.c_void_p
     u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+    f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
     f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
     L.orc_initial_positions.argtypes = [C.c_uint32, C.c_uint32, C.c_int, f64p]
     L.orc_jiggle.argtypes = [C.c_uint32] * 5
     L.orc_jiggle.restype = C.c_double
+    L.orc_stress.argtypes = [C.c_uint32, C.c_int64, u32p, u32p, f32p, f32p, C.c_uint32]
+    L.orc_stress.restype = C.c_double
+    L.orc_bfs.argtypes = [C.c_uint32, C.c_int64, u32p, u32p, C.c_uint32, u32p, u32p]
     L.orc_gate_edges.argtypes = [C.c_uint32, u32p, u32p, f64p, C.c_int64]
     L.orc_gate_edges.restype = C.c_int64
     L.orc_simple_graph.argtypes = [C.c_uint32, C.c_int64, u32p, u32p, P, u32p, u32p, f64p]
@@ -116,6 +120,30 @@ def gate_edges(count: int):
     m = lib().orc_gate_edges(count, src, dst, st, cap)
     assert m <= cap
     return src[:m].copy(), dst[:m].copy(), st[:m].copy()
+
+
+def _nonempty_u32(a):
+    a = np.ascontiguousarray(a, np.uint32)
+    return a if len(a) else np.zeros(1, np.uint32)
+
+
+def stress(x, y, src, dst, sources: int = 16) -> float:
+    """graph-cli/src/bench.rs:255-295: Kruskal stress-1 against hop distance from
+    every max(n / sources, 1)-th node, in the reference's order."""
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    m = len(src)
+    return lib().orc_stress(len(x), m, _nonempty_u32(src), _nonempty_u32(dst), x if len(x) else np.zeros(1, np.float32),
+                            y if len(y) else np.zeros(1, np.float32), sources)
+
+
+def bfs_hops(n, src, dst, sources) -> np.ndarray:
+    """Hop counts (k x n uint32, UINT32_MAX when unreachable) by one FIFO BFS per source."""
+    sources = np.ascontiguousarray(sources, np.uint32)
+    out = np.zeros((len(sources), max(n, 1)), np.uint32)
+    lib().orc_bfs(n, len(src), _nonempty_u32(src), _nonempty_u32(dst), len(sources), _nonempty_u32(sources),
+                  out.reshape(-1))
+    return out[:, :n]
 
 
 def simple_graph(n, src, dst, w=None):

@@ -263,3 +263,19 @@ def test_oracle_3d_tree_theta0_equals_dense():
     b = O.State(300, lo, hi, pos0=pos, dim=3, theta=0.0).accumulate(2)
     node, total = errors(b, a)
     assert node < 1e-12 and total < 1e-12
+
+
+def test_oracle_stress_matches_the_references_unit_tests():
+    """crates/graph-cli/src/bench/tests/plan.rs:70-90, restated."""
+    assert O.stress([0.0, 2.0, 4.0], [0.0] * 3, [0, 1], [1, 2]) == 0.0  # isometric path
+    assert O.stress([0.0, 1.0, 0.0], [0.0] * 3, [0, 1], [1, 2]) == (8.0 / 12.0) ** 0.5  # folded
+    assert O.stress([5.0] * 3, [5.0] * 3, [0, 1], [1, 2]) == 1.0  # collapsed
+    assert O.stress([0.0, 1.0], [0.0, 0.0], [], []) == 1.0  # edgeless
+    assert O.stress([0.0, 1.0, 100.0, 101.0], [0.0] * 4, [0, 2], [1, 3]) == 0.0  # two components
+
+
+def test_oracle_bfs_hops_on_a_path_with_a_loop_and_a_stray_node():
+    h = O.bfs_hops(5, [0, 1, 2, 2], [1, 2, 3, 2], [0, 3])
+    none = np.iinfo(np.uint32).max
+    assert h[0].tolist() == [0, 1, 2, 3, none]
+    assert h[1].tolist() == [3, 2, 1, 0, none]
