@@ -443,6 +443,18 @@ def run_gpu(args, dist: Dist):
                "step": f"one layout call: create from host edges + {ran} ticks + positions back",
                "seconds": el}
 
+    # the reference's quality measure of that layout (graph-cli bench.rs stress), on the device
+    quality = None
+    if e2e is not None and dist.rank == 0:
+        from graph_render_b200 import stress as S
+
+        t0 = time.perf_counter()
+        s_end = S.kruskal_stress(out[:, 0], out[:, 1], wl.src, wl.dst, 16)
+        t_s = time.perf_counter() - t0
+        s_start = S.kruskal_stress(wl.pos0[:, 0], wl.pos0[:, 1], wl.src, wl.dst, 16)
+        quality = {"kruskal_stress": s_end, "start_stress": s_start, "after_ticks": ran, "bfs_sources": 16,
+                   "seconds": t_s, "how": "gr_stress: 16 evenly spaced BFS sources, every reachable target"}
+
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -486,6 +498,7 @@ def run_gpu(args, dist: Dist):
                                                            for i in range(len(WALK_SCHEDULE_NAMES))}}},
             "clocks": clocks,
             "e2e": e2e,
+            "quality": quality,
             "gpu_launches": int(info1["graph_kernels"]) * done,
             "roofline": {"kernel": "k_walk_s", "bound": "fp32", "achieved": achieved / 1e12,
                          "peak": fp32_peak / 1e12, "unit": "TFLOP/s", "frac": achieved / fp32_peak,

@@ -28,6 +28,7 @@
 #endif
 
 #define MAXD 3
+#define DBL_MIN_POS 2.2250738585072014e-308 /* f64::MIN_POSITIVE */
 
 /* ---------------------------------------------------------------- rng ---- */
 
@@ -209,6 +210,7 @@ typedef struct {
     int32_t root;
     int32_t *chain_next;
     tcell *cells;
+    int32_t *node_id; /* preorder cell -> its arena (shape) index, quadtree.rs node_id */
     size_t ncells, capcells;
     uint32_t *order;
     size_t norder;
@@ -377,11 +379,13 @@ static void tree_add(ttree *t, const double *pos, uint32_t point) {
     }
 }
 
-static void cell_push(ttree *t, const double *b0, const double *b1, uint32_t start) {
+static void cell_push(ttree *t, const double *b0, const double *b1, uint32_t start, int32_t node) {
     if (t->ncells == t->capcells) {
         t->capcells = t->capcells ? t->capcells * 2 : 1024;
         t->cells = (tcell *)realloc(t->cells, t->capcells * sizeof(tcell));
+        t->node_id = (int32_t *)realloc(t->node_id, t->capcells * sizeof(int32_t));
     }
+    t->node_id[t->ncells] = node;
     tcell *c = &t->cells[t->ncells++];
     memcpy(c->b0, b0, sizeof c->b0);
     memcpy(c->b1, b1, sizeof c->b1);
@@ -418,7 +422,7 @@ static void tree_flatten(ttree *t, const double *pos, uint32_t n) {
         }
         uint32_t k = (uint32_t)t->ncells;
         uint32_t start = (uint32_t)t->norder;
-        cell_push(t, v.b0, v.b1, start);
+        cell_push(t, v.b0, v.b1, start, v.node);
         tshape *s = &t->shape[v.node];
         if (s->head >= 0) {
             for (int32_t p = s->head; p >= 0; p = t->chain_next[p]) t->order[t->norder++] = (uint32_t)p;
@@ -560,6 +564,7 @@ void orc_fa2_free(orc_fa2 *s) {
     free(s->tree.shape);
     free(s->tree.chain_next);
     free(s->tree.cells);
+    free(s->tree.node_id);
     free(s->tree.order);
     free(s->tree.bodies);
     free(s);
@@ -1372,3 +1377,413 @@ void orc_bfs(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst, u
     free(adj);
     free(rp);
 }
+
+
+/* ============================================== d3-force Barnes-Hut ======= */
+/*
+ * The frozen d3-force layout of graph-core (crates/graph-core/src/layout/force/
+ * barnes_hut.rs, barnes_hut/{sim,seed,link,charge,collide}.rs, charge/{aggregate,
+ * threshold}.rs, params.rs, session.rs), restated in FP64 in the reference's
+ * operation order: golden-spiral start, then per tick alpha decay, link (Jacobi:
+ * every edge's force from the tick's state, then each node's shares in its row's
+ * order), many-body over the insertion quadtree of the positions (cell bodies in
+ * reverse preorder, the stackless walk with d3's `open >= l` test, distanceMin /
+ * distanceMax, jiggle keyed on the cell's arena index), center, collide over the
+ * quadtree of the projected positions, integrate. Each pass adds one delta per
+ * node to its velocity.
+ */
+
+typedef struct {
+    double charge, theta, distance_min, distance_max, link_distance, link_strength_scale, collide_radius,
+        center_strength, velocity_decay, alpha_decay, alpha_min, initial_alpha;
+} orc_d3_params;
+
+typedef struct {
+    double comx, comy, open;
+    uint32_t count, skip, start;
+} d3body;
+
+typedef struct {
+    orc_d3_params P;
+    uint32_t n, m, seed, tick_no;
+    double alpha;
+    uint32_t *lo, *hi;
+    double *dist, *stren, *bias;
+    uint32_t *rp, *rows; /* node -> its simple edges, ascending edge index */
+    double *x, *y, *vx, *vy, *px, *py, *pos, *dvx, *dvy, *fx, *fy;
+    ttree ct, kt; /* charge tree, collide tree */
+    d3body *bodies;
+} orc_d3;
+
+/* seed.rs spiral_point: radius 12 sqrt(i + 1), angle i * golden angle. */
+static void d3_spiral(uint32_t i, double *x, double *y) {
+    const double golden = 2.399963229728653;
+    double radius = 12.0 * sqrt((double)i + 1.0);
+    double angle = (double)i * golden;
+    *x = cos(angle) * radius;
+    *y = sin(angle) * radius;
+}
+
+/* params.rs:60-75 defaults (the production engine's values). */
+void orc_d3_default_params(orc_d3_params *p) {
+    p->charge = -90.0;
+    p->theta = 0.9;
+    p->distance_min = 1.0;
+    p->distance_max = 520.0;
+    p->link_distance = 60.0;
+    p->link_strength_scale = 0.15;
+    p->collide_radius = 16.0;
+    p->center_strength = 1.0;
+    p->velocity_decay = 1.0 - 0.42;
+    p->alpha_decay = 0.06;
+    p->alpha_min = 0.001;
+    p->initial_alpha = 1.0;
+}
+
+/* Sim::new over the simple graph (lo < hi, first-wins strength, edge order). A
+ * null pos0 starts from the golden spiral (seed.rs golden_spiral). */
+orc_d3 *orc_d3_new(uint32_t n, uint32_t m, const uint32_t *lo, const uint32_t *hi, const double *strength,
+                   const orc_d3_params *P, const double *pos0) {
+    orc_d3 *s = (orc_d3 *)calloc(1, sizeof(orc_d3));
+    s->P = *P;
+    s->n = n;
+    s->m = m;
+    s->alpha = P->initial_alpha;
+    size_t nn = n ? n : 1, mm = m ? m : 1;
+    s->lo = (uint32_t *)malloc(mm * 4);
+    s->hi = (uint32_t *)malloc(mm * 4);
+    s->dist = (double *)malloc(mm * 8);
+    s->stren = (double *)malloc(mm * 8);
+    s->bias = (double *)malloc(mm * 8);
+    s->fx = (double *)malloc(mm * 8);
+    s->fy = (double *)malloc(mm * 8);
+    memcpy(s->lo, lo, (size_t)m * 4);
+    memcpy(s->hi, hi, (size_t)m * 4);
+    /* mod.rs:177-180 row_csr: (lo[e], e), (hi[e], e) in edge order */
+    s->rp = (uint32_t *)calloc(nn + 1, 4);
+    for (uint32_t e = 0; e < m; e++) {
+        s->rp[lo[e] + 1]++;
+        s->rp[hi[e] + 1]++;
+    }
+    for (uint32_t i = 0; i < n; i++) s->rp[i + 1] += s->rp[i];
+    s->rows = (uint32_t *)malloc((2 * (size_t)m + 1) * 4);
+    uint32_t *fill = (uint32_t *)malloc(nn * 4);
+    for (uint32_t i = 0; i < n; i++) fill[i] = s->rp[i];
+    for (uint32_t e = 0; e < m; e++) {
+        s->rows[fill[lo[e]]++] = e;
+        s->rows[fill[hi[e]]++] = e;
+    }
+    free(fill);
+    /* link.rs edge_geometry: distance, strength, degree bias */
+    for (uint32_t e = 0; e < m; e++) {
+        double st = strength[e];
+        double dlo = (double)(s->rp[lo[e] + 1] - s->rp[lo[e]]), dhi = (double)(s->rp[hi[e] + 1] - s->rp[hi[e]]);
+        s->dist[e] = P->link_distance / fmax(0.4, st);
+        s->stren[e] = fmin(0.7, P->link_strength_scale * st);
+        s->bias[e] = dlo / (dlo + dhi);
+    }
+    s->x = (double *)malloc(nn * 8);
+    s->y = (double *)malloc(nn * 8);
+    s->vx = (double *)calloc(nn, 8);
+    s->vy = (double *)calloc(nn, 8);
+    s->px = (double *)calloc(nn, 8);
+    s->py = (double *)calloc(nn, 8);
+    s->dvx = (double *)calloc(nn, 8);
+    s->dvy = (double *)calloc(nn, 8);
+    s->pos = (double *)calloc(nn * MAXD, 8);
+    for (uint32_t i = 0; i < n; i++) {
+        if (pos0) {
+            s->x[i] = pos0[2 * i];
+            s->y[i] = pos0[2 * i + 1];
+        } else {
+            d3_spiral(i, &s->x[i], &s->y[i]);
+        }
+    }
+    return s;
+}
+
+void orc_d3_free(orc_d3 *s) {
+    if (!s) return;
+    ttree *ts[2] = {&s->ct, &s->kt};
+    for (int k = 0; k < 2; k++) {
+        free(ts[k]->shape);
+        free(ts[k]->chain_next);
+        free(ts[k]->cells);
+        free(ts[k]->node_id);
+        free(ts[k]->order);
+        free(ts[k]->bodies);
+    }
+    free(s->bodies);
+    free(s->lo);
+    free(s->hi);
+    free(s->dist);
+    free(s->stren);
+    free(s->bias);
+    free(s->fx);
+    free(s->fy);
+    free(s->rp);
+    free(s->rows);
+    free(s->x);
+    free(s->y);
+    free(s->vx);
+    free(s->vy);
+    free(s->px);
+    free(s->py);
+    free(s->dvx);
+    free(s->dvy);
+    free(s->pos);
+    free(s);
+}
+
+static void d3_tree(orc_d3 *s, ttree *t, const double *x, const double *y) {
+    for (uint32_t i = 0; i < s->n; i++) {
+        s->pos[(size_t)i * MAXD] = x[i];
+        s->pos[(size_t)i * MAXD + 1] = y[i];
+    }
+    tree_build(t, s->pos, s->n, 2, 0);
+}
+
+/* link.rs force / share + step.rs LinkPass::node_share + merge. */
+static void d3_link(orc_d3 *s) {
+    for (uint32_t e = 0; e < s->m; e++) {
+        uint32_t lo = s->lo[e], hi = s->hi[e];
+        double dx = (s->x[hi] + s->vx[hi]) - (s->x[lo] + s->vx[lo]);
+        double dy = (s->y[hi] + s->vy[hi]) - (s->y[lo] + s->vy[lo]);
+        if (dx == 0.0) dx = orc_jiggle(s->seed, s->tick_no, 0, lo, hi);
+        if (dy == 0.0) dy = orc_jiggle(s->seed, s->tick_no, 1, lo, hi);
+        double l = sqrt(dx * dx + dy * dy);
+        if (l == 0.0) {
+            s->fx[e] = s->fy[e] = 0.0;
+            continue;
+        }
+        double factor = (l - s->dist[e]) / l * s->alpha * s->stren[e];
+        s->fx[e] = dx * factor;
+        s->fy[e] = dy * factor;
+    }
+    for (uint32_t v = 0; v < s->n; v++) {
+        double ax = 0.0, ay = 0.0;
+        for (uint32_t q = s->rp[v]; q < s->rp[v + 1]; q++) {
+            uint32_t e = s->rows[q];
+            double b = s->bias[e];
+            if (s->hi[e] == v) {
+                ax += -s->fx[e] * b;
+                ay += -s->fy[e] * b;
+            } else {
+                ax += s->fx[e] * (1.0 - b);
+                ay += s->fy[e] * (1.0 - b);
+            }
+        }
+        s->vx[v] += ax;
+        s->vy[v] += ay;
+    }
+}
+
+/* threshold.rs opening_threshold. */
+static double d3_open(double w, double theta, double theta2) {
+    if (theta == 0.0) return INFINITY;
+    double naive = w * w / theta2;
+    if (!isnan(naive)) return naive;
+    if (!isfinite(theta)) return INFINITY;
+    double ratio = w / theta;
+    return isfinite(ratio) ? ratio * ratio : INFINITY;
+}
+
+/* charge.rs settle: 0 past distanceMax, a zero axis jiggled (passes 2, 3), l
+ * clamped up to distanceMin. Returns 0 when the term is dropped. */
+static int d3_settle(const orc_d3 *s, uint32_t i, uint32_t key, double *dx, double *dy, double *l) {
+    double dmin2 = s->P.distance_min * s->P.distance_min, dmax2 = s->P.distance_max * s->P.distance_max;
+    if (*l >= dmax2) return 0;
+    if (*dx == 0.0) {
+        *dx = orc_jiggle(s->seed, s->tick_no, 2, i, key);
+        *l += *dx * *dx;
+    }
+    if (*dy == 0.0) {
+        *dy = orc_jiggle(s->seed, s->tick_no, 3, i, key);
+        *l += *dy * *dy;
+    }
+    if (*l < dmin2) *l = sqrt(dmin2 * *l);
+    if (*l == 0.0) *l = dmin2 > DBL_MIN_POS ? dmin2 : DBL_MIN_POS;
+    return 1;
+}
+
+/* charge.rs: aggregate (reverse preorder) then node_delta for every node. */
+static void d3_charge(orc_d3 *s) {
+    ttree *t = &s->ct;
+    d3_tree(s, t, s->x, s->y);
+    size_t nc = t->ncells;
+    s->bodies = (d3body *)realloc(s->bodies, (nc ? nc : 1) * sizeof(d3body));
+    double theta = s->P.theta, theta2 = theta * theta;
+    for (size_t kk = nc; kk-- > 0;) {
+        const tcell *c = &t->cells[kk];
+        double cx, cy;
+        if (c->skip == kk + 1) {
+            uint32_t head = t->order[c->start];
+            cx = s->x[head];
+            cy = s->y[head];
+        } else {
+            double m = 0.0, sx = 0.0, sy = 0.0;
+            for (uint32_t ch = (uint32_t)kk + 1; ch < c->skip; ch = s->bodies[ch].skip) {
+                double cm = (double)s->bodies[ch].count;
+                m += cm;
+                sx += cm * s->bodies[ch].comx;
+                sy += cm * s->bodies[ch].comy;
+            }
+            cx = sx / m;
+            cy = sy / m;
+        }
+        d3body *b = &s->bodies[kk];
+        b->comx = cx;
+        b->comy = cy;
+        b->open = d3_open(c->b1[0] - c->b0[0], theta, theta2);
+        b->count = c->end - c->start;
+        b->skip = c->skip;
+        b->start = c->start;
+    }
+    double ca = s->P.charge * s->alpha;
+    for (uint32_t i = 0; i < s->n; i++) {
+        double xi = s->x[i], yi = s->y[i], ox = 0.0, oy = 0.0;
+        uint32_t k = 0;
+        while (k < nc) {
+            const d3body *b = &s->bodies[k];
+            double dx = b->comx - xi, dy = b->comy - yi;
+            double l = dx * dx + dy * dy;
+            double ddx = 0.0, ddy = 0.0;
+            uint32_t next;
+            if (b->open >= l) {
+                if (b->skip != k + 1) {
+                    k++;
+                    continue;
+                }
+                const uint32_t *chain = t->order + b->start;
+                if (d3_settle(s, i, chain[0], &dx, &dy, &l)) {
+                    for (uint32_t q = 0; q < b->count; q++) {
+                        if (chain[q] == i) continue;
+                        double f = s->P.charge * s->alpha / l;
+                        ddx += dx * f;
+                        ddy += dy * f;
+                    }
+                }
+                next = k + 1;
+            } else {
+                if (d3_settle(s, i, (uint32_t)t->node_id[k], &dx, &dy, &l)) {
+                    double m = (double)b->count;
+                    double f = m * s->P.charge * s->alpha / l;
+                    ddx = dx * f;
+                    ddy = dy * f;
+                }
+                next = b->skip;
+            }
+            ox += ddx;
+            oy += ddy;
+            k = next;
+        }
+        s->dvx[i] = ox;
+        s->dvy[i] = oy;
+    }
+    (void)ca;
+    for (uint32_t i = 0; i < s->n; i++) {
+        s->vx[i] += s->dvx[i];
+        s->vy[i] += s->dvy[i];
+    }
+}
+
+/* sim.rs center / center_shift. */
+static void d3_center(orc_d3 *s) {
+    if (s->n == 0) return;
+    double sx = 0.0, sy = 0.0;
+    for (uint32_t i = 0; i < s->n; i++) {
+        sx += s->x[i];
+        sy += s->y[i];
+    }
+    double dx = (sx / (double)s->n) * s->P.center_strength, dy = (sy / (double)s->n) * s->P.center_strength;
+    for (uint32_t i = 0; i < s->n; i++) {
+        s->x[i] -= dx;
+        s->y[i] -= dy;
+    }
+}
+
+/* collide.rs: tree over x + vx, every point within 2 r pushed apart by half. */
+static void d3_collide(orc_d3 *s) {
+    for (uint32_t i = 0; i < s->n; i++) {
+        s->px[i] = s->x[i] + s->vx[i];
+        s->py[i] = s->y[i] + s->vy[i];
+    }
+    ttree *t = &s->kt;
+    d3_tree(s, t, s->px, s->py);
+    double diameter = 2.0 * s->P.collide_radius, d2 = diameter * diameter, reach = sqrt(d2);
+    for (uint32_t i = 0; i < s->n; i++) {
+        double xi = s->px[i], yi = s->py[i], ox = 0.0, oy = 0.0;
+        uint32_t k = 0;
+        while (k < t->ncells) {
+            const tcell *c = &t->cells[k];
+            if (c->skip == k + 1) {
+                for (uint32_t q = c->start; q < c->end; q++) {
+                    uint32_t p = t->order[q];
+                    if (p == i) continue;
+                    double dx = xi - s->px[p], dy = yi - s->py[p];
+                    double l = dx * dx + dy * dy;
+                    if (l >= d2) continue;
+                    if (dx == 0.0) {
+                        dx = orc_jiggle(s->seed, s->tick_no, 4, i, p);
+                        l += dx * dx;
+                    }
+                    if (dy == 0.0) {
+                        dy = orc_jiggle(s->seed, s->tick_no, 5, i, p);
+                        l += dy * dy;
+                    }
+                    double dist = sqrt(l);
+                    double push = (reach - dist) / dist * 0.5;
+                    ox += dx * push;
+                    oy += dy * push;
+                }
+                k = k + 1;
+            } else if (c->b0[0] > xi + reach || c->b1[0] < xi - reach || c->b0[1] > yi + reach ||
+                       c->b1[1] < yi - reach) {
+                k = c->skip;
+            } else {
+                k = k + 1;
+            }
+        }
+        s->dvx[i] = ox;
+        s->dvy[i] = oy;
+    }
+    for (uint32_t i = 0; i < s->n; i++) {
+        s->vx[i] += s->dvx[i];
+        s->vy[i] += s->dvy[i];
+    }
+}
+
+/* sim.rs tick: alpha decay, link, charge, center, collide, integrate. */
+void orc_d3_tick(orc_d3 *s, uint32_t ticks) {
+    for (uint32_t t = 0; t < ticks; t++) {
+        s->alpha += (0.0 - s->alpha) * s->P.alpha_decay;
+        d3_link(s);
+        d3_charge(s);
+        d3_center(s);
+        d3_collide(s);
+        double decay = s->P.velocity_decay;
+        for (uint32_t i = 0; i < s->n; i++) {
+            s->vx[i] *= decay;
+            s->x[i] += s->vx[i];
+            s->vy[i] *= decay;
+            s->y[i] += s->vy[i];
+        }
+        s->tick_no++;
+    }
+}
+
+void orc_d3_positions(const orc_d3 *s, double *out) {
+    for (uint32_t i = 0; i < s->n; i++) {
+        out[2 * i] = s->x[i];
+        out[2 * i + 1] = s->y[i];
+    }
+}
+
+void orc_d3_velocities(const orc_d3 *s, double *out) {
+    for (uint32_t i = 0; i < s->n; i++) {
+        out[2 * i] = s->vx[i];
+        out[2 * i + 1] = s->vy[i];
+    }
+}
+
+double orc_d3_alpha(const orc_d3 *s) { return s->alpha; }

@@ -72,6 +72,15 @@ def lib():
     L.orc_stress.argtypes = [C.c_uint32, C.c_int64, u32p, u32p, f32p, f32p, C.c_uint32]
     L.orc_stress.restype = C.c_double
     L.orc_bfs.argtypes = [C.c_uint32, C.c_int64, u32p, u32p, C.c_uint32, u32p, u32p]
+    L.orc_d3_default_params.argtypes = [C.POINTER(D3Params)]
+    L.orc_d3_new.argtypes = [C.c_uint32, C.c_uint32, u32p, u32p, f64p, C.POINTER(D3Params), P]
+    L.orc_d3_new.restype = P
+    L.orc_d3_free.argtypes = [P]
+    L.orc_d3_tick.argtypes = [P, C.c_uint32]
+    L.orc_d3_positions.argtypes = [P, f64p]
+    L.orc_d3_velocities.argtypes = [P, f64p]
+    L.orc_d3_alpha.argtypes = [P]
+    L.orc_d3_alpha.restype = C.c_double
     L.orc_gate_edges.argtypes = [C.c_uint32, u32p, u32p, f64p, C.c_int64]
     L.orc_gate_edges.restype = C.c_int64
     L.orc_simple_graph.argtypes = [C.c_uint32, C.c_int64, u32p, u32p, P, u32p, u32p, f64p]
@@ -125,6 +134,60 @@ def gate_edges(count: int):
 def _nonempty_u32(a):
     a = np.ascontiguousarray(a, np.uint32)
     return a if len(a) else np.zeros(1, np.uint32)
+
+
+class D3Params(C.Structure):
+    """crates/graph-core/src/layout/force/params.rs ForceParams (defaults at 60-75)."""
+    _fields_ = [(k, C.c_double) for k in (
+        "charge", "theta", "distance_min", "distance_max", "link_distance", "link_strength_scale",
+        "collide_radius", "center_strength", "velocity_decay", "alpha_decay", "alpha_min", "initial_alpha")]
+
+
+D3_TICKS = 112  # params.rs TICKS: the least k with 0.94^k < 0.001
+
+
+def d3_params(**kw) -> D3Params:
+    p = D3Params()
+    lib().orc_d3_default_params(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, float(v))
+    return p
+
+
+class D3:
+    """The frozen d3-force Barnes-Hut layout (barnes_hut.rs) over a simple graph
+    (lo < hi, first-wins strength, simple_graph's edge order)."""
+
+    def __init__(self, n, lo, hi, strength, pos0=None, **kw):
+        self.n = int(n)
+        self._lo = _nonempty_u32(lo)
+        self._hi = _nonempty_u32(hi)
+        st = np.ascontiguousarray(strength, np.float64)
+        self._st = st if len(st) else np.zeros(1)
+        self.p = d3_params(**kw)
+        self._pos0 = None if pos0 is None else np.ascontiguousarray(pos0, np.float64).reshape(-1)
+        self.h = lib().orc_d3_new(self.n, len(lo), self._lo, self._hi, self._st, C.byref(self.p), _ptr(self._pos0))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_d3_free(self.h)
+            self.h = None
+
+    def tick(self, ticks: int = 1) -> None:
+        lib().orc_d3_tick(self.h, ticks)
+
+    def positions(self) -> np.ndarray:
+        out = np.zeros(2 * max(self.n, 1))
+        lib().orc_d3_positions(self.h, out)
+        return out[:2 * self.n].reshape(self.n, 2)
+
+    def velocities(self) -> np.ndarray:
+        out = np.zeros(2 * max(self.n, 1))
+        lib().orc_d3_velocities(self.h, out)
+        return out[:2 * self.n].reshape(self.n, 2)
+
+    def alpha(self) -> float:
+        return lib().orc_d3_alpha(self.h)
 
 
 def stress(x, y, src, dst, sources: int = 16) -> float:
