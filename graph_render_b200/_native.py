@@ -88,6 +88,17 @@ SIGNATURES = {
     "gr_run": ([C.c_char_p, C.c_uint32, C.c_uint64, u32p, u32p, f64p, u8p, C.c_size_t, f32p], C.c_int),
     "gr_fa2_forces_static": ([C.c_uint32, P, P, P, P, u8p, C.c_size_t, C.c_uint32, P, P], C.c_int),
     "gr_bfs_hops": ([C.c_uint32, C.c_uint64, P, P, C.c_uint32, P, P], C.c_int),
+    "gr_force_default_params": ([P], None),
+    "gr_force_session_create": ([P, C.c_uint32, C.c_uint64, P, P, P, P, P], C.c_int),
+    "gr_force_session_destroy": ([P], None),
+    "gr_force_session_tick": ([P, C.c_uint32], C.c_int),
+    "gr_force_session_positions": ([P, P], C.c_int),
+    "gr_force_session_velocities": ([P, P], C.c_int),
+    "gr_force_session_alpha": ([P, C.POINTER(C.c_double), C.POINTER(C.c_uint32)], C.c_int),
+    "gr_force_session_reheat": ([P, C.c_double], C.c_int),
+    "gr_force_session_info": ([P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)], C.c_int),
+    "gr_force_session_set_state": ([P, P, P, C.c_double, C.c_uint32], C.c_int),
+    "gr_force_run": ([C.c_uint32, C.c_uint64, P, P, P, P], C.c_int),
     "gr_stress": ([C.c_uint32, C.c_uint64, P, P, P, P, C.c_uint32, C.POINTER(C.c_double)], C.c_int),
     "gr_fa2_batch_create": ([C.POINTER(P), C.c_uint32, P, P, P, P, P, P, C.c_uint32, P], C.c_int),
     "gr_fa2_batch_destroy": ([P], None),

@@ -88,6 +88,7 @@ __host__ __device__ inline size_t slot_carve(unsigned char *base, uint32_t nmax,
     v.cells.A = slot_take<float4>(base, off, 2 * n);
     v.cells.B = slot_take<float4>(base, off, 2 * n);
     v.cells.C = D == 3 ? slot_take<int2>(base, off, 2 * n) : nullptr;
+    v.cells.bounds = nullptr;
     v.rep = slot_take<float>(base, off, n * D);
     v.U = slot_take<float>(base, off, n * D);
     v.att = slot_take<float>(base, off, n * D);

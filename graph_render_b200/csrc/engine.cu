@@ -30,6 +30,7 @@
 #include "batch.cuh"
 #include "adjoint.cuh"
 #include "stress.cuh"
+#include "d3force.cuh"
 
 using namespace gr;
 
@@ -630,9 +631,9 @@ int gr_last_error(void) { return g_err; }
 const char *gr_last_error_message(void) { return g_msg; }
 int gr_last_error_index(void) { return g_err_index; }
 
-static const char *kLayouts[] = {"layout.forceatlas2.barnes_hut.cuda"};
+static const char *kLayouts[] = {"layout.forceatlas2.barnes_hut.cuda", "layout.force.barnes_hut.cuda"};
 
-uint32_t gr_layout_count(void) { return 1; }
+uint32_t gr_layout_count(void) { return 2; }
 const char *gr_layout_id(uint32_t i) {
     if (i >= gr_layout_count()) {
         set_err(GR_INDEX_OUT_OF_RANGE, "layout index past the end");
@@ -924,6 +925,11 @@ int gr_fa2_set_stream(gr_fa2 *h, void *cuda_stream) {
 
 int gr_run(const char *layout_id, uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
            const double *weight, const uint8_t *params, size_t params_len, float *out) {
+    if (layout_id && strcmp(layout_id, kLayouts[1]) == 0) {
+        // the d3-force row publishes no parameters (registry/layouts.rs LayoutParams::NONE)
+        if (params_len) return set_err(GR_PARAMS_NOT_ACCEPTED, "layout.force.barnes_hut.cuda takes no parameters");
+        return gr_force_run(n, m, src, dst, weight, out);
+    }
     if (!layout_id || strcmp(layout_id, kLayouts[0]) != 0)
         return set_err(GR_UNKNOWN_LAYOUT_ID, "unknown layout id");
     gr_fa2 *h = nullptr;
@@ -1817,6 +1823,299 @@ int gr_stress(uint32_t n, uint64_t m, const uint32_t *source, const uint32_t *ta
     if (ee == 0.0 || dd == 0.0) return ok();
     *out = std::sqrt(std::max((dd - de / ee * de) / dd, 0.0));
     return ok();
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------- d3-force session ----
+//
+// A d3-force Barnes-Hut session (d3force.cuh) over an internal FA2 handle that
+// holds the simple graph (CSR, edge strengths as weights, heavy-row segments),
+// the stream and the tree buffers; every tick is one captured CUDA graph that
+// builds the tree twice (positions for many-body, projected positions for
+// collide).
+
+struct gr_force_session {
+    gr_fa2 *t = nullptr;
+    uint32_t n = 0;
+    gr_force_params prm{};
+    D3Params P{};
+    float4 *p4 = nullptr, *pp4 = nullptr, *bounds = nullptr;
+    float2 *vel = nullptr, *seg_out = nullptr;
+    D3State *ds = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t graph_kernels = 0;
+    ~gr_force_session() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (t) {
+            if (t->stream) cudaStreamSynchronize(t->stream);
+            delete t;  // also frees the session's buffers (allocated through t)
+        }
+    }
+};
+
+namespace {
+
+int d3_validate(const gr_force_params &p) {
+    const double v[] = {p.charge, p.theta, p.distance_min, p.distance_max, p.link_distance, p.link_strength_scale,
+                        p.collide_radius, p.center_strength, p.velocity_decay, p.alpha_decay, p.alpha_min,
+                        p.initial_alpha};
+    for (size_t i = 0; i < sizeof v / sizeof v[0]; i++)
+        if (!std::isfinite(v[i])) return set_err(GR_PARAM_OUT_OF_RANGE, "force parameter not finite", (int)i);
+    if (p.theta < 0.0) return set_err(GR_PARAM_OUT_OF_RANGE, "theta must be >= 0", 1);
+    if (p.distance_min < 0.0 || p.distance_max < 0.0)
+        return set_err(GR_PARAM_OUT_OF_RANGE, "distances must be >= 0", 2);
+    if (p.initial_alpha < 0.0 || p.initial_alpha > 1.0)
+        return set_err(GR_PARAM_OUT_OF_RANGE, "initial alpha must be in [0, 1]", 11);
+    return GR_OK;
+}
+
+void d3_enqueue(gr_force_session *S) {
+    gr_fa2 *t = S->t;
+    cudaStream_t s = t->stream;
+    const uint32_t n = S->n, g = div_up(n, D3_T);
+    k_d3_alpha<<<1, 1, 0, s>>>(S->ds, S->prm.alpha_decay);
+    k_d3_project<<<g, D3_T, 0, s>>>(n, S->p4, S->vel, S->pp4);
+    if (t->nseg)
+        k_d3_link_seg<<<div_up((uint64_t)t->nseg * GR_WARP, D3_T), D3_T, 0, s>>>(
+            S->P, t->nseg, S->ds, S->pp4, t->rp, t->col, t->wt, t->seg_row, t->seg_first, S->seg_out);
+    k_d3_link<<<g, D3_T, 0, s>>>(S->P, S->ds, S->pp4, t->rp, t->col, t->wt, t->nseg ? t->seg_first : nullptr,
+                                 S->seg_out, S->vel);
+    t->pos = S->p4;  // many-body: the tree of the positions
+    enqueue_tick<2>(t, false, PH_TREE);
+    k_d3_charge<<<g, D3_T, 0, s>>>(S->P, S->ds, t->st, t->cells, t->sp, t->sorig, S->vel);
+    k_d3_center<<<g, D3_T, 0, s>>>(n, (float)S->prm.center_strength, t->st, S->p4);
+    k_d3_project<<<g, D3_T, 0, s>>>(n, S->p4, S->vel, S->pp4);
+    t->pos = S->pp4;  // collide: the tree of the projected positions, with cell squares
+    t->cells.bounds = S->bounds;
+    enqueue_tick<2>(t, false, PH_TREE);
+    Cells cb = t->cells;
+    t->cells.bounds = nullptr;
+    t->pos = S->p4;
+    k_d3_collide<<<g, D3_T, 0, s>>>(S->P, S->ds, t->st, cb, t->sp, t->sorig, S->vel);
+    k_d3_integrate<<<g, D3_T, 0, s>>>(n, (float)S->prm.velocity_decay, S->p4, S->vel);
+    k_d3_end<<<1, 1, 0, s>>>(S->ds);
+}
+
+int d3_build_graph(gr_force_session *S) {
+    if (S->exec) return GR_OK;
+    cudaStream_t s = S->t->stream;
+    CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    d3_enqueue(S);
+    cudaGraph_t g = nullptr;
+    CU(cudaStreamEndCapture(s, &g));
+    S->graph = g;
+    size_t count = 0;
+    CU(cudaGraphGetNodes(g, nullptr, &count));
+    std::vector<cudaGraphNode_t> nodes(count);
+    CU(cudaGraphGetNodes(g, nodes.data(), &count));
+    S->graph_kernels = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType ty;
+        CU(cudaGraphNodeGetType(nd, &ty));
+        if (ty == cudaGraphNodeTypeKernel) S->graph_kernels++;
+    }
+    CU(cudaGraphInstantiate(&S->exec, g, 0));
+    return GR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void gr_force_default_params(gr_force_params *p) {
+    if (!p) return;
+    // crates/graph-core/src/layout/force/params.rs:60-75
+    p->charge = -90.0;
+    p->theta = 0.9;
+    p->distance_min = 1.0;
+    p->distance_max = 520.0;
+    p->link_distance = 60.0;
+    p->link_strength_scale = 0.15;
+    p->collide_radius = 16.0;
+    p->center_strength = 1.0;
+    p->velocity_decay = 1.0 - 0.42;
+    p->alpha_decay = 0.06;
+    p->alpha_min = 0.001;
+    p->initial_alpha = 1.0;
+}
+
+int gr_force_session_create(gr_force_session **out, uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                            const double *strength, const gr_force_params *params, const float *pos0) {
+    if (!out) return set_err(GR_INVALID_ARGUMENT, "out is null");
+    *out = nullptr;
+    gr_force_params prm;
+    gr_force_default_params(&prm);
+    if (params) prm = *params;
+    if (int c = d3_validate(prm)) return c;
+    if (pos0)
+        for (size_t i = 0; i < 2 * (size_t)n; i++)
+            if (!std::isfinite(pos0[i])) return set_err(GR_INVALID_ARGUMENT, "non-finite start position");
+    if (strength)
+        for (uint64_t e = 0; e < m; e++)
+            if (!std::isfinite(strength[e])) return set_err(GR_INVALID_ARGUMENT, "non-finite edge strength", (int)e);
+    // the internal FA2 handle: 2D, edge strengths as the CSR weights (influence 1)
+    double fv[11] = {100, 1.0, 2.0, 1.0, 0, 2, 0.8, 0, 0, 0, 1.0};
+    uint8_t fb[sizeof fv];
+    memcpy(fb, fv, sizeof fv);
+    gr_fa2 *t = nullptr;
+    if (int c = create_impl(&t, n, m, src, dst, strength, fb, sizeof fb, nullptr)) return c;
+    gr_force_session *S = new (std::nothrow) gr_force_session();
+    if (!S) {
+        delete t;
+        return set_err(GR_ALLOC_FAILED, "host allocation failed");
+    }
+    S->t = t;
+    S->n = n;
+    S->prm = prm;
+    D3Params &P = S->P;
+    P.n = n;
+    P.seed = 0;  // session.rs:78 SEED
+    P.charge = (float)prm.charge;
+    P.th2 = (float)(prm.theta * prm.theta);
+    P.dmin2 = (float)(prm.distance_min * prm.distance_min);
+    P.dmax2 = (float)(prm.distance_max * prm.distance_max);
+    P.link_distance = (float)prm.link_distance;
+    P.link_strength_scale = (float)prm.link_strength_scale;
+    const double diameter = 2.0 * prm.collide_radius;
+    P.reach2 = (float)(diameter * diameter);
+    P.reach = (float)std::sqrt(diameter * diameter);
+    P.center_strength = (float)prm.center_strength;
+    P.velocity_decay = (float)prm.velocity_decay;
+    P.alpha_decay = prm.alpha_decay;
+    cudaError_t e;
+    if ((e = t->alloc(&S->p4, n)) || (e = t->alloc(&S->pp4, n)) || (e = t->alloc(&S->bounds, 2 * (size_t)n)) ||
+        (e = t->alloc(&S->vel, n)) || (e = t->alloc(&S->seg_out, std::max<uint32_t>(t->nseg, 1))) ||
+        (e = t->alloc(&S->ds, 1))) {
+        delete S;
+        return set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+    }
+    // seed.rs golden_spiral: radius 12 sqrt(i + 1), angle i * golden angle, FP64 then narrowed
+    std::vector<float4> host(n);
+    for (uint32_t i = 0; i < n; i++) {
+        double x, y;
+        if (pos0) {
+            x = pos0[2 * (size_t)i];
+            y = pos0[2 * (size_t)i + 1];
+        } else {
+            const double radius = 12.0 * std::sqrt((double)i + 1.0), angle = (double)i * 2.399963229728653;
+            x = std::cos(angle) * radius;
+            y = std::sin(angle) * radius;
+        }
+        host[i] = make_float4((float)x, (float)y, 0.f, 1.f);
+    }
+    D3State d0{prm.initial_alpha, 0.0, 0u, 0u};
+    cudaStream_t s = t->stream;
+    if (n) {
+        CU(cudaMemcpyAsync(S->p4, host.data(), (size_t)n * sizeof(float4), cudaMemcpyHostToDevice, s));
+        CU(cudaMemsetAsync(S->vel, 0, (size_t)n * sizeof(float2), s));
+    }
+    CU(cudaMemcpyAsync(S->ds, &d0, sizeof d0, cudaMemcpyHostToDevice, s));
+    CU(cudaStreamSynchronize(s));
+    *out = S;
+    return ok();
+}
+
+void gr_force_session_destroy(gr_force_session *S) { delete S; }
+
+int gr_force_session_tick(gr_force_session *S, uint32_t ticks) {
+    if (!S) return set_err(GR_INVALID_HANDLE, "null session");
+    if (S->n == 0 || ticks == 0) return ok();
+    if (int c = d3_build_graph(S)) return c;
+    for (uint32_t k = 0; k < ticks; k++) CU(cudaGraphLaunch(S->exec, S->t->stream));
+    DevState st;
+    if (int c = read_state(S->t, &st)) return c;
+    if (int c = check_device(S->t, st)) return c;
+    return ok();
+}
+
+int gr_force_session_positions(gr_force_session *S, float *out) {
+    if (!S) return set_err(GR_INVALID_HANDLE, "null session");
+    if (!out && S->n) return set_err(GR_INVALID_ARGUMENT, "out is null");
+    std::vector<float4> host(S->n);
+    if (S->n) CU(cudaMemcpyAsync(host.data(), S->p4, (size_t)S->n * sizeof(float4), cudaMemcpyDeviceToHost, S->t->stream));
+    CU(cudaStreamSynchronize(S->t->stream));
+    for (uint32_t i = 0; i < S->n; i++) {
+        out[2 * (size_t)i] = host[i].x;
+        out[2 * (size_t)i + 1] = host[i].y;
+        if (!std::isfinite(host[i].x) || !std::isfinite(host[i].y))
+            return set_err(GR_LAYOUT_FAILED, "non-finite position (StageError::NonFinite)");
+    }
+    return ok();
+}
+
+int gr_force_session_velocities(gr_force_session *S, float *out) {
+    if (!S) return set_err(GR_INVALID_HANDLE, "null session");
+    if (!out && S->n) return set_err(GR_INVALID_ARGUMENT, "out is null");
+    if (S->n) CU(cudaMemcpyAsync(out, S->vel, (size_t)S->n * sizeof(float2), cudaMemcpyDeviceToHost, S->t->stream));
+    CU(cudaStreamSynchronize(S->t->stream));
+    return ok();
+}
+
+int gr_force_session_alpha(gr_force_session *S, double *alpha, uint32_t *ticks_done) {
+    if (!S) return set_err(GR_INVALID_HANDLE, "null session");
+    D3State d;
+    CU(cudaMemcpyAsync(&d, S->ds, sizeof d, cudaMemcpyDeviceToHost, S->t->stream));
+    CU(cudaStreamSynchronize(S->t->stream));
+    if (alpha) *alpha = d.alpha;
+    if (ticks_done) *ticks_done = d.tick_no;
+    return ok();
+}
+
+int gr_force_session_reheat(gr_force_session *S, double alpha) {
+    if (!S) return set_err(GR_INVALID_HANDLE, "null session");
+    if (!std::isfinite(alpha) || alpha < 0.0 || alpha > 1.0)
+        return set_err(GR_PARAM_OUT_OF_RANGE, "alpha must be a finite value in [0, 1]");
+    CU(cudaMemcpyAsync(&S->ds->alpha, &alpha, sizeof alpha, cudaMemcpyHostToDevice, S->t->stream));
+    CU(cudaStreamSynchronize(S->t->stream));
+    return ok();
+}
+
+int gr_force_session_set_state(gr_force_session *S, const float *pos, const float *vel, double alpha,
+                               uint32_t ticks_done) {
+    if (!S) return set_err(GR_INVALID_HANDLE, "null session");
+    if (!std::isfinite(alpha) || alpha < 0.0 || alpha > 1.0)
+        return set_err(GR_PARAM_OUT_OF_RANGE, "alpha must be a finite value in [0, 1]");
+    const size_t n = S->n;
+    for (size_t i = 0; i < 2 * n; i++)
+        if ((pos && !std::isfinite(pos[i])) || (vel && !std::isfinite(vel[i])))
+            return set_err(GR_INVALID_ARGUMENT, "non-finite position or velocity", (int)(i / 2));
+    cudaStream_t s = S->t->stream;
+    std::vector<float4> host(n);
+    if (pos && n) {
+        for (size_t i = 0; i < n; i++) host[i] = make_float4(pos[2 * i], pos[2 * i + 1], 0.f, 1.f);
+        CU(cudaMemcpyAsync(S->p4, host.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s));
+    }
+    if (vel && n) CU(cudaMemcpyAsync(S->vel, vel, n * sizeof(float2), cudaMemcpyHostToDevice, s));
+    D3State d;
+    CU(cudaMemcpyAsync(&d, S->ds, sizeof d, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    d.alpha = alpha;
+    d.tick_no = ticks_done;
+    CU(cudaMemcpyAsync(S->ds, &d, sizeof d, cudaMemcpyHostToDevice, s));
+    CU(cudaStreamSynchronize(s));
+    return ok();
+}
+
+int gr_force_session_info(gr_force_session *S, uint32_t *graph_kernels, uint32_t *n_cells) {
+    if (!S) return set_err(GR_INVALID_HANDLE, "null session");
+    if (graph_kernels) *graph_kernels = S->graph_kernels;
+    DevState st;
+    if (int c = read_state(S->t, &st)) return c;
+    if (n_cells) *n_cells = st.n_cells;
+    return ok();
+}
+
+int gr_force_run(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst, const double *strength,
+                 float *out) {
+    gr_force_session *S = nullptr;
+    if (int c = gr_force_session_create(&S, n, m, src, dst, strength, nullptr, nullptr)) return c;
+    int c = gr_force_session_tick(S, GR_FORCE_TICKS);
+    if (c == GR_OK) c = gr_force_session_positions(S, out);
+    delete S;
+    return c;
 }
 
 }  // extern "C"

@@ -642,7 +642,18 @@ __global__ void k_count(const DevState *st, BinTree t, uint32_t *__restrict__ ce
 struct Cells {
     float4 *A, *B;
     int2 *C;
+    float4 *bounds;  // nullable: each cell's square {x0, y0, x1, y1} (2D), for range pruning
 };
+
+// The square of the level-`level` cell holding point p: the root corner plus
+// floor((p - corner) / w) sides, exact in FP64 (w is a power of two times the
+// root side). Rounded to FP32 it still contains every point of the cell.
+__device__ __forceinline__ void write_bounds(Cells c, uint32_t idx, const float4 &p, int level, const DevState *st) {
+    const double w = ldexp(st->root_w, -level);
+    const double bx = st->root0[0] + floor(((double)p.x - st->root0[0]) / w) * w;
+    const double by = st->root0[1] + floor(((double)p.y - st->root0[1]) / w) * w;
+    c.bounds[idx] = make_float4((float)bx, (float)by, (float)(bx + w), (float)(by + w));
+}
 
 template <int D>
 __device__ __forceinline__ void write_cell(Cells c, uint32_t idx, const Body &b, int level, double root_w,
@@ -733,6 +744,7 @@ __global__ void k_assign_dd(const DevState *st, BinTree t, const float4 *__restr
     bool coinc;
     write_cell<D>(cells, idx, leaf_sum<D>(sp, a0, a1, coinc), level, rw, -(int32_t)(a1 - a0), a0,
                   a1 - a0 == 1 ? &one : nullptr);
+    if (D == 2 && cells.bounds) write_bounds(cells, idx, one, level, st);
     leaf_pre[s] = idx;
     if (par >= 0 && R.x == (int)s) {
         const BodyDD ps = prefix[s];
@@ -743,6 +755,7 @@ __global__ void k_assign_dd(const DevState *st, BinTree t, const float4 *__restr
                 const uint32_t end = (uint32_t)R.y + 1;
                 const uint32_t skip = end == nu ? ncells : P[end];
                 write_cell<D>(cells, idx, range_body(ps, prefix[end]), R.w / D, rw, (int32_t)skip, a0);
+                if (D == 2 && cells.bounds) write_bounds(cells, idx, one, R.w / D, st);
                 if (t.cell_of) t.cell_of[par] = idx;
             }
             if (R.z < 0 || Q.x != (int)s) break;

@@ -235,6 +235,20 @@ FA2_META = Metadata(
     degradation="past device memory the create call refuses with GR_ALLOC_FAILED",
 )
 
+D3_ID = "layout.force.barnes_hut.cuda"
+
+D3_META = Metadata(
+    tier=1,
+    stage="layout",
+    oracle=("the FP64 CPU restatement of graph-core's layout.force.barnes_hut (oracle/, orc_d3_*), itself "
+            "reproducing the reference's 65 frozen-layout digests and 8 snapshot hashes bit for bit; the "
+            "FP32 GPU tick against it pass by pass, the layout's stress against it at the end"),
+    complexity="O(n log n) per tick x 112 ticks: two Morton trees (positions, projected positions), "
+               "link as a CSR gather",
+    scale_ceiling=50_000_000,
+    degradation="past device memory the create call refuses with GR_ALLOC_FAILED",
+)
+
 _LAYOUTS: Optional[List[Capability]] = None
 
 
@@ -246,8 +260,13 @@ def layouts() -> List[Capability]:
 
         specs = _native_specs()
         view = ParamsView(specs, accepted_lengths=(5,))
+        from . import d3force
+
+        none = ParamsView([])  # registry/layouts.rs: LayoutParams::NONE
         _LAYOUTS = [Capability(FA2_ID, run=lambda t: fa2.run_values(t, view.defaults()), params=view,
-                               meta=FA2_META, run_with=fa2.run_values)]
+                               meta=FA2_META, run_with=fa2.run_values),
+                    Capability(D3_ID, run=lambda t: d3force.run_values(t, []), params=none, meta=D3_META,
+                               run_with=d3force.run_values)]
     return _LAYOUTS
 
 

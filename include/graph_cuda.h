@@ -191,6 +191,45 @@ int gr_bfs_hops(uint32_t n, uint64_t m, const uint32_t *source, const uint32_t *
 int gr_stress(uint32_t n, uint64_t m, const uint32_t *source, const uint32_t *target, const float *x, const float *y,
               uint32_t sources, double *out);
 
+/* d3-force Barnes-Hut session (2D), the layout behind graph-core's
+ * `layout.force.barnes_hut` (crates/graph-core/src/layout/force/barnes_hut.rs,
+ * barnes_hut/sim.rs:170-270 tick) and the per-tick surface of the reference's live
+ * session (crates/graph-core/src/layout/force/session.rs; graph-wasm
+ * gm_force_session_*, docs/contract/wasm-abi.md): link, many-body over the
+ * quadtree, center, collide, integrate, from the golden spiral (seed.rs) unless
+ * pos0 (n x 2) is given. FP32 positions and velocities on the device.
+ * gr_force_params mirrors params.rs ForceParams; gr_force_default_params fills its
+ * defaults (params.rs:60-75), and a NULL params means those. strength (m, NULL:
+ * 1) is each raw edge's strength; the first raw edge of a pair keeps it. */
+typedef struct gr_force_session gr_force_session;
+typedef struct gr_force_params {
+    double charge, theta, distance_min, distance_max, link_distance, link_strength_scale, collide_radius,
+        center_strength, velocity_decay, alpha_decay, alpha_min, initial_alpha;
+} gr_force_params;
+#define GR_FORCE_TICKS 112 /* params.rs TICKS: the frozen layout's tick count */
+void gr_force_default_params(gr_force_params *out);
+int gr_force_session_create(gr_force_session **out, uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                            const double *strength, const gr_force_params *params, const float *pos0);
+void gr_force_session_destroy(gr_force_session *s);
+int gr_force_session_tick(gr_force_session *s, uint32_t ticks);
+int gr_force_session_positions(gr_force_session *s, float *out);
+int gr_force_session_velocities(gr_force_session *s, float *out);
+/* alpha after the ticks so far, and how many ticks have run. */
+int gr_force_session_alpha(gr_force_session *s, double *alpha, uint32_t *ticks_done);
+/* session.rs:247-251 reheat: alpha set outright, a finite value in [0, 1], never clamped. */
+int gr_force_session_reheat(gr_force_session *s, double alpha);
+/* Carries a state into the session (the reference session's columns handed over,
+ * session/carry.rs): positions and velocities (n x 2 each; NULL keeps the session's
+ * own), alpha (a finite value in [0, 1]) and the tick count the jiggle is keyed on. */
+int gr_force_session_set_state(gr_force_session *s, const float *pos, const float *vel, double alpha,
+                               uint32_t ticks_done);
+/* Kernels in the captured tick graph, and the cell count of the last tree. */
+int gr_force_session_info(gr_force_session *s, uint32_t *graph_kernels, uint32_t *n_cells);
+/* The frozen layout (BarnesHut::run, barnes_hut.rs:134-140): default parameters,
+ * GR_FORCE_TICKS ticks from the golden spiral, positions (n x 2) into out. */
+int gr_force_run(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst, const double *strength,
+                 float *out);
+
 /* The stream every call of this handle enqueues on (default: the handle's own). */
 int gr_fa2_set_stream(gr_fa2 *h, void *cuda_stream);
 

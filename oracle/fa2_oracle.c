@@ -1787,3 +1787,15 @@ void orc_d3_velocities(const orc_d3 *s, double *out) {
 }
 
 double orc_d3_alpha(const orc_d3 *s) { return s->alpha; }
+
+/* Replaces positions and velocities (n x 2 each), alpha and the tick count. */
+void orc_d3_set_state(orc_d3 *s, const double *pos, const double *vel, double alpha, uint32_t tick_no) {
+    for (uint32_t i = 0; i < s->n; i++) {
+        s->x[i] = pos[2 * i];
+        s->y[i] = pos[2 * i + 1];
+        s->vx[i] = vel[2 * i];
+        s->vy[i] = vel[2 * i + 1];
+    }
+    s->alpha = alpha;
+    s->tick_no = tick_no;
+}

@@ -81,6 +81,7 @@ def lib():
     L.orc_d3_velocities.argtypes = [P, f64p]
     L.orc_d3_alpha.argtypes = [P]
     L.orc_d3_alpha.restype = C.c_double
+    L.orc_d3_set_state.argtypes = [P, f64p, f64p, C.c_double, C.c_uint32]
     L.orc_gate_edges.argtypes = [C.c_uint32, u32p, u32p, f64p, C.c_int64]
     L.orc_gate_edges.restype = C.c_int64
     L.orc_simple_graph.argtypes = [C.c_uint32, C.c_int64, u32p, u32p, P, u32p, u32p, f64p]
@@ -188,6 +189,10 @@ class D3:
 
     def alpha(self) -> float:
         return lib().orc_d3_alpha(self.h)
+
+    def set_state(self, pos, vel, alpha: float, tick_no: int) -> None:
+        lib().orc_d3_set_state(self.h, np.ascontiguousarray(pos, np.float64).reshape(-1),
+                               np.ascontiguousarray(vel, np.float64).reshape(-1), float(alpha), int(tick_no))
 
 
 def stress(x, y, src, dst, sources: int = 16) -> float:

@@ -46,11 +46,14 @@ def test_static_library_is_built_beside_the_shared_one():
 def test_abi_version_and_registry_face():
     L = N.lib()
     assert L.gr_abi_version() == 1
-    assert L.gr_layout_count() == 1
+    assert L.gr_layout_count() == 2
+    assert [L.gr_layout_id(i).decode() for i in range(2)] == [
+        "layout.forceatlas2.barnes_hut.cuda", "layout.force.barnes_hut.cuda"]
     assert L.gr_layout_id(0) == FA2_ID.encode()
-    assert L.gr_layout_id(1) is None
+    assert L.gr_layout_id(2) is None
     assert L.gr_last_error() == N.GR_INDEX_OUT_OF_RANGE
-    assert [c.id for c in layouts()] == [FA2_ID]
+    assert [c.id for c in layouts()] == [FA2_ID, "layout.force.barnes_hut.cuda"]
+    assert find("layout.force.barnes_hut.cuda").params.is_empty()
 
 
 def test_schema_starts_with_the_reference_fa2_schema():
@@ -151,3 +154,11 @@ def test_static_entry_point_refuses_oversize_without_touching_a_device():
     assert rc == N.GR_INVALID_ARGUMENT
     rc = N.lib().gr_fa2_forces_static(10, None, None, None, None, C.c_char_p(b"\0" * 8), 8, 0, None, None)
     assert rc == N.GR_PARAMS_MALFORMED
+
+
+def test_d3_row_refuses_parameters_before_any_device_work():
+    from graph_render_b200 import D3_ID, StageError, Topology
+
+    with pytest.raises(StageError) as e:
+        find(D3_ID).run_params(Topology(3, [0, 1], [1, 2]), b"\0" * 8)
+    assert e.value.code == N.GR_PARAMS_NOT_ACCEPTED
