@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-3d", action="store_true")
+    ap.add_argument("--no-d3", action="store_true")
     ap.add_argument("--batched-graphs", type=int, default=4096, help="graphs per GPU")
     ap.add_argument("--batched-ticks", type=int, default=200)
     ap.add_argument("--batched-sample", type=int, default=48, help="graphs timed one launch sequence each")
@@ -373,6 +374,43 @@ def run_3d(args, dist: Dist):
                               "tuned_walk_ms": {WALK_SCHEDULE_NAMES[i]: v for i, v in tuned.items()}}}
 
 
+def run_d3(args, dist: Dist):
+    """The d3-force Barnes-Hut session (layout.force.barnes_hut.cuda) on the
+    reference's benchmark model at 1M nodes (synthetic.rs, the graph of its
+    `tick --n 1000000` bench): ms per tick after 3 warm-up ticks, then the whole
+    frozen layout (112 ticks from the golden spiral) and its stress."""
+    from graph_render_b200 import ForceSession, stress as S, synth
+
+    n = 1_000_000
+    src, dst, st = synth.gate(n)
+    t0 = time.perf_counter()
+    with ForceSession(n, src, dst, st) as s:
+        create_s = time.perf_counter() - t0
+        s.tick(3)
+        T = 20
+        t0 = time.perf_counter()
+        s.tick(T)  # returns after the device finished the ticks
+        tick_ms = (time.perf_counter() - t0) * 1e3 / T
+        info = s.info()
+    t0 = time.perf_counter()
+    with ForceSession(n, src, dst, st) as s:
+        t1 = time.perf_counter()
+        s.tick(1)  # captures the tick graph
+        t2 = time.perf_counter()
+        s.tick(111)
+        t3 = time.perf_counter()
+        p = s.positions()
+        t4 = time.perf_counter()
+    frozen_s = t4 - t0
+    frozen = {"create_s": t1 - t0, "first_tick_s": t2 - t1, "ticks_2_112_s": t3 - t2, "positions_s": t4 - t3}
+    return {"workload": f"gate model, {n} nodes, {len(src)} raw edges (the reference's synthetic benchmark graph)",
+            "ms_per_tick": tick_ms, "node_ticks_per_s": n / (tick_ms / 1e3), "graph_kernels": info["graph_kernels"],
+            "create_s": create_s, "frozen_layout_s": frozen_s, "frozen_layout_parts": frozen,
+            "kruskal_stress": S.kruskal_stress(p[:, 0], p[:, 1], src, dst, 16),
+            "reference_published_ms_per_tick": {"1 worker": 1987.73, "16 workers": 664.12,
+                                                "source": "docs/measurements/perf-bh-1m.md:36-43, other host"}}
+
+
 # --------------------------------------------------------------- GPU arm --
 
 def run_gpu(args, dist: Dist):
@@ -472,6 +510,9 @@ def run_gpu(args, dist: Dist):
     three_d = None
     if not args.no_3d and dist.rank == 0:
         three_d = run_3d(args, dist)
+    d3 = None
+    if not args.no_d3 and dist.rank == 0:
+        d3 = run_d3(args, dist)
 
     if dist.rank == 0:
         line = {
@@ -513,6 +554,7 @@ def run_gpu(args, dist: Dist):
             "batched": batched,
             "adjoint": adjoint,
             "powerlaw_1m_3d": three_d,
+            "d3_force_1m": d3,
             "vs_baseline_basis": "reference's own 1M-node FA2-BH run, 1 thread, other host "
                                  "(perf-fa2bh.md:60-63; theta 0.8, its gate-model graph)",
         }

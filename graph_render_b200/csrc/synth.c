@@ -218,3 +218,55 @@ void syn_unit(uint64_t count, uint64_t seed, double *out) {
     sm64 r = {seed};
     for (uint64_t i = 0; i < count; i++) out[i] = sm_unit(&r);
 }
+
+/* The reference's benchmark model (crates/graph-core/src/synthetic.rs:92-170,
+ * the graph its `tick` and snapshot benches run on): one mulberry32 stream from
+ * 0x051042, read first by the node records (an icon roll and, below 0.8, a table
+ * pick), then by preferential attachment (node i to floor(u v i), a second such
+ * edge with probability 1/2) and floor(0.05 n) uniform extra pairs; every edge
+ * that is not a self-edge draws its strength 0.4 + 0.4 u. Returns the edge
+ * count; writes at most cap edges. */
+static double mb32_unit(uint32_t *s) {
+    *s += 0x6D2B79F5u;
+    uint32_t a = *s;
+    uint32_t t = (a ^ (a >> 15)) * (1u | a);
+    t = (t + ((t ^ (t >> 7)) * (61u | t))) ^ t;
+    return (double)(t ^ (t >> 14)) / 4294967296.0;
+}
+
+int64_t syn_gate(uint32_t count, uint32_t *src, uint32_t *dst, double *strength, int64_t cap) {
+    uint32_t s = 0x051042u;
+    for (uint32_t i = 0; i < count; i++) {
+        const double roll = mb32_unit(&s);
+        if (roll < 0.8) (void)mb32_unit(&s); /* the emoji (12) or icon (4) pick */
+    }
+    int64_t m = 0;
+    for (uint32_t pass = 0; pass < 2; pass++) {
+        const uint32_t rounds = pass == 0 ? (count ? count - 1 : 0) : (uint32_t)floor((double)count * 0.05);
+        for (uint32_t r = 0; r < rounds; r++) {
+            for (int second = 0; second < 2; second++) {
+                uint32_t a, b;
+                if (pass == 0) {
+                    const uint32_t i = r + 1;
+                    if (second && !(mb32_unit(&s) < 0.5)) break;
+                    const double u = mb32_unit(&s), v = mb32_unit(&s);
+                    a = i;
+                    b = (uint32_t)floor(u * v * (double)i);
+                } else {
+                    if (second) break;
+                    a = (uint32_t)floor(mb32_unit(&s) * (double)count);
+                    b = (uint32_t)floor(mb32_unit(&s) * (double)count);
+                }
+                if (a == b) continue;
+                const double st = 0.4 + mb32_unit(&s) * 0.4;
+                if (m < cap) {
+                    src[m] = a;
+                    dst[m] = b;
+                    strength[m] = st;
+                }
+                m++;
+            }
+        }
+    }
+    return m;
+}

@@ -41,6 +41,8 @@ def lib():
         L.syn_lognormal.argtypes = [u64, d, d, u64, vp]
         L.syn_randint.argtypes = [u64, u32, u64, vp]
         L.syn_unit.argtypes = [u64, u64, vp]
+        L.syn_gate.argtypes = [u32, vp, vp, vp, i64]
+        L.syn_gate.restype = i64
         _lib = L
     return _lib
 
@@ -160,3 +162,15 @@ def sbm_50k(seed: int = 5, n: int = 50_000, blocks: int = 16) -> Workload:
     pos = uniform(n, 2, 0.0, math.sqrt(n) * 10.0, seed + 1000)
     return Workload(f"sbm{n}-2d", n, s, d, np.ones(len(s)), pos,
                     dict(theta=1.2, dim=2, seed=seed, max_iter=200, edge_weight_influence=1.0), 200)
+
+
+def gate(n: int):
+    """The reference's benchmark model with n nodes (crates/graph-core/src/synthetic.rs:92-170):
+    (source, target, strength) of its raw edges, in edge order."""
+    cap = 2 * n + n // 20 + 16
+    src = np.zeros(cap, np.uint32)
+    dst = np.zeros(cap, np.uint32)
+    st = np.zeros(cap, np.float64)
+    m = lib().syn_gate(n, _p(src), _p(dst), _p(st), cap)
+    assert m <= cap
+    return src[:m].copy(), dst[:m].copy(), st[:m].copy()

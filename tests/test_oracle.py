@@ -279,3 +279,11 @@ def test_oracle_bfs_hops_on_a_path_with_a_loop_and_a_stray_node():
     none = np.iinfo(np.uint32).max
     assert h[0].tolist() == [0, 1, 2, 3, none]
     assert h[1].tolist() == [3, 2, 1, 0, none]
+
+
+@pytest.mark.parametrize("n", [2, 3, 17, 601, 20_000])
+def test_product_gate_generator_draws_the_oracles_model(n):
+    from graph_render_b200 import synth
+
+    for a, b in zip(synth.gate(n), O.gate_edges(n)):
+        assert np.array_equal(a, b)
