@@ -118,3 +118,29 @@ def run_values(topology: Topology, values) -> Geometry:
         raise StageError("NonFinite", "node.x", "non-finite position", rc)
     N.check(rc)
     return Geometry.points(out[:n])
+
+
+def _main(argv=None) -> None:
+    """python -m graph_render_b200.d3force --n N --ticks T: a session on the
+    reference's benchmark model, T ticks after 3 warm-up ticks; prints ms per tick."""
+    import argparse
+    import json
+    import time
+
+    from . import synth
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--ticks", type=int, default=5)
+    a = ap.parse_args(argv)
+    src, dst, st = synth.gate(a.n)
+    with ForceSession(a.n, src, dst, st) as s:
+        s.tick(3)
+        t0 = time.perf_counter()
+        s.tick(a.ticks)
+        ms = (time.perf_counter() - t0) * 1e3 / max(a.ticks, 1)
+        print(json.dumps({"n": a.n, "ticks": a.ticks, "ms_per_tick": ms, **s.info()}))
+
+
+if __name__ == "__main__":
+    _main()
