@@ -153,7 +153,13 @@ __device__ __forceinline__ bool d3_settle(const D3Params &P, uint32_t tick, uint
 
 // Many-body: per sorted node, the stackless preorder walk of charge.rs
 // node_delta over the cells (A {cx, cy, count, w^2}, B {cx_lo, cy_lo, skip |
-// -count, start}); the delta goes onto the node's own velocity.
+// -count, start}); the delta goes onto the node's own velocity. A cell the
+// opening test resolves acts as one body of its count; a leaf it does not takes
+// its points directly, every point at the leaf centre's offset (charge.rs
+// direct), which is the same term with the count less this node when it lies in
+// the leaf. So the common outcomes need no branch: the term is selected by
+// predicate, the next cell by select; only an exactly zero axis (the jiggle)
+// branches.
 __global__ void __launch_bounds__(D3_T)
 k_d3_charge(D3Params P, const D3State *st, const DevState *ts, Cells cells, const float4 *__restrict__ sp,
             const uint32_t *__restrict__ sorig, float2 *__restrict__ v) {
@@ -172,31 +178,30 @@ k_d3_charge(D3Params P, const D3State *st, const DevState *ts, Cells cells, cons
         const bool leaf = sk < 0;
         float dx = (A.x - me.x) + B.x, dy = (A.y - me.y) + B.y;
         float l = dx * dx + dy * dy;
-        if (A.w >= P.th2 * l) {  // open >= l: w^2 / theta^2 >= l
-            if (!leaf) {
-                k++;
-                continue;
+        const bool open = A.w >= P.th2 * l;  // open >= l: w^2 / theta^2 >= l
+        const bool in_range = l < P.dmax2;   // settle: nothing at or past distanceMax
+        const uint32_t start = __float_as_uint(B.w), cnt = leaf ? (uint32_t)(-sk) : 0u;
+        const bool self_in = leaf && p - start < cnt;  // this node is one of the leaf's points
+        if (dx == 0.f || dy == 0.f) {  // the jiggle, keyed on the chain head (direct) or the cell (body)
+            const uint32_t key = (open && leaf) ? __ldg(&sorig[start + cnt - 1]) : k;
+            if (dx == 0.f) {
+                dx = (float)jiggle(P.seed, tick, 2, oi, key);
+                l += dx * dx;
             }
-            const uint32_t start = __float_as_uint(B.w), cnt = (uint32_t)(-sk);
-            // the jiggle key is the leaf's chain head: its most recently inserted,
-            // so highest-numbered, point (the last in key-then-index order)
-            if (d3_settle(P, tick, oi, __ldg(&sorig[start + cnt - 1]), dx, dy, l)) {
-                const float f = ca / l;
-                for (uint32_t q = start; q < start + cnt; q++) {
-                    if (q == p) continue;
-                    ax += dx * f;
-                    ay += dy * f;
-                }
+            if (dy == 0.f) {
+                dy = (float)jiggle(P.seed, tick, 3, oi, key);
+                l += dy * dy;
             }
-            k++;
-        } else {
-            if (d3_settle(P, tick, oi, k, dx, dy, l)) {
-                const float f = A.z * ca / l;
-                ax += dx * f;
-                ay += dy * f;
-            }
-            k = leaf ? k + 1 : max((uint32_t)sk, k + 1);
         }
+        l = l < P.dmin2 ? sqrtf(P.dmin2 * l) : l;
+        l = l == 0.f ? fmaxf(P.dmin2, 1.17549435e-38f) : l;
+        const bool descend = open && !leaf;
+        const bool counted = !descend && in_range;
+        const float m = (open && self_in) ? A.z - 1.f : A.z;
+        const float f = counted ? m * ca / l : 0.f;
+        ax += dx * f;
+        ay += dy * f;
+        k = (descend || leaf) ? k + 1 : max((uint32_t)sk, k + 1);
     }
     float2 w = v[oi];
     w.x += ax;
