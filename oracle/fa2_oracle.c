@@ -1413,6 +1413,9 @@ typedef struct {
     double *x, *y, *vx, *vy, *px, *py, *pos, *dvx, *dvy, *fx, *fy;
     ttree ct, kt; /* charge tree, collide tree */
     d3body *bodies;
+    int mesh;       /* many-body on the particle mesh (particle_mesh.rs) instead of the tree */
+    uint32_t side;  /* mesh side (mesh.rs side_for) */
+    double *gre, *gim, *kre, *kim, *twr, *twi; /* density/field, kernel spectrum, twiddles */
 } orc_d3;
 
 /* seed.rs spiral_point: radius 12 sqrt(i + 1), angle i * golden angle. */
@@ -1514,6 +1517,12 @@ void orc_d3_free(orc_d3 *s) {
         free(ts[k]->bodies);
     }
     free(s->bodies);
+    free(s->gre);
+    free(s->gim);
+    free(s->kre);
+    free(s->kim);
+    free(s->twr);
+    free(s->twi);
     free(s->lo);
     free(s->hi);
     free(s->dist);
@@ -1753,12 +1762,250 @@ static void d3_collide(orc_d3 *s) {
     }
 }
 
-/* sim.rs tick: alpha decay, link, charge, center, collide, integrate. */
+/* ------------------------------------------------- particle mesh -------- */
+/*
+ * The many-body pass of graph-core's particle-mesh layout
+ * (crates/graph-core/src/layout/force/particle_mesh/{mesh,frame,deposit,kernel,
+ * fft,charge}.rs): the positions' bounding box placed on a side x side mesh
+ * (frame.rs place / fit: cell size 2^(step/4), the smallest step whose cells +
+ * reach fit), cloud-in-cell deposit of unit masses (deposit.rs weights), the
+ * law's vector Green's function sampled within reach and scaled by 1/side^2
+ * (kernel.rs sample / green: -r/l, l clamped up to distanceMin, nothing at or
+ * past distanceMax), one complex FFT convolution (field = re, im), bilinear read
+ * at every node, times charge * alpha onto the velocity. The FFT here is a plain
+ * radix-2 transform with the reference's sign and normalisation (forward
+ * exp(-2 pi i k / N), both directions unscaled).
+ */
+
+/* mesh.rs side_for: next power of two of ceil(sqrt(n)), clamped to [128, 1024]. */
+static uint32_t pm_side(uint32_t n) {
+    uint32_t root = (uint32_t)ceil(sqrt((double)n)), side = 1;
+    while (side < root) side <<= 1;
+    return side < 128 ? 128 : (side > 1024 ? 1024 : side);
+}
+
+typedef struct {
+    int step;
+    double h, ox, oy;
+    uint32_t cells, reach;
+} pm_frame;
+
+/* frame.rs fit / place. */
+static int pm_place(double lx, double ly, double hx, double hy, uint32_t side, double dmax, pm_frame *f) {
+    double span = fmax(hx - lx, hy - ly);
+    if (!isfinite(span)) return 0;
+    int step = (int)floor(4.0 * log2(span / (double)side));
+    if (step < -32) step = -32;
+    for (;; step++) {
+        double h = exp2((double)step / 4.0);
+        double cells = floor(span / h) + 3.0;
+        if (cells > (double)side) continue;
+        uint32_t c = (uint32_t)cells;
+        double rr = ceil(dmax / h);
+        uint32_t reach = rr > (double)(c - 1) ? c - 1 : (uint32_t)rr;
+        if (c + reach > side) continue;
+        f->step = step;
+        f->h = h;
+        f->cells = c;
+        f->reach = reach;
+        f->ox = floor(lx / h) * h;
+        f->oy = floor(ly / h) * h;
+        return 1;
+    }
+}
+
+/* frame.rs scaled + split: the node's cell and its fractions within it. */
+static void pm_split(const pm_frame *f, double px, double py, uint32_t *cx, uint32_t *cy, double *fx, double *fy) {
+    double u[2] = {(px - f->ox) / f->h, (py - f->oy) / f->h};
+    uint32_t c[2];
+    double fr[2];
+    for (int a = 0; a < 2; a++) {
+        double v = u[a] > 0.0 ? u[a] : 0.0; /* `u as usize` saturates at 0 */
+        uint32_t cell = (uint32_t)v;
+        if (cell > f->cells - 2) cell = f->cells - 2;
+        double t = u[a] - (double)cell;
+        fr[a] = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+        c[a] = cell;
+    }
+    *cx = c[0];
+    *cy = c[1];
+    *fx = fr[0];
+    *fy = fr[1];
+}
+
+/* One radix-2 line transform (bit reversal, then log2(N) butterfly stages). */
+static void pm_line(double *re, double *im, uint32_t N, size_t stride, const double *twr, const double *twi,
+                    int inverse) {
+    uint32_t bits = 0;
+    while ((1u << bits) < N) bits++;
+    for (uint32_t i = 0; i < N; i++) {
+        uint32_t j = 0;
+        for (uint32_t b = 0; b < bits; b++) j |= ((i >> b) & 1u) << (bits - 1 - b);
+        if (i < j) {
+            double t = re[i * stride];
+            re[i * stride] = re[j * stride];
+            re[j * stride] = t;
+            t = im[i * stride];
+            im[i * stride] = im[j * stride];
+            im[j * stride] = t;
+        }
+    }
+    for (uint32_t m = 1; m < N; m <<= 1) {
+        for (uint32_t g = 0; g < N; g += 2 * m) {
+            for (uint32_t k = 0; k < m; k++) {
+                uint32_t t = k * (N / (2 * m));
+                double wr = twr[t], wi = inverse ? -twi[t] : twi[t];
+                size_t i0 = (size_t)(g + k) * stride, i1 = (size_t)(g + k + m) * stride;
+                double br = re[i1] * wr - im[i1] * wi, bi = re[i1] * wi + im[i1] * wr;
+                re[i1] = re[i0] - br;
+                im[i1] = im[i0] - bi;
+                re[i0] += br;
+                im[i0] += bi;
+            }
+        }
+    }
+}
+
+static void pm_fft2(orc_d3 *s, double *re, double *im, int inverse) {
+    uint32_t N = s->side;
+    for (uint32_t r = 0; r < N; r++) pm_line(re + (size_t)r * N, im + (size_t)r * N, N, 1, s->twr, s->twi, inverse);
+    for (uint32_t c = 0; c < N; c++) pm_line(re + c, im + c, N, N, s->twr, s->twi, inverse);
+}
+
+/* mesh.rs solve + charge.rs apply: returns 0 when the mesh does not apply
+ * (fewer than two nodes, distanceMax 0, no finite extent). */
+static int d3_mesh(orc_d3 *s) {
+    double dmin2 = s->P.distance_min * s->P.distance_min, dmax2 = s->P.distance_max * s->P.distance_max;
+    if (s->n < 2 || !(dmax2 > 0.0)) return 0;
+    double lx = INFINITY, ly = INFINITY, hx = -INFINITY, hy = -INFINITY;
+    for (uint32_t i = 0; i < s->n; i++) {
+        if (!isfinite(s->x[i]) || !isfinite(s->y[i])) continue;
+        lx = fmin(lx, s->x[i]);
+        ly = fmin(ly, s->y[i]);
+        hx = fmax(hx, s->x[i]);
+        hy = fmax(hy, s->y[i]);
+    }
+    if (!(lx <= hx)) return 0;
+    uint32_t N = s->side;
+    pm_frame f;
+    if (!pm_place(lx, ly, hx, hy, N, sqrt(dmax2), &f)) return 0;
+    size_t NN = (size_t)N * N;
+    memset(s->gre, 0, NN * 8);
+    memset(s->gim, 0, NN * 8);
+    for (uint32_t i = 0; i < s->n; i++) { /* deposit.rs: cloud in cell */
+        uint32_t cx, cy;
+        double fx, fy;
+        pm_split(&f, s->x[i], s->y[i], &cx, &cy, &fx, &fy);
+        size_t at = (size_t)cy * N + cx;
+        s->gre[at] += (1.0 - fx) * (1.0 - fy);
+        s->gre[at + 1] += fx * (1.0 - fy);
+        s->gre[at + N] += (1.0 - fx) * fy;
+        s->gre[at + N + 1] += fx * fy;
+    }
+    /* kernel.rs sample + green */
+    memset(s->kre, 0, NN * 8);
+    memset(s->kim, 0, NN * 8);
+    double scale = 1.0 / (double)NN;
+    int reach = (int)f.reach;
+    for (int dy = -reach; dy <= reach; dy++) {
+        size_t row = (size_t)((dy % (int)N + (int)N) % (int)N) * N;
+        for (int dx = -reach; dx <= reach; dx++) {
+            double rx = (double)dx * f.h, ry = (double)dy * f.h;
+            double l = rx * rx + ry * ry;
+            size_t at = row + (size_t)((dx % (int)N + (int)N) % (int)N);
+            if (l == 0.0 || l >= dmax2) {
+                s->kre[at] = 0.0;
+                s->kim[at] = 0.0;
+                continue;
+            }
+            if (l < dmin2) l = sqrt(dmin2 * l);
+            s->kre[at] = -rx / l * scale;
+            s->kim[at] = -ry / l * scale;
+        }
+    }
+    pm_fft2(s, s->kre, s->kim, 0);
+    pm_fft2(s, s->gre, s->gim, 0);
+    for (size_t q = 0; q < NN; q++) {
+        double a = s->gre[q], b = s->gim[q], c = s->kre[q], d = s->kim[q];
+        s->gre[q] = a * c - b * d;
+        s->gim[q] = a * d + b * c;
+    }
+    pm_fft2(s, s->gre, s->gim, 1);
+    double strength = s->P.charge * s->alpha;
+    for (uint32_t i = 0; i < s->n; i++) { /* mesh.rs read: bilinear */
+        uint32_t cx, cy;
+        double fx, fy;
+        pm_split(&f, s->x[i], s->y[i], &cx, &cy, &fx, &fy);
+        size_t at = (size_t)cy * N + cx;
+        double w[4] = {(1.0 - fx) * (1.0 - fy), fx * (1.0 - fy), (1.0 - fx) * fy, fx * fy};
+        size_t cell[4] = {at, at + 1, at + N, at + N + 1};
+        double ex = 0.0, ey = 0.0;
+        for (int k = 0; k < 4; k++) {
+            ex += s->gre[cell[k]] * w[k];
+            ey += s->gim[cell[k]] * w[k];
+        }
+        s->dvx[i] = ex * strength;
+        s->dvy[i] = ey * strength;
+    }
+    for (uint32_t i = 0; i < s->n; i++) {
+        s->vx[i] += s->dvx[i];
+        s->vy[i] += s->dvy[i];
+    }
+    return 1;
+}
+
+/* The mesh's field (re, im) at every node for the current positions, without
+ * touching the velocities: charge * alpha left out (tests against the direct
+ * law, particle_mesh/tests.rs:44-69). */
+int orc_pm_field(orc_d3 *s, double *out) {
+    double keep_alpha = s->alpha, keep_charge = s->P.charge;
+    double *vx = (double *)malloc((size_t)(s->n ? s->n : 1) * 8), *vy = (double *)malloc((size_t)(s->n ? s->n : 1) * 8);
+    memcpy(vx, s->vx, (size_t)s->n * 8);
+    memcpy(vy, s->vy, (size_t)s->n * 8);
+    s->alpha = 1.0;
+    s->P.charge = 1.0;
+    int ok = d3_mesh(s);
+    for (uint32_t i = 0; i < s->n; i++) {
+        out[2 * i] = ok ? s->dvx[i] : 0.0;
+        out[2 * i + 1] = ok ? s->dvy[i] : 0.0;
+    }
+    memcpy(s->vx, vx, (size_t)s->n * 8);
+    memcpy(s->vy, vy, (size_t)s->n * 8);
+    free(vx);
+    free(vy);
+    s->alpha = keep_alpha;
+    s->P.charge = keep_charge;
+    return ok;
+}
+
+/* ForceSession::with_particle_mesh: the many-body pass moves onto the mesh. */
+void orc_d3_use_mesh(orc_d3 *s) {
+    s->mesh = 1;
+    s->side = pm_side(s->n);
+    size_t NN = (size_t)s->side * s->side;
+    s->gre = (double *)calloc(NN, 8);
+    s->gim = (double *)calloc(NN, 8);
+    s->kre = (double *)calloc(NN, 8);
+    s->kim = (double *)calloc(NN, 8);
+    s->twr = (double *)malloc((size_t)s->side / 2 * 8);
+    s->twi = (double *)malloc((size_t)s->side / 2 * 8);
+    for (uint32_t k = 0; k < s->side / 2; k++) { /* fft.rs Plan::new root */
+        double angle = -6.283185307179586 * (double)k / (double)s->side; /* -TAU k / side */
+        s->twr[k] = cos(angle);
+        s->twi[k] = sin(angle);
+    }
+}
+
+/* sim.rs tick (particle_mesh.rs tick): alpha decay, link, charge, center,
+ * collide, integrate. */
 void orc_d3_tick(orc_d3 *s, uint32_t ticks) {
     for (uint32_t t = 0; t < ticks; t++) {
         s->alpha += (0.0 - s->alpha) * s->P.alpha_decay;
         d3_link(s);
-        d3_charge(s);
+        if (s->mesh)
+            (void)d3_mesh(s);
+        else
+            d3_charge(s);
         d3_center(s);
         d3_collide(s);
         double decay = s->P.velocity_decay;

@@ -82,6 +82,9 @@ def lib():
     L.orc_d3_alpha.argtypes = [P]
     L.orc_d3_alpha.restype = C.c_double
     L.orc_d3_set_state.argtypes = [P, f64p, f64p, C.c_double, C.c_uint32]
+    L.orc_d3_use_mesh.argtypes = [P]
+    L.orc_pm_field.argtypes = [P, f64p]
+    L.orc_pm_field.restype = C.c_int
     L.orc_gate_edges.argtypes = [C.c_uint32, u32p, u32p, f64p, C.c_int64]
     L.orc_gate_edges.restype = C.c_int64
     L.orc_simple_graph.argtypes = [C.c_uint32, C.c_int64, u32p, u32p, P, u32p, u32p, f64p]
@@ -189,6 +192,16 @@ class D3:
 
     def alpha(self) -> float:
         return lib().orc_d3_alpha(self.h)
+
+    def use_mesh(self) -> None:
+        """Many-body on the particle mesh (particle_mesh.rs) from here on."""
+        lib().orc_d3_use_mesh(self.h)
+
+    def mesh_field(self) -> np.ndarray:
+        """The mesh's field (charge * alpha left out) at every node, n x 2."""
+        out = np.zeros(2 * max(self.n, 1))
+        lib().orc_pm_field(self.h, out)
+        return out[:2 * self.n].reshape(self.n, 2)
 
     def set_state(self, pos, vel, alpha: float, tick_no: int) -> None:
         lib().orc_d3_set_state(self.h, np.ascontiguousarray(pos, np.float64).reshape(-1),
