@@ -7,12 +7,12 @@ this package is its host-side face (registry mirror, parameter schema,
 per-tick handle) and the workload generators.
 """
 
-from .registry import (D3_ID, FA2_ID, Capability, Geometry, ParamSpec, ParamsError, ParamsView, StageError,
+from .registry import (D3_ID, FA2_ID, PM_ID, Capability, Geometry, ParamSpec, ParamsError, ParamsView, StageError,
                        Topology, find, layouts)
 from .fa2 import Fa2, layout, params_bytes, run_values
 from .d3force import ForceParams, ForceSession
 
 __all__ = [
-    "D3_ID", "FA2_ID", "ForceParams", "ForceSession", "Capability", "Geometry", "ParamSpec", "ParamsError", "ParamsView", "StageError",
+    "D3_ID", "FA2_ID", "PM_ID", "ForceParams", "ForceSession", "Capability", "Geometry", "ParamSpec", "ParamsError", "ParamsView", "StageError",
     "Topology", "find", "layouts", "Fa2", "layout", "params_bytes", "run_values",
 ]

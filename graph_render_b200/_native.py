@@ -98,6 +98,8 @@ SIGNATURES = {
     "gr_force_session_reheat": ([P, C.c_double], C.c_int),
     "gr_force_session_info": ([P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)], C.c_int),
     "gr_force_session_set_state": ([P, P, P, C.c_double, C.c_uint32], C.c_int),
+    "gr_force_session_use_mesh": ([P], C.c_int),
+    "gr_force_mesh_run": ([C.c_uint32, C.c_uint64, P, P, P, P], C.c_int),
     "gr_force_run": ([C.c_uint32, C.c_uint64, P, P, P, P], C.c_int),
     "gr_stress": ([C.c_uint32, C.c_uint64, P, P, P, P, C.c_uint32, C.POINTER(C.c_double)], C.c_int),
     "gr_fa2_batch_create": ([C.POINTER(P), C.c_uint32, P, P, P, P, P, P, C.c_uint32, P], C.c_int),

@@ -209,12 +209,13 @@ k_d3_charge(D3Params P, const D3State *st, const DevState *ts, Cells cells, cons
     v[oi] = w;
 }
 
-// center.js: every position shifted by the mean (FP64, from the tree's bounds
-// pass over the same positions) times the centering strength.
-__global__ void k_d3_center(uint32_t n, float strength, const DevState *ts, float4 *__restrict__ p) {
+// center.js: every position shifted by the mean (FP64, from the bounds pass
+// over the same positions: the many-body tree's, or the mesh's) times the
+// centering strength.
+__global__ void k_d3_center(uint32_t n, float strength, const double *mean, float4 *__restrict__ p) {
     const uint32_t i = blockIdx.x * D3_T + threadIdx.x;
     if (i >= n) return;
-    const float sx = (float)(ts->mean[0] * (double)strength), sy = (float)(ts->mean[1] * (double)strength);
+    const float sx = (float)(mean[0] * (double)strength), sy = (float)(mean[1] * (double)strength);
     float4 a = p[i];
     a.x -= sx;
     a.y -= sy;

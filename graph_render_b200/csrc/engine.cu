@@ -31,6 +31,7 @@
 #include "adjoint.cuh"
 #include "stress.cuh"
 #include "d3force.cuh"
+#include "pm.cuh"
 
 using namespace gr;
 
@@ -631,9 +632,10 @@ int gr_last_error(void) { return g_err; }
 const char *gr_last_error_message(void) { return g_msg; }
 int gr_last_error_index(void) { return g_err_index; }
 
-static const char *kLayouts[] = {"layout.forceatlas2.barnes_hut.cuda", "layout.force.barnes_hut.cuda"};
+static const char *kLayouts[] = {"layout.forceatlas2.barnes_hut.cuda", "layout.force.barnes_hut.cuda",
+                                  "layout.force.particle_mesh.cuda"};
 
-uint32_t gr_layout_count(void) { return 2; }
+uint32_t gr_layout_count(void) { return 3; }
 const char *gr_layout_id(uint32_t i) {
     if (i >= gr_layout_count()) {
         set_err(GR_INDEX_OUT_OF_RANGE, "layout index past the end");
@@ -929,6 +931,10 @@ int gr_run(const char *layout_id, uint32_t n, uint64_t m, const uint32_t *src, c
         // the d3-force row publishes no parameters (registry/layouts.rs LayoutParams::NONE)
         if (params_len) return set_err(GR_PARAMS_NOT_ACCEPTED, "layout.force.barnes_hut.cuda takes no parameters");
         return gr_force_run(n, m, src, dst, weight, out);
+    }
+    if (layout_id && strcmp(layout_id, kLayouts[2]) == 0) {
+        if (params_len) return set_err(GR_PARAMS_NOT_ACCEPTED, "layout.force.particle_mesh.cuda takes no parameters");
+        return gr_force_mesh_run(n, m, src, dst, weight, out);
     }
     if (!layout_id || strcmp(layout_id, kLayouts[0]) != 0)
         return set_err(GR_UNKNOWN_LAYOUT_ID, "unknown layout id");
@@ -1846,7 +1852,17 @@ struct gr_force_session {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint32_t graph_kernels = 0;
+    // particle mesh (many-body on an FFT mesh instead of the tree)
+    bool mesh = false;
+    uint32_t side = 0, bits = 0, pm_blocks = 0;
+    PmState *pm = nullptr;
+    double *pm_part = nullptr;
+    uint64_t *pm_key = nullptr;
+    uint32_t *pm_val = nullptr, *pm_cs = nullptr, *pm_ce = nullptr;
+    float2 *pm_frac = nullptr, *ga = nullptr, *gk = nullptr, *gt = nullptr, *tw = nullptr;
+    RadixSorter pm_sorter;
     ~gr_force_session() {
+        pm_sorter.release();
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (t) {
@@ -1872,6 +1888,45 @@ int d3_validate(const gr_force_params &p) {
     return GR_OK;
 }
 
+// The mesh's many-body pass (pm.cuh): frame, stencils, cell sort, deposit,
+// Green's function, forward FFTs (spectra transposed), product, inverse FFT
+// (natural layout), bilinear read onto the velocities.
+void pm_fft2(gr_force_session *S, float2 *a, float2 *scratch, bool inverse, cudaStream_t s) {
+    const uint32_t side = S->side, th = std::min<uint32_t>(side / 2, 512);
+    const size_t sm = (size_t)side * sizeof(float2);
+    const dim3 tg(side / 32, side / 32), tb(32, 8);
+    if (inverse) {
+        k_pm_fft_rows<true><<<side, th, sm, s>>>(a, S->tw, side, S->bits, S->pm);
+        k_pm_transpose<<<tg, tb, 0, s>>>(a, scratch, side, S->pm);
+        k_pm_fft_rows<true><<<side, th, sm, s>>>(scratch, S->tw, side, S->bits, S->pm);
+    } else {
+        k_pm_fft_rows<false><<<side, th, sm, s>>>(a, S->tw, side, S->bits, S->pm);
+        k_pm_transpose<<<tg, tb, 0, s>>>(a, scratch, side, S->pm);
+        k_pm_fft_rows<false><<<side, th, sm, s>>>(scratch, S->tw, side, S->bits, S->pm);
+    }
+}
+
+void pm_enqueue(gr_force_session *S) {
+    cudaStream_t s = S->t->stream;
+    const uint32_t n = S->n, side = S->side, g = div_up(n, PM_T);
+    const uint32_t mg = div_up(side * side, PM_T);
+    const double dmin2 = S->prm.distance_min * S->prm.distance_min;
+    const double dmax2 = S->prm.distance_max * S->prm.distance_max;
+    k_pm_bounds<<<S->pm_blocks, PM_T, 0, s>>>(n, S->p4, side, S->prm.distance_max, dmax2, S->pm_part, S->pm);
+    k_pm_stencil<<<g, PM_T, 0, s>>>(n, S->p4, S->pm, side, S->pm_key, S->pm_val, S->pm_frac);
+    S->pm_sorter.sort(S->pm_key, S->pm_val, n, 32, s);
+    cudaMemsetAsync(S->pm_cs, 0, (size_t)side * side * 4, s);
+    cudaMemsetAsync(S->pm_ce, 0, (size_t)side * side * 4, s);
+    k_pm_mark<<<g, PM_T, 0, s>>>(n, S->pm, S->pm_key, S->pm_cs, S->pm_ce);
+    k_pm_deposit<<<mg, PM_T, 0, s>>>(side, S->pm, S->pm_cs, S->pm_ce, S->pm_val, S->pm_frac, S->ga);
+    k_pm_green<<<mg, PM_T, 0, s>>>(side, S->pm, dmin2, dmax2, S->gk);
+    pm_fft2(S, S->gk, S->gt, false, s);  // kernel spectrum, transposed, in gt
+    pm_fft2(S, S->ga, S->gk, false, s);  // density spectrum, transposed, in gk
+    k_pm_mul<<<mg, PM_T, 0, s>>>(side * side, S->gk, S->gt, S->pm);
+    pm_fft2(S, S->gk, S->ga, true, s);   // field, natural layout, in ga
+    k_pm_read<<<g, PM_T, 0, s>>>(n, S->p4, S->pm, side, (float)S->prm.charge, &S->ds->alpha, S->ga, S->vel);
+}
+
 void d3_enqueue(gr_force_session *S) {
     gr_fa2 *t = S->t;
     cudaStream_t s = t->stream;
@@ -1883,10 +1938,15 @@ void d3_enqueue(gr_force_session *S) {
             S->P, t->nseg, S->ds, S->pp4, t->rp, t->col, t->wt, t->seg_row, t->seg_first, S->seg_out);
     k_d3_link<<<g, D3_T, 0, s>>>(S->P, S->ds, S->pp4, t->rp, t->col, t->wt, t->nseg ? t->seg_first : nullptr,
                                  S->seg_out, S->vel);
-    t->pos = S->p4;  // many-body: the tree of the positions
-    enqueue_tick<2>(t, false, PH_TREE);
-    k_d3_charge<<<g, D3_T, 0, s>>>(S->P, S->ds, t->st, t->cells, t->sp, t->sorig, S->vel);
-    k_d3_center<<<g, D3_T, 0, s>>>(n, (float)S->prm.center_strength, t->st, S->p4);
+    if (S->mesh) {  // many-body on the particle mesh
+        pm_enqueue(S);
+        k_d3_center<<<g, D3_T, 0, s>>>(n, (float)S->prm.center_strength, S->pm->mean, S->p4);
+    } else {  // many-body: the tree of the positions
+        t->pos = S->p4;
+        enqueue_tick<2>(t, false, PH_TREE);
+        k_d3_charge<<<g, D3_T, 0, s>>>(S->P, S->ds, t->st, t->cells, t->sp, t->sorig, S->vel);
+        k_d3_center<<<g, D3_T, 0, s>>>(n, (float)S->prm.center_strength, t->st->mean, S->p4);
+    }
     k_d3_project<<<g, D3_T, 0, s>>>(n, S->p4, S->vel, S->pp4);
     t->pos = S->pp4;  // collide: the tree of the projected positions, with cell squares
     t->cells.bounds = S->bounds;
@@ -2097,6 +2157,68 @@ int gr_force_session_set_state(gr_force_session *S, const float *pos, const floa
     CU(cudaMemcpyAsync(S->ds, &d, sizeof d, cudaMemcpyHostToDevice, s));
     CU(cudaStreamSynchronize(s));
     return ok();
+}
+
+int gr_force_session_use_mesh(gr_force_session *S) {
+    if (!S) return set_err(GR_INVALID_HANDLE, "null session");
+    if (S->mesh) return ok();
+    gr_fa2 *t = S->t;
+    const uint32_t n = S->n;
+    // mesh.rs side_for: next power of two of ceil(sqrt(n)), in [128, 1024]
+    uint32_t root = (uint32_t)std::ceil(std::sqrt((double)n)), side = 1, bits = 0;
+    while (side < root) {
+        side <<= 1;
+        bits++;
+    }
+    while (side < (uint32_t)PM_MIN_SIDE) {
+        side <<= 1;
+        bits++;
+    }
+    while (side > (uint32_t)PM_MAX_SIDE) {
+        side >>= 1;
+        bits--;
+    }
+    const size_t NN = (size_t)side * side;
+    const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>(div_up(n, PM_T), 592));
+    cudaError_t e;
+    if ((e = t->alloc(&S->pm, 1)) || (e = t->alloc(&S->pm_part, 6 * (size_t)blocks)) ||
+        (e = t->alloc(&S->pm_key, n)) || (e = t->alloc(&S->pm_val, n)) || (e = t->alloc(&S->pm_frac, n)) ||
+        (e = t->alloc(&S->pm_cs, NN)) || (e = t->alloc(&S->pm_ce, NN)) || (e = t->alloc(&S->ga, NN)) ||
+        (e = t->alloc(&S->gk, NN)) || (e = t->alloc(&S->gt, NN)) || (e = t->alloc(&S->tw, side / 2)) ||
+        (e = S->pm_sorter.init(std::max<uint32_t>(n, 1))))
+        return set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+    // fft.rs Plan::new root: e^(-i TAU k / side), FP64 then narrowed
+    std::vector<float2> tw(side / 2);
+    for (uint32_t k = 0; k < side / 2; k++) {
+        const double angle = -6.283185307179586 * (double)k / (double)side;
+        tw[k] = make_float2((float)std::cos(angle), (float)std::sin(angle));
+    }
+    cudaStream_t s = t->stream;
+    CU(cudaMemcpyAsync(S->tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, s));
+    CU(cudaMemsetAsync(S->pm, 0, sizeof(PmState), s));
+    CU(cudaMemsetAsync(S->pm_key, 0, (size_t)std::max(n, 1u) * 8, s));
+    CU(cudaMemsetAsync(S->pm_val, 0, (size_t)std::max(n, 1u) * 4, s));
+    CU(cudaStreamSynchronize(s));
+    S->side = side;
+    S->bits = bits;
+    S->pm_blocks = blocks;
+    S->mesh = true;
+    if (S->exec) cudaGraphExecDestroy(S->exec);
+    if (S->graph) cudaGraphDestroy(S->graph);
+    S->exec = nullptr;
+    S->graph = nullptr;
+    return ok();
+}
+
+int gr_force_mesh_run(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst, const double *strength,
+                      float *out) {
+    gr_force_session *S = nullptr;
+    if (int c = gr_force_session_create(&S, n, m, src, dst, strength, nullptr, nullptr)) return c;
+    int c = gr_force_session_use_mesh(S);
+    if (c == GR_OK) c = gr_force_session_tick(S, GR_FORCE_TICKS);
+    if (c == GR_OK) c = gr_force_session_positions(S, out);
+    delete S;
+    return c;
 }
 
 int gr_force_session_info(gr_force_session *S, uint32_t *graph_kernels, uint32_t *n_cells) {

@@ -94,6 +94,10 @@ class ForceSession:
     def reheat(self, alpha: float) -> None:
         N.check(self._L.gr_force_session_reheat(self.h, float(alpha)))
 
+    def use_mesh(self) -> None:
+        """Many-body on the particle mesh from the next tick on (ForceSession::with_particle_mesh)."""
+        N.check(self._L.gr_force_session_use_mesh(self.h))
+
     def set_state(self, positions=None, velocities=None, alpha: float = 1.0, ticks_done: int = 0) -> None:
         """Carries positions and velocities (n x 2; None keeps the session's), alpha
         and the tick count into the session."""
@@ -120,6 +124,19 @@ def run_values(topology: Topology, values) -> Geometry:
     return Geometry.points(out[:n])
 
 
+def run_values_mesh(topology: Topology, values) -> Geometry:
+    """The frozen particle-mesh layout for the registry row (no parameters):
+    ParticleMesh::run, 112 ticks at the defaults with many-body on the mesh."""
+    n = topology.node_count
+    out = np.zeros((max(n, 1), 2), np.float32)
+    src, dst = topology.source, topology.target
+    rc = N.lib().gr_force_mesh_run(n, len(src), _ptr(src), _ptr(dst), _ptr(topology.strength), _ptr(out))
+    if rc == N.GR_LAYOUT_FAILED:
+        raise StageError("NonFinite", "node.x", "non-finite position", rc)
+    N.check(rc)
+    return Geometry.points(out[:n])
+
+
 def _main(argv=None) -> None:
     """python -m graph_render_b200.d3force --n N --ticks T: a session on the
     reference's benchmark model, T ticks after 3 warm-up ticks; prints ms per tick."""
@@ -132,9 +149,12 @@ def _main(argv=None) -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--ticks", type=int, default=5)
+    ap.add_argument("--mesh", action="store_true", help="many-body on the particle mesh")
     a = ap.parse_args(argv)
     src, dst, st = synth.gate(a.n)
     with ForceSession(a.n, src, dst, st) as s:
+        if a.mesh:
+            s.use_mesh()
         s.tick(3)
         t0 = time.perf_counter()
         s.tick(a.ticks)

@@ -249,6 +249,20 @@ D3_META = Metadata(
     degradation="past device memory the create call refuses with GR_ALLOC_FAILED",
 )
 
+PM_ID = "layout.force.particle_mesh.cuda"
+
+PM_META = Metadata(
+    tier=1,
+    stage="layout",
+    oracle=("the FP64 CPU restatement of graph-core's layout.force.particle_mesh many-body pass (oracle/, "
+            "orc_d3_use_mesh), passing the reference's own particle-mesh tests; the FP32 GPU mesh field and "
+            "tick against it, the layout's stress at the end"),
+    complexity="O(n + P^2 log P) per tick x 112 ticks (P the mesh side, <= 1024): deposit gather, two 2D FFTs, "
+               "bilinear read; collide on the tree of projected positions",
+    scale_ceiling=50_000_000,
+    degradation="past device memory the create call refuses with GR_ALLOC_FAILED",
+)
+
 _LAYOUTS: Optional[List[Capability]] = None
 
 
@@ -266,7 +280,9 @@ def layouts() -> List[Capability]:
         _LAYOUTS = [Capability(FA2_ID, run=lambda t: fa2.run_values(t, view.defaults()), params=view,
                                meta=FA2_META, run_with=fa2.run_values),
                     Capability(D3_ID, run=lambda t: d3force.run_values(t, []), params=none, meta=D3_META,
-                               run_with=d3force.run_values)]
+                               run_with=d3force.run_values),
+                    Capability(PM_ID, run=lambda t: d3force.run_values_mesh(t, []), params=none, meta=PM_META,
+                               run_with=d3force.run_values_mesh)]
     return _LAYOUTS
 
 

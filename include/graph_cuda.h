@@ -223,6 +223,15 @@ int gr_force_session_reheat(gr_force_session *s, double alpha);
  * own), alpha (a finite value in [0, 1]) and the tick count the jiggle is keyed on. */
 int gr_force_session_set_state(gr_force_session *s, const float *pos, const float *vel, double alpha,
                                uint32_t ticks_done);
+/* ForceSession::with_particle_mesh (crates/graph-core/src/layout/force/
+ * particle_mesh.rs): from the next tick on, the session's many-body pass runs on
+ * a side x side FFT mesh (side the power of two of ceil(sqrt(n)) in [128, 1024])
+ * instead of the tree; link, center, collide and the integration are unchanged. */
+int gr_force_session_use_mesh(gr_force_session *s);
+/* The frozen particle-mesh layout (ParticleMesh::run, particle_mesh.rs): a default
+ * session on the mesh, GR_FORCE_TICKS ticks, positions (n x 2) into out. */
+int gr_force_mesh_run(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst, const double *strength,
+                      float *out);
 /* Kernels in the captured tick graph, and the cell count of the last tree. */
 int gr_force_session_info(gr_force_session *s, uint32_t *graph_kernels, uint32_t *n_cells);
 /* The frozen layout (BarnesHut::run, barnes_hut.rs:134-140): default parameters,

@@ -46,13 +46,13 @@ def test_static_library_is_built_beside_the_shared_one():
 def test_abi_version_and_registry_face():
     L = N.lib()
     assert L.gr_abi_version() == 1
-    assert L.gr_layout_count() == 2
-    assert [L.gr_layout_id(i).decode() for i in range(2)] == [
-        "layout.forceatlas2.barnes_hut.cuda", "layout.force.barnes_hut.cuda"]
+    assert L.gr_layout_count() == 3
+    assert [L.gr_layout_id(i).decode() for i in range(3)] == [
+        "layout.forceatlas2.barnes_hut.cuda", "layout.force.barnes_hut.cuda", "layout.force.particle_mesh.cuda"]
     assert L.gr_layout_id(0) == FA2_ID.encode()
-    assert L.gr_layout_id(2) is None
+    assert L.gr_layout_id(3) is None
     assert L.gr_last_error() == N.GR_INDEX_OUT_OF_RANGE
-    assert [c.id for c in layouts()] == [FA2_ID, "layout.force.barnes_hut.cuda"]
+    assert [c.id for c in layouts()] == [FA2_ID, "layout.force.barnes_hut.cuda", "layout.force.particle_mesh.cuda"]
     assert find("layout.force.barnes_hut.cuda").params.is_empty()
 
 
