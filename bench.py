@@ -403,7 +403,19 @@ def run_d3(args, dist: Dist):
         t4 = time.perf_counter()
     frozen_s = t4 - t0
     frozen = {"create_s": t1 - t0, "first_tick_s": t2 - t1, "ticks_2_112_s": t3 - t2, "positions_s": t4 - t3}
+    with ForceSession(n, src, dst, st) as s:  # the same session, many-body on the particle mesh
+        s.use_mesh()
+        s.tick(3)
+        t0 = time.perf_counter()
+        s.tick(T)
+        mesh_ms = (time.perf_counter() - t0) * 1e3 / T
+        s.tick(112 - 3 - T)
+        pm = s.positions()
+    mesh = {"ms_per_tick": mesh_ms, "kruskal_stress_after_112": S.kruskal_stress(pm[:, 0], pm[:, 1], src, dst, 16),
+            "reference_published_ms_per_tick": {"8 workers": 107,
+                                                "source": "docs/measurements/perf-bh-1m.md:98, other host"}}
     return {"workload": f"gate model, {n} nodes, {len(src)} raw edges (the reference's synthetic benchmark graph)",
+            "particle_mesh": mesh,
             "ms_per_tick": tick_ms, "node_ticks_per_s": n / (tick_ms / 1e3), "graph_kernels": info["graph_kernels"],
             "create_s": create_s, "frozen_layout_s": frozen_s, "frozen_layout_parts": frozen,
             "kruskal_stress": S.kruskal_stress(p[:, 0], p[:, 1], src, dst, 16),
