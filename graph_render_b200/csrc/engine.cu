@@ -170,9 +170,12 @@ struct gr_fa2 {
 
     std::vector<void *> allocs;
 
+    // Device buffers come from the stream-ordered pool on the handle's stream
+    // (keep_pool below keeps freed memory pooled), so creating and destroying a
+    // handle costs no device-wide synchronisation per buffer.
     template <typename T>
     cudaError_t alloc(T **p, size_t count) {
-        cudaError_t e = cudaMalloc((void **)p, (count ? count : 1) * sizeof(T));
+        cudaError_t e = cudaMallocAsync((void **)p, (count ? count : 1) * sizeof(T), stream);
         if (e == cudaSuccess) allocs.push_back((void *)*p);
         return e;
     }
@@ -194,10 +197,13 @@ struct gr_fa2 {
         for (int i = 0; i < 4; i++)
             if (ev[i]) cudaEventDestroy(ev[i]);
         if (flush) cudaFree(flush);
-        for (void *p : allocs) cudaFree(p);
+        for (void *p : allocs) cudaFreeAsync(p, stream);
         sorter.release();
         scanner.release();
-        if (own_stream && stream) cudaStreamDestroy(stream);
+        if (own_stream && stream) {
+            cudaStreamSynchronize(stream);
+            cudaStreamDestroy(stream);
+        }
     }
     uint32_t bnd_blocks() const { return std::max<uint32_t>(1, std::min<uint32_t>(div_up(n, BND_THREADS), 592)); }
 };
@@ -243,8 +249,8 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
     size_t np = std::max<size_t>((size_t)h->bnd_blocks() * 3 * D, 2 * (size_t)div_up(n, FRC_THREADS)) + 8;
     A(h->part, np);
 #undef A
-    if ((e = h->sorter.init(n))) return e;
-    if ((e = h->scanner.init(n))) return e;
+    if ((e = h->sorter.init(n, h->stream, true))) return e;
+    if ((e = h->scanner.init(n, h->stream, true))) return e;
     return cudaSuccess;
 }
 
@@ -429,6 +435,24 @@ static int build_segments(gr_fa2 *h) {
     return GR_OK;
 }
 
+// Once per device and process: the default stream-ordered pool keeps the memory
+// it is given back instead of returning it to the device, so the next handle's
+// buffers come from the pool. A process setting; nothing on the GPU outlives it.
+static void keep_pool() {
+    static std::mutex mu;
+    static std::vector<int> done;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    std::lock_guard<std::mutex> lock(mu);
+    if (std::find(done.begin(), done.end(), dev) != done.end()) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    done.push_back(dev);
+}
+
 static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
                        const double *weight, const uint8_t *params, size_t params_len, const float *pos0,
                        bool tick_buffers = true) {
@@ -468,6 +492,7 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
             break;
         }
         h->own_stream = true;
+        keep_pool();
         cudaStream_t s = h->stream;
         cudaError_t e = cudaSuccess;
         // --- simple graph + CSR on the device
@@ -478,27 +503,21 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
         RadixSorter esort;
         Scanner escan;
         uint32_t ms = 0;
+        // create's own buffers: the stream-ordered pool, freed on the stream
+        auto tmp = [&](auto **p, size_t bytes) { return cudaMallocAsync((void **)p, bytes, s); };
         auto cleanup = [&]() {
-            cudaFree(d_src);
-            cudaFree(d_dst);
-            cudaFree(d_w);
-            cudaFree(d_err);
-            cudaFree(ek);
-            cudaFree(ev);
-            cudaFree(dk);
-            cudaFree(dv);
-            cudaFree(eflag);
-            cudaFree(eexcl);
-            cudaFree(ms_d);
+            for (void *p : {(void *)d_src, (void *)d_dst, (void *)d_w, (void *)d_err, (void *)ek, (void *)ev,
+                            (void *)dk, (void *)dv, (void *)eflag, (void *)eexcl, (void *)ms_d})
+                if (p) cudaFreeAsync(p, s);
             esort.release();
             escan.release();
         };
         const uint64_t cap = std::max<uint64_t>(2 * m, 1);
-        if ((e = cudaMalloc(&d_err, 2 * sizeof(uint32_t))) || (e = cudaMalloc(&ms_d, 2 * sizeof(uint32_t))) ||
-            (e = cudaMalloc(&ek, cap * sizeof(uint64_t))) || (e = cudaMalloc(&ev, cap * sizeof(uint32_t))) ||
-            (e = cudaMalloc(&dk, cap * sizeof(uint64_t))) || (e = cudaMalloc(&dv, cap * sizeof(uint32_t))) ||
-            (e = cudaMalloc(&eflag, cap * sizeof(uint32_t))) || (e = cudaMalloc(&eexcl, cap * sizeof(uint32_t))) ||
-            (e = esort.init((uint32_t)cap)) || (e = escan.init((uint32_t)cap))) {
+        if ((e = tmp(&d_err, 2 * sizeof(uint32_t))) || (e = tmp(&ms_d, 2 * sizeof(uint32_t))) ||
+            (e = tmp(&ek, cap * sizeof(uint64_t))) || (e = tmp(&ev, cap * sizeof(uint32_t))) ||
+            (e = tmp(&dk, cap * sizeof(uint64_t))) || (e = tmp(&dv, cap * sizeof(uint32_t))) ||
+            (e = tmp(&eflag, cap * sizeof(uint32_t))) || (e = tmp(&eexcl, cap * sizeof(uint32_t))) ||
+            (e = esort.init((uint32_t)cap, s, true)) || (e = escan.init((uint32_t)cap, s, true))) {
             cleanup();
             rc = set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
             break;
@@ -506,8 +525,7 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
         cudaMemsetAsync(d_err, 0, 2 * sizeof(uint32_t), s);
         cudaMemsetAsync(ms_d, 0, 2 * sizeof(uint32_t), s);
         if (m) {
-            if ((e = cudaMalloc(&d_src, m * 4)) || (e = cudaMalloc(&d_dst, m * 4)) ||
-                (weight && (e = cudaMalloc(&d_w, m * 8)))) {
+            if ((e = tmp(&d_src, m * 4)) || (e = tmp(&d_dst, m * 4)) || (weight && (e = tmp(&d_w, m * 8)))) {
                 cleanup();
                 rc = set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
                 break;
@@ -557,7 +575,7 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
             cudaMemcpyAsync(h->csr_simple, dv, 2 * (size_t)ms * 4, cudaMemcpyDeviceToDevice, s);
         }
         float *d_xyz = nullptr;
-        if ((e = cudaMalloc(&d_xyz, std::max<size_t>(xyz.size(), 1) * 4))) {
+        if ((e = tmp(&d_xyz, std::max<size_t>(xyz.size(), 1) * 4))) {
             cleanup();
             rc = set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
             break;
@@ -575,9 +593,9 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
         init.converged = n == 0 ? 1u : 0u;
         cudaMemcpyAsync(h->st, &init, sizeof init, cudaMemcpyHostToDevice, s);
         cudaMemcpyAsync(hdr, d_err, sizeof hdr, cudaMemcpyDeviceToHost, s);
-        e = cudaStreamSynchronize(s);
-        cudaFree(d_xyz);
+        cudaFreeAsync(d_xyz, s);
         cleanup();
+        e = cudaStreamSynchronize(s);
         if (e) {
             rc = set_err(GR_CUDA_ERROR, cudaGetErrorString(e));
             break;
@@ -2185,7 +2203,7 @@ int gr_force_session_use_mesh(gr_force_session *S) {
         (e = t->alloc(&S->pm_key, n)) || (e = t->alloc(&S->pm_val, n)) || (e = t->alloc(&S->pm_frac, n)) ||
         (e = t->alloc(&S->pm_cs, NN)) || (e = t->alloc(&S->pm_ce, NN)) || (e = t->alloc(&S->ga, NN)) ||
         (e = t->alloc(&S->gk, NN)) || (e = t->alloc(&S->gt, NN)) || (e = t->alloc(&S->tw, side / 2)) ||
-        (e = S->pm_sorter.init(std::max<uint32_t>(n, 1))))
+        (e = S->pm_sorter.init(std::max<uint32_t>(n, 1), t->stream, true)))
         return set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
     // fft.rs Plan::new root: e^(-i TAU k / side), FP64 then narrowed
     std::vector<float2> tw(side / 2);

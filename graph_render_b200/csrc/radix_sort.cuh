@@ -416,26 +416,44 @@ struct RadixSorter {
     uint32_t *os_ghist = nullptr;   // OS_MAX_PASSES * RS_BINS digit counts, then OS_MAX_PASSES tile counters
     uint32_t *os_status = nullptr;  // OS_MAX_PASSES * os_tiles * RS_BINS look-back words
 
-    cudaError_t init(uint32_t capacity) {
+    // With a stream, the buffers come from the device's stream-ordered pool on it
+    // and go back to it on release (no device-wide synchronisation).
+    cudaStream_t pool_stream = nullptr;
+    bool pooled = false;
+    template <typename T>
+    cudaError_t get(T **p, size_t bytes) {
+        return pooled ? cudaMallocAsync((void **)p, bytes, pool_stream) : cudaMalloc((void **)p, bytes);
+    }
+    void put(void *p) {
+        if (!p) return;
+        if (pooled)
+            cudaFreeAsync(p, pool_stream);
+        else
+            cudaFree(p);
+    }
+
+    cudaError_t init(uint32_t capacity, cudaStream_t s = nullptr, bool pool = false) {
         cap = capacity ? capacity : 1;
         ntiles = div_up(cap, RS_TILE);
         os_tiles = div_up(cap, OS_T * OS_I);
+        pool_stream = s;
+        pooled = pool;
         cudaError_t e;
-        if ((e = cudaMalloc(&os_ghist, (size_t)OS_MAX_PASSES * (RS_BINS + 1) * sizeof(uint32_t)))) return e;
-        if ((e = cudaMalloc(&os_status, (size_t)OS_MAX_PASSES * os_tiles * RS_BINS * sizeof(uint32_t)))) return e;
-        if ((e = cudaMalloc(&k_alt, (size_t)cap * sizeof(uint64_t)))) return e;
-        if ((e = cudaMalloc(&v_alt, (size_t)cap * sizeof(uint32_t)))) return e;
-        if ((e = cudaMalloc(&hist, (size_t)RS_BINS * ntiles * sizeof(uint32_t)))) return e;
-        if ((e = cudaMalloc(&totals, (size_t)8 * RS_BINS * sizeof(uint32_t)))) return e;
+        if ((e = get(&os_ghist, (size_t)OS_MAX_PASSES * (RS_BINS + 1) * sizeof(uint32_t)))) return e;
+        if ((e = get(&os_status, (size_t)OS_MAX_PASSES * os_tiles * RS_BINS * sizeof(uint32_t)))) return e;
+        if ((e = get(&k_alt, (size_t)cap * sizeof(uint64_t)))) return e;
+        if ((e = get(&v_alt, (size_t)cap * sizeof(uint32_t)))) return e;
+        if ((e = get(&hist, (size_t)RS_BINS * ntiles * sizeof(uint32_t)))) return e;
+        if ((e = get(&totals, (size_t)8 * RS_BINS * sizeof(uint32_t)))) return e;
         return cudaSuccess;
     }
     void release() {
-        if (k_alt) cudaFree(k_alt);
-        if (v_alt) cudaFree(v_alt);
-        if (hist) cudaFree(hist);
-        if (totals) cudaFree(totals);
-        if (os_ghist) cudaFree(os_ghist);
-        if (os_status) cudaFree(os_status);
+        put(k_alt);
+        put(v_alt);
+        put(hist);
+        put(totals);
+        put(os_ghist);
+        put(os_status);
         os_ghist = nullptr;
         os_status = nullptr;
         k_alt = nullptr;

@@ -120,13 +120,23 @@ sc_down(const uint32_t *__restrict__ in, uint32_t *__restrict__ out, uint32_t n_
 struct Scanner {
     uint32_t cap = 0, nb = 0;
     uint32_t *bsum = nullptr;
-    cudaError_t init(uint32_t capacity) {
+    cudaStream_t pool_stream = nullptr;  // with pooled: stream-ordered pool allocation on it
+    bool pooled = false;
+    cudaError_t init(uint32_t capacity, cudaStream_t s = nullptr, bool pool = false) {
         cap = capacity ? capacity : 1;
         nb = div_up(cap, SC_TILE);
-        return cudaMalloc(&bsum, (size_t)nb * sizeof(uint32_t));
+        pool_stream = s;
+        pooled = pool;
+        const size_t bytes = (size_t)nb * sizeof(uint32_t);
+        return pooled ? cudaMallocAsync((void **)&bsum, bytes, s) : cudaMalloc(&bsum, bytes);
     }
     void release() {
-        if (bsum) cudaFree(bsum);
+        if (bsum) {
+            if (pooled)
+                cudaFreeAsync(bsum, pool_stream);
+            else
+                cudaFree(bsum);
+        }
         bsum = nullptr;
     }
     void scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev, uint32_t n_add,
