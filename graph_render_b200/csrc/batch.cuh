@@ -385,7 +385,8 @@ __global__ void __launch_bounds__(BT) k_batch(BatchArgs A) {
                 assign_leaf<D>(s, nu, ncells, s_root_w, S.bt, S.sp, S.P, S.cells_at, S.leaf_start, S.leaf_body,
                                S.int_body, S.leaf_coinc, S.cells, S.leaf_pre, &s_st.error);
             __syncthreads();
-            // ---- repulsion walk: warp w takes groups of 32 sorted nodes
+            // ---- repulsion walk: warp w takes groups of 32 sorted nodes, one per lane
+            //      (walk_lane: the same forces, bit for bit, as the warp-union walk)
             {
                 WalkView V{S.cells, S.sp, S.sorig, S.uid, S.leaf_pre, n, ncells, s_st.iter_no, G.seed, G.kr, G.th2,
                            &s_st.error};
@@ -393,7 +394,7 @@ __global__ void __launch_bounds__(BT) k_batch(BatchArgs A) {
                 for (uint32_t base = (uint32_t)w * GR_WARP; base < n; base += BT) {
                     float f0, f1, f2;
                     uint32_t nf, np_;
-                    walk_group<D>(V, base + lane, f0, f1, f2, nf, np_);
+                    walk_lane<D>(V, base + lane, f0, f1, f2, nf, np_);
                     const uint32_t p = base + lane;
                     if (p < n) {
                         const uint32_t oi = S.sorig[p];
