@@ -162,102 +162,128 @@ __device__ __forceinline__ void walk_group(const WalkView &V, uint32_t p, float 
 // the union of its 32 paths. Each lane meets its cells in the same preorder and
 // adds the same terms in the same order as walk_group, so the forces are
 // bit-identical; only the schedule differs.
+// One node's per-lane walk, as state and one cell visit at a time.
+struct LaneNode {
+    float4 me;
+    uint32_t p, mylp, oi, k;
+    float mk, f0, f1, f2;
+    uint32_t nfar, npair;
+};
+
+template <int D>
+__device__ __forceinline__ void lane_init(const WalkView &V, uint32_t p, LaneNode &X) {
+    const bool valid = p < V.n;
+    X.p = p;
+    X.me = valid ? V.sp[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+    X.mylp = valid ? V.leaf_pre[V.uid[p]] : 0u;
+    X.oi = valid ? V.sorig[p] : 0u;
+    X.mk = X.me.w * V.kr;
+    X.f0 = X.f1 = X.f2 = 0.f;
+    X.nfar = X.npair = 0;
+    X.k = valid ? 0u : V.ncells;
+}
+
+// The visit of cell X.k (X.k < ncells): a body term, a leaf's pairs, or a
+// descent; X.k moves on.
+template <int D>
+__device__ __forceinline__ void lane_step(const WalkView &V, LaneNode &X) {
+    const Cells cells = V.cells;
+    const float4 *__restrict__ sp = V.sp;
+    const uint32_t n = V.n, iter = V.iter, k = X.k, oi = X.oi;
+    const float4 me = X.me;
+    const float th2 = V.th2, mk = X.mk;
+    const float4 A = __ldg(&cells.A[k]);
+    const float4 B = __ldg(&cells.B[k]);
+    int32_t sk;
+    uint32_t start;
+    float cx, cy, cz, cm, w2, lx, ly, lz;
+    if (D == 2) {
+        cx = A.x; cy = A.y; cz = 0.f; cm = A.z; w2 = A.w;
+        lx = B.x; ly = B.y; lz = 0.f;
+        sk = __float_as_int(B.z);
+        start = __float_as_uint(B.w);
+    } else {
+        const int2 Cc = __ldg(&cells.C[k]);
+        cx = A.x; cy = A.y; cz = A.z; cm = A.w;
+        lx = B.x; ly = B.y; lz = B.z; w2 = B.w;
+        sk = Cc.x;
+        start = (uint32_t)Cc.y;
+    }
+    const bool leaf = sk < 0;
+    uint32_t skip = leaf ? k + 1 : (uint32_t)sk;
+    skip = max(skip, k + 1);  // every step moves forward, whatever a cell holds
+    const bool holds = (k <= X.mylp) && (X.mylp < skip);
+    const float dx = (me.x - cx) - lx;
+    const float dy = (me.y - cy) - ly;
+    const float dz = (D == 3) ? (me.z - cz) - lz : 0.f;
+    const float d2 = (D == 3) ? dx * dx + dy * dy + dz * dz : dx * dx + dy * dy;
+    const bool far = !holds && w2 < th2 * d2;  // w2 > 0, so this is false at d2 == 0
+    // The common outcomes without a branch: a body term (far cell, or a
+    // one-point leaf's pair) is added, anything else adds +-0 (an exact no-op:
+    // the sums start at +0 and never hold -0); the walk moves to skip or k + 1.
+    const bool body = far || (sk == -1 && !holds && d2 > 0.f);
+    const float fb = __fdividef(mk * cm, d2);
+    const float f = body ? fb : 0.f;
+    X.f0 += dx * f;
+    X.f1 += dy * f;
+    if (D == 3) X.f2 += dz * f;
+    X.nfar += far ? 1u : 0u;
+    X.npair += (body && !far) ? 1u : 0u;
+    if (!leaf || body) {
+        X.k = body ? skip : k + 1;
+    } else if (!holds && sk == -1) {  // coincident one-point leaf: the jiggle
+        const uint32_t oj = __ldg(&V.sorig[start]);
+        const float sg = oi < oj ? 1.f : -1.f;
+        const float ex = sg * (float)jiggle(V.seed, iter, 0, oi, oj);
+        const float ey = sg * (float)jiggle(V.seed, iter, 1, oi, oj);
+        const float ez = (D == 3) ? sg * (float)jiggle(V.seed, iter, 2, oi, oj) : 0.f;
+        const float e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
+        const float g = __fdividef(mk * cm, e2);
+        X.f0 += ex * g;
+        X.f1 += ey * g;
+        if (D == 3) X.f2 += ez * g;
+        X.npair++;
+        X.k = k + 1;
+    } else {  // several points (or this node's own leaf): exact pairs
+        int32_t cnt = -sk;
+        if (start >= n || (uint32_t)cnt > n - start) {
+            atomicOr(V.err, (uint32_t)ERR_TREE);
+            cnt = 0;
+        }
+        for (int32_t q = 0; q < cnt; q++) {
+            const uint32_t jp = start + (uint32_t)q;
+            if (jp == X.p) continue;
+            const float4 o = __ldg(&sp[jp]);
+            float ex = me.x - o.x, ey = me.y - o.y, ez = (D == 3) ? me.z - o.z : 0.f;
+            if (ex == 0.f && ey == 0.f && (D == 2 || ez == 0.f)) {
+                const uint32_t oj = __ldg(&V.sorig[jp]);
+                const float sg = oi < oj ? 1.f : -1.f;
+                ex = sg * (float)jiggle(V.seed, iter, 0, oi, oj);
+                ey = sg * (float)jiggle(V.seed, iter, 1, oi, oj);
+                if (D == 3) ez = sg * (float)jiggle(V.seed, iter, 2, oi, oj);
+            }
+            const float e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
+            const float g = __fdividef(mk * o.w, e2);
+            X.f0 += ex * g;
+            X.f1 += ey * g;
+            if (D == 3) X.f2 += ez * g;
+            X.npair++;
+        }
+        X.k = k + 1;
+    }
+}
+
 template <int D>
 __device__ __forceinline__ void walk_lane(const WalkView &V, uint32_t p, float &f0, float &f1, float &f2,
                                           uint32_t &nfar, uint32_t &npair) {
-    const Cells cells = V.cells;
-    const float4 *__restrict__ sp = V.sp;
-    const uint32_t n = V.n, ncells = V.ncells, iter = V.iter;
-    const bool valid = p < n;
-    const float4 me = valid ? sp[p] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const uint32_t mylp = valid ? V.leaf_pre[V.uid[p]] : 0u;
-    const uint32_t oi = valid ? V.sorig[p] : 0u;
-    f0 = f1 = f2 = 0.f;
-    nfar = npair = 0;
-    const float th2 = V.th2, mk = me.w * V.kr;
-    uint32_t k = valid ? 0u : ncells;
-    while (k < ncells) {
-        const float4 A = __ldg(&cells.A[k]);
-        const float4 B = __ldg(&cells.B[k]);
-        int32_t sk;
-        uint32_t start;
-        float cx, cy, cz, cm, w2, lx, ly, lz;
-        if (D == 2) {
-            cx = A.x; cy = A.y; cz = 0.f; cm = A.z; w2 = A.w;
-            lx = B.x; ly = B.y; lz = 0.f;
-            sk = __float_as_int(B.z);
-            start = __float_as_uint(B.w);
-        } else {
-            const int2 Cc = __ldg(&cells.C[k]);
-            cx = A.x; cy = A.y; cz = A.z; cm = A.w;
-            lx = B.x; ly = B.y; lz = B.z; w2 = B.w;
-            sk = Cc.x;
-            start = (uint32_t)Cc.y;
-        }
-        const bool leaf = sk < 0;
-        uint32_t skip = leaf ? k + 1 : (uint32_t)sk;
-        skip = max(skip, k + 1);  // every step moves forward, whatever a cell holds
-        const bool holds = (k <= mylp) && (mylp < skip);
-        const float dx = (me.x - cx) - lx;
-        const float dy = (me.y - cy) - ly;
-        const float dz = (D == 3) ? (me.z - cz) - lz : 0.f;
-        const float d2 = (D == 3) ? dx * dx + dy * dy + dz * dz : dx * dx + dy * dy;
-        const bool far = !holds && w2 < th2 * d2;  // w2 > 0, so this is false at d2 == 0
-        // The common outcomes without a branch: a body term (far cell, or a
-        // one-point leaf's pair) is added, anything else adds +-0 (an exact no-op:
-        // the sums start at +0 and never hold -0); the walk moves to skip or k + 1.
-        const bool body = far || (sk == -1 && !holds && d2 > 0.f);
-        const float fb = __fdividef(mk * cm, d2);
-        const float f = body ? fb : 0.f;
-        f0 += dx * f;
-        f1 += dy * f;
-        if (D == 3) f2 += dz * f;
-        nfar += far ? 1u : 0u;
-        npair += (body && !far) ? 1u : 0u;
-        const uint32_t kn = body ? skip : k + 1;
-        if (!leaf || body) {
-            k = kn;
-        } else if (!holds && sk == -1) {  // coincident one-point leaf: the jiggle
-            const uint32_t oj = __ldg(&V.sorig[start]);
-            const float sg = oi < oj ? 1.f : -1.f;
-            const float ex = sg * (float)jiggle(V.seed, iter, 0, oi, oj);
-            const float ey = sg * (float)jiggle(V.seed, iter, 1, oi, oj);
-            const float ez = (D == 3) ? sg * (float)jiggle(V.seed, iter, 2, oi, oj) : 0.f;
-            const float e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
-            const float f = __fdividef(mk * cm, e2);
-            f0 += ex * f;
-            f1 += ey * f;
-            if (D == 3) f2 += ez * f;
-            npair++;
-            k = k + 1;
-        } else {  // several points (or this node's own leaf): exact pairs
-            int32_t cnt = -sk;
-            if (start >= n || (uint32_t)cnt > n - start) {
-                atomicOr(V.err, (uint32_t)ERR_TREE);
-                cnt = 0;
-            }
-            for (int32_t q = 0; q < cnt; q++) {
-                const uint32_t jp = start + (uint32_t)q;
-                if (jp == p) continue;
-                const float4 o = __ldg(&sp[jp]);
-                float ex = me.x - o.x, ey = me.y - o.y, ez = (D == 3) ? me.z - o.z : 0.f;
-                if (ex == 0.f && ey == 0.f && (D == 2 || ez == 0.f)) {
-                    const uint32_t oj = __ldg(&V.sorig[jp]);
-                    const float sg = oi < oj ? 1.f : -1.f;
-                    ex = sg * (float)jiggle(V.seed, iter, 0, oi, oj);
-                    ey = sg * (float)jiggle(V.seed, iter, 1, oi, oj);
-                    if (D == 3) ez = sg * (float)jiggle(V.seed, iter, 2, oi, oj);
-                }
-                const float e2 = (D == 3) ? ex * ex + ey * ey + ez * ez : ex * ex + ey * ey;
-                const float f = __fdividef(mk * o.w, e2);
-                f0 += ex * f;
-                f1 += ey * f;
-                if (D == 3) f2 += ez * f;
-                npair++;
-            }
-            k = k + 1;
-        }
-    }
+    LaneNode X;
+    lane_init<D>(V, p, X);
+    while (X.k < V.ncells) lane_step<D>(V, X);
+    f0 = X.f0;
+    f1 = X.f1;
+    f2 = X.f2;
+    nfar = X.nfar;
+    npair = X.npair;
 }
 
 // One node of a two-node walk (walk_pair): its own state and its visit of

@@ -149,8 +149,8 @@ def test_walk_schedules_give_bit_identical_forces_and_tuning_keeps_the_state(dim
         chosen, ms = eng.tune(2)
         assert chosen in (0, 1, 2) and all(ms[i] > 0 for i in (0, 1, 2))
         assert np.array_equal(eng.positions(), pos)
-    assert np.array_equal(outs[0][0], outs[1][0])
-    assert np.array_equal(outs[0][0], outs[2][0])
+    for sch in (1, 2):
+        assert np.array_equal(outs[0][0], outs[sch][0])
 
 
 def _full_sort_forces(n, src, dst, pos, prm):
