@@ -82,6 +82,7 @@ __host__ __device__ inline size_t slot_carve(unsigned char *base, uint32_t nmax,
     v.bt.visit = slot_take<uint32_t>(base, off, n);
     v.bt.cell_of = nullptr;
     v.bt.rec = nullptr;
+    v.bt.levels = nullptr;
     v.leaf_body = slot_take<Body>(base, off, n);
     v.int_body = slot_take<Body>(base, off, n);
     v.leaf_coinc = slot_take<uint8_t>(base, off, n);

@@ -144,7 +144,7 @@ struct gr_fa2 {
     uint32_t *too_long = nullptr;  // count of runs of equal high key words longer than 64
     uint2 *long_runs = nullptr;    // those runs (start, length)
     uint32_t *vals = nullptr, *sorig = nullptr, *flag = nullptr, *excl = nullptr, *uid = nullptr;
-    uint32_t *leaf_start = nullptr, *cells_at = nullptr, *P = nullptr, *leaf_pre = nullptr;
+    uint32_t *leaf_start = nullptr, *levels = nullptr, *P = nullptr, *leaf_pre = nullptr;
     float4 *sp = nullptr;
     BinTree bt{};
     Body *leaf_body = nullptr, *int_body = nullptr;
@@ -223,7 +223,7 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
     A(h->excl, n);
     A(h->uid, n);
     A(h->leaf_start, (size_t)n + 1);
-    A(h->cells_at, n);
+    A(h->levels, n);
     A(h->P, (size_t)n + 1);
     A(h->leaf_pre, n);
     A(h->sp, n);
@@ -305,19 +305,24 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
             h->sorter.sort(h->keys, h->vals, n, 64, s, conv);
         k_gather<<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals, h->sp, h->sorig, h->flag);
         h->scanner.scan(h->flag, h->excl, n, nullptr, 0, &st->n_unique, nullptr, s, conv);
-        k_leaves<<<gn, 256, 0, s>>>(n, st, h->keys, h->flag, h->excl, h->leaf_start, h->ukey, h->uid);
-        k_karras<<<gn, 256, 0, s>>>(st, h->ukey, h->bt);
+        k_leaves<<<gn, 256, 0, s>>>(n, st, h->keys, h->flag, h->excl, h->leaf_start, h->ukey, h->uid, h->levels);
         const bool adjoint = h->bt.cell_of != nullptr;  // the adjoint reads leaf and node bodies as arrays
+        BinTree bt = h->bt;  // the tick itself reads only the packed records and leaf_parent
+        bt.levels = h->levels;
+        if (!adjoint) {
+            bt.first = bt.last = bt.left = bt.right = bt.visit = nullptr;
+            bt.delta = bt.int_parent = nullptr;
+        }
+        k_karras<D><<<gn, 256, 0, s>>>(st, h->ukey, bt);
         if (adjoint) k_leaf_body<D><<<gn, 256, 0, s>>>(st, h->sp, h->leaf_start, h->leaf_body, h->leaf_coinc);
         const uint32_t ab = div_up(n, AG_TILE);
         k_dd_reduce<D><<<ab, AG_T, 0, s>>>(st, h->sp, h->leaf_start, h->dd_bsum);
         k_dd_blocks<D><<<1, AG_T, 0, s>>>(st, h->dd_bsum, h->dd_prefix);
         k_dd_down<D><<<ab, AG_T, 0, s>>>(st, h->sp, h->leaf_start, h->dd_bsum, h->dd_prefix, h->leaf_coinc);
         if (adjoint) k_node_body<<<gn, 256, 0, s>>>(st, h->bt, h->dd_prefix, h->int_body);
-        k_count<D><<<gn, 256, 0, s>>>(st, h->bt, h->cells_at);
-        h->scanner.scan(h->cells_at, h->P, n, &st->n_unique, 0, &st->n_cells, nullptr, s, conv);
-        k_assign_dd<D><<<gn, 256, 0, s>>>(st, h->bt, h->sp, h->P, h->cells_at, h->leaf_start, h->dd_prefix,
-                                          h->leaf_coinc, h->cells, h->leaf_pre, st);
+        h->scanner.scan_levels(h->levels, h->P, n, &st->n_unique, &st->n_cells, s, conv);
+        k_assign_cells<D><<<2 * gn, 256, 0, s>>>(st, bt, gn * 256, h->sp, h->P, h->levels, h->leaf_start,
+                                                 h->dd_prefix, h->leaf_coinc, h->cells, h->leaf_pre, st);
     }
     if (phases & PH_WALK) {
         WalkParams wp;
@@ -1051,7 +1056,7 @@ static int forces_static(uint32_t n, const float4 *nodes, const uint32_t *rp, co
     h.excl = cv.take<uint32_t>(n);
     h.uid = cv.take<uint32_t>(n);
     h.leaf_start = cv.take<uint32_t>((size_t)n + 1);
-    h.cells_at = cv.take<uint32_t>(n);
+    h.levels = cv.take<uint32_t>(n);
     h.P = cv.take<uint32_t>((size_t)n + 1);
     h.leaf_pre = cv.take<uint32_t>(n);
     h.sp = cv.take<float4>(n);

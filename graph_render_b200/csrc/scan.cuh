@@ -16,6 +16,14 @@ __device__ __forceinline__ uint32_t scan_count(uint32_t n_host, const uint32_t *
     return n_dev ? *n_dev + add : n_host;
 }
 
+// The scanned value of an input word: the word itself, or with LV the count
+// 1 + popc(word) of a cell level mask.
+template <bool LV>
+__device__ __forceinline__ uint32_t scan_item(uint32_t x) {
+    return LV ? 1u + (uint32_t)__popc(x) : x;
+}
+
+template <bool LV>
 __global__ void __launch_bounds__(SC_THREADS)
 sc_reduce(const uint32_t *__restrict__ in, uint32_t n_host, const uint32_t *n_dev, uint32_t n_add,
           uint32_t *__restrict__ bsum, const uint32_t *skip) {
@@ -28,7 +36,7 @@ sc_reduce(const uint32_t *__restrict__ in, uint32_t n_host, const uint32_t *n_de
 #pragma unroll
         for (int r = 0; r < SC_ITEMS; r++) {
             uint64_t i = base + (uint64_t)r * SC_THREADS + threadIdx.x;
-            if (i < n) v += in[i];
+            if (i < n) v += scan_item<LV>(in[i]);
         }
     }
     v = __reduce_add_sync(GR_FULL, v);
@@ -77,6 +85,7 @@ sc_blocks(uint32_t *__restrict__ bsum, uint32_t nb, uint32_t *total, uint32_t *t
     }
 }
 
+template <bool LV>
 __global__ void __launch_bounds__(SC_THREADS)
 sc_down(const uint32_t *__restrict__ in, uint32_t *__restrict__ out, uint32_t n_host,
         const uint32_t *n_dev, uint32_t n_add, const uint32_t *__restrict__ bsum, const uint32_t *skip) {
@@ -92,7 +101,7 @@ sc_down(const uint32_t *__restrict__ in, uint32_t *__restrict__ out, uint32_t n_
 #pragma unroll
     for (int r = 0; r < SC_ITEMS; r++) {
         uint64_t i = base + (uint64_t)t * SC_ITEMS + r;
-        x[r] = i < n ? in[i] : 0u;
+        x[r] = i < n ? scan_item<LV>(in[i]) : 0u;
         sum += x[r];
     }
     uint32_t s = sum;
@@ -139,13 +148,23 @@ struct Scanner {
         }
         bsum = nullptr;
     }
-    void scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev, uint32_t n_add,
-              uint32_t *total, uint32_t *total2, cudaStream_t s, const uint32_t *skip = nullptr) {
+    template <bool LV>
+    void run(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev, uint32_t n_add,
+             uint32_t *total, uint32_t *total2, cudaStream_t s, const uint32_t *skip) {
         if (n_host == 0) return;
         uint32_t b = div_up(n_host, SC_TILE);
-        sc_reduce<<<b, SC_THREADS, 0, s>>>(in, n_host, n_dev, n_add, bsum, skip);
+        sc_reduce<LV><<<b, SC_THREADS, 0, s>>>(in, n_host, n_dev, n_add, bsum, skip);
         sc_blocks<<<1, 1024, 0, s>>>(bsum, b, total, total2, skip);
-        sc_down<<<b, SC_THREADS, 0, s>>>(in, out, n_host, n_dev, n_add, bsum, skip);
+        sc_down<LV><<<b, SC_THREADS, 0, s>>>(in, out, n_host, n_dev, n_add, bsum, skip);
+    }
+    void scan(const uint32_t *in, uint32_t *out, uint32_t n_host, const uint32_t *n_dev, uint32_t n_add,
+              uint32_t *total, uint32_t *total2, cudaStream_t s, const uint32_t *skip = nullptr) {
+        run<false>(in, out, n_host, n_dev, n_add, total, total2, s, skip);
+    }
+    // Exclusive scan of 1 + popc(levels[s]): the first cell index of every leaf.
+    void scan_levels(const uint32_t *levels, uint32_t *out, uint32_t n_host, const uint32_t *n_dev,
+                     uint32_t *total, cudaStream_t s, const uint32_t *skip = nullptr) {
+        run<true>(levels, out, n_host, n_dev, 0, total, nullptr, s, skip);
     }
 };
 

@@ -229,11 +229,12 @@ __global__ void k_gather(const float4 *__restrict__ pos, uint32_t n, const DevSt
     flag[p] = (p == 0 || keys[p] != keys[p - 1]) ? 1u : 0u;
 }
 
-// Unique keys: leaf s starts at the first sorted point with its key.
+// Unique keys: leaf s starts at the first sorted point with its key; its cell
+// level mask starts empty.
 __global__ void k_leaves(uint32_t n, const DevState *st, const uint64_t *__restrict__ keys,
                          const uint32_t *__restrict__ flag, const uint32_t *__restrict__ excl,
                          uint32_t *__restrict__ leaf_start, uint64_t *__restrict__ ukey,
-                         uint32_t *__restrict__ uid) {
+                         uint32_t *__restrict__ uid, uint32_t *__restrict__ levels) {
     if (st->converged) return;
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
@@ -242,6 +243,7 @@ __global__ void k_leaves(uint32_t n, const DevState *st, const uint64_t *__restr
     if (f) {
         leaf_start[e] = p;
         ukey[e] = keys[p];
+        if (levels) levels[e] = 0;
     }
     if (p == n - 1) leaf_start[e + f] = n;
 }
@@ -259,6 +261,13 @@ struct BinTree {
     uint32_t *visit;      // bottom-up arrival tickets
     uint32_t *cell_of;    // internal node -> its cell's preorder index, when it is a cell (nullable)
     int4 *rec;            // internal node -> {first, last, parent, delta} in one load (nullable)
+    uint32_t *levels;     // unique leaf s -> bit l set when a cell of level l begins at s (nullable)
+};
+
+// What karras_node found for internal node i: its leaf range, split and
+// common-prefix length.
+struct KarrasNode {
+    int32_t first, last, gamma, delta;
 };
 
 __device__ __forceinline__ int kdelta(const uint64_t *__restrict__ k, int32_t a, int32_t b, int32_t nu) {
@@ -266,8 +275,10 @@ __device__ __forceinline__ int kdelta(const uint64_t *__restrict__ k, int32_t a,
     return __clzll(k[a] ^ k[b]);
 }
 
-// Internal node i of the binary radix tree over nu unique keys.
-__device__ __forceinline__ void karras_node(int32_t i, int32_t nu, const uint64_t *__restrict__ k, BinTree t) {
+// Internal node i of the binary radix tree over nu unique keys. The per-node
+// arrays (first .. int_parent, visit) are written when t.left is set; the
+// packed records when t.rec is set; leaf_parent always.
+__device__ __forceinline__ KarrasNode karras_node(int32_t i, int32_t nu, const uint64_t *__restrict__ k, BinTree t) {
     const int dir = (kdelta(k, i, i + 1, nu) - kdelta(k, i, i - 1, nu)) > 0 ? 1 : -1;
     const int dmin = kdelta(k, i, i - dir, nu);
     int32_t lmax = 2;
@@ -285,10 +296,13 @@ __device__ __forceinline__ void karras_node(int32_t i, int32_t nu, const uint64_
     } while (step > 1);
     const int32_t gamma = i + s * dir + (dir < 0 ? -1 : 0);
     const int32_t first = min(i, j), last = max(i, j);
-    t.first[i] = (uint32_t)first;
-    t.last[i] = (uint32_t)last;
-    t.delta[i] = dnode;
-    t.visit[i] = 0;
+    const bool arrays = t.left != nullptr;
+    if (arrays) {
+        t.first[i] = (uint32_t)first;
+        t.last[i] = (uint32_t)last;
+        t.delta[i] = dnode;
+        t.visit[i] = 0;
+    }
     if (t.rec) {  // z (parent) is written by the parent
         int *r = (int *)&t.rec[i];
         r[0] = first;
@@ -296,34 +310,63 @@ __device__ __forceinline__ void karras_node(int32_t i, int32_t nu, const uint64_
         r[3] = dnode;
     }
     if (first == gamma) {
-        t.left[i] = (uint32_t)gamma | LEAF_BIT;
+        if (arrays) t.left[i] = (uint32_t)gamma | LEAF_BIT;
         t.leaf_parent[gamma] = i;
     } else {
-        t.left[i] = (uint32_t)gamma;
-        t.int_parent[gamma] = i;
+        if (arrays) {
+            t.left[i] = (uint32_t)gamma;
+            t.int_parent[gamma] = i;
+        }
         if (t.rec) ((int *)&t.rec[gamma])[2] = i;
     }
     if (last == gamma + 1) {
-        t.right[i] = (uint32_t)(gamma + 1) | LEAF_BIT;
+        if (arrays) t.right[i] = (uint32_t)(gamma + 1) | LEAF_BIT;
         t.leaf_parent[gamma + 1] = i;
     } else {
-        t.right[i] = (uint32_t)(gamma + 1);
-        t.int_parent[gamma + 1] = i;
+        if (arrays) {
+            t.right[i] = (uint32_t)(gamma + 1);
+            t.int_parent[gamma + 1] = i;
+        }
         if (t.rec) ((int *)&t.rec[gamma + 1])[2] = i;
     }
     if (i == 0) {
-        t.int_parent[0] = -1;
+        if (arrays) t.int_parent[0] = -1;
         if (t.rec) ((int *)&t.rec[0])[2] = -1;
+    }
+    return KarrasNode{first, last, gamma, dnode};
+}
+
+// The cells among node i's internal children (and the root): a node is a cell
+// when its level (common prefix / D) differs from its parent's. Each cell sets
+// bit `level` of its first leaf's mask; the cells beginning at one leaf lie on
+// one chain of ancestors and have distinct levels, so leaf s starts
+// 1 + popc(levels[s]) cells and the level-l one is the popc(levels[s] & (2^l -
+// 1))-th of them in preorder. A level is at most 31 (2D, 64-bit keys) or 20
+// (3D, 63-bit keys).
+template <int D>
+__device__ __forceinline__ void mark_cells(int32_t i, int32_t nu, const uint64_t *__restrict__ k,
+                                           const KarrasNode &q, uint32_t *__restrict__ levels) {
+    const int lv = q.delta / D;
+    if (i == 0) atomicOr(&levels[0], 1u << lv);
+    if (q.first != q.gamma) {  // left child [first, gamma]
+        const int c = kdelta(k, q.first, q.gamma, nu) / D;
+        if (c != lv) atomicOr(&levels[q.first], 1u << c);
+    }
+    if (q.last != q.gamma + 1) {  // right child [gamma + 1, last]
+        const int c = kdelta(k, q.gamma + 1, q.last, nu) / D;
+        if (c != lv) atomicOr(&levels[q.gamma + 1], 1u << c);
     }
 }
 
+template <int D>
 __global__ void k_karras(const DevState *st, const uint64_t *__restrict__ k, BinTree t) {
     if (st->converged) return;
     const int32_t nu = (int32_t)st->n_unique;
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0 && nu == 1) t.leaf_parent[0] = -1;
     if (i >= nu - 1) return;
-    karras_node(i, nu, k, t);
+    const KarrasNode q = karras_node(i, nu, k, t);
+    if (t.levels) mark_cells<D>(i, nu, k, q, t.levels);
 }
 
 // Leaf s's FP64 sums, then the bottom-up pass: the second thread to reach a
@@ -609,32 +652,6 @@ __device__ __forceinline__ uint32_t count_leaf(uint32_t s, const BinTree &t) {
     return c;
 }
 
-// count_leaf over the packed records: one dependent load per level (the
-// parent's record tells whether this node is a cell and is the next level).
-template <int D>
-__device__ __forceinline__ uint32_t count_leaf_rec(uint32_t s, const BinTree &t) {
-    uint32_t c = 1;
-    const int32_t par = t.leaf_parent[s];
-    if (par < 0) return c;
-    int4 R = t.rec[par];
-    for (int depth = 0; R.x == (int)s && depth <= 66; depth++) {
-        if (R.z < 0) return c + 1;  // the root is a cell
-        const int4 Q = t.rec[R.z];
-        if (R.w / D != Q.w / D) c++;
-        R = Q;
-    }
-    return c;
-}
-
-template <int D>
-__global__ void k_count(const DevState *st, BinTree t, uint32_t *__restrict__ cells_at) {
-    if (st->converged) return;
-    const uint32_t nu = st->n_unique;
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nu) return;
-    cells_at[s] = t.rec ? count_leaf_rec<D>(s, t) : count_leaf<D>(s, t);
-}
-
 // Cell record, 2D: A = {cx, cy, mass, w^2}, B = {cx_lo, cy_lo, skip | -count, start}.
 // 3D: A = {cx, cy, cz, mass}, B = {cx_lo, cy_lo, cz_lo, w^2}, C = {skip | -count, start}.
 // The centre is an FP32 hi/lo pair of the FP64 centre of mass, so a node at
@@ -718,52 +735,63 @@ __device__ __forceinline__ void assign_leaf(uint32_t s, uint32_t nu, uint32_t nc
     if (idx != P[s]) atomicOr(err, (uint32_t)ERR_TREE);
 }
 
-// assign_leaf with the bodies computed on the spot: the leaf's from its points
-// (leaf_sum), each cell ancestor's from the prefix at its range ends
-// (range_body) — the values k_leaf_body and k_node_body store.
+// Every cell at its preorder index, without walking chains: threads
+// [0, n_slots) take unique leaf s = thread (its cell is the last of the
+// 1 + popc(levels[s]) cells beginning at s), threads [n_slots, 2 n_slots) take
+// internal node i = thread - n_slots when it is a cell (level l, first leaf f:
+// index P[f] + popc(levels[f] & (2^l - 1))). A leaf's body comes from its
+// points (leaf_sum), an internal cell's from the prefix at its range ends
+// (range_body); skip(cell) = P[last leaf + 1]. A leaf of coincident points sits
+// one level below its parent cell (where the reference chains them); a leaf of
+// distinct points the key could not separate sits at the key's last level.
 template <int D>
-__global__ void k_assign_dd(const DevState *st, BinTree t, const float4 *__restrict__ sp,
-                            const uint32_t *__restrict__ P, const uint32_t *__restrict__ cells_at,
-                            const uint32_t *__restrict__ leaf_start, const BodyDD *__restrict__ prefix,
-                            const uint8_t *__restrict__ leaf_coinc, Cells cells, uint32_t *__restrict__ leaf_pre,
-                            DevState *stw) {
+__global__ void k_assign_cells(const DevState *st, BinTree t, uint32_t n_slots, const float4 *__restrict__ sp,
+                               const uint32_t *__restrict__ P, const uint32_t *__restrict__ levels,
+                               const uint32_t *__restrict__ leaf_start, const BodyDD *__restrict__ prefix,
+                               const uint8_t *__restrict__ leaf_coinc, Cells cells, uint32_t *__restrict__ leaf_pre,
+                               DevState *stw) {
     if (st->converged) return;
     constexpr int L = Levels<D>::L;
     const uint32_t nu = st->n_unique;
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nu) return;
     const uint32_t ncells = st->n_cells;
     const double rw = st->root_w;
-    uint32_t idx = P[s] + cells_at[s] - 1;
-    int32_t par = t.leaf_parent[s];
-    int4 R = par >= 0 ? t.rec[par] : make_int4(-1, -1, -1, 0);
-    int level = 0;
-    if (par >= 0) level = leaf_coinc[s] ? R.w / D + 1 : L;
-    const uint32_t a0 = leaf_start[s], a1 = leaf_start[s + 1];
-    const float4 one = sp[a0];
-    bool coinc;
-    write_cell<D>(cells, idx, leaf_sum<D>(sp, a0, a1, coinc), level, rw, -(int32_t)(a1 - a0), a0,
-                  a1 - a0 == 1 ? &one : nullptr);
-    if (D == 2 && cells.bounds) write_bounds(cells, idx, one, level, st);
-    leaf_pre[s] = idx;
-    if (par >= 0 && R.x == (int)s) {
-        const BodyDD ps = prefix[s];
-        for (int depth = 0; depth <= 66; depth++) {
-            const int4 Q = R.z >= 0 ? t.rec[R.z] : make_int4(-1, -1, -1, 0);
-            if (R.z < 0 || R.w / D != Q.w / D) {  // par is a cell
-                idx--;
-                const uint32_t end = (uint32_t)R.y + 1;
-                const uint32_t skip = end == nu ? ncells : P[end];
-                write_cell<D>(cells, idx, range_body(ps, prefix[end]), R.w / D, rw, (int32_t)skip, a0);
-                if (D == 2 && cells.bounds) write_bounds(cells, idx, one, R.w / D, st);
-                if (t.cell_of) t.cell_of[par] = idx;
-            }
-            if (R.z < 0 || Q.x != (int)s) break;
-            par = R.z;
-            R = Q;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < n_slots) {
+        const uint32_t s = g;
+        if (s >= nu) return;
+        const uint32_t idx = P[s] + __popc(levels[s]);
+        const int32_t par = t.leaf_parent[s];
+        int level = 0;
+        if (par >= 0) level = leaf_coinc[s] ? t.rec[par].w / D + 1 : L;
+        const uint32_t a0 = leaf_start[s], a1 = leaf_start[s + 1];
+        if (idx >= ncells || a1 <= a0) {
+            atomicOr(&stw->error, (uint32_t)ERR_TREE);
+            return;
         }
+        const float4 one = sp[a0];
+        bool coinc;
+        write_cell<D>(cells, idx, leaf_sum<D>(sp, a0, a1, coinc), level, rw, -(int32_t)(a1 - a0), a0,
+                      a1 - a0 == 1 ? &one : nullptr);
+        if (D == 2 && cells.bounds) write_bounds(cells, idx, one, level, st);
+        leaf_pre[s] = idx;
+        return;
     }
-    if (idx != P[s]) atomicOr(&stw->error, (uint32_t)ERR_TREE);
+    const uint32_t i = g - n_slots;
+    if (i + 1 >= nu) return;
+    const int4 R = t.rec[i];
+    if (R.z >= 0 && R.w / D == t.rec[R.z].w / D) return;  // not a cell: its parent has its level
+    const int lv = R.w / D;
+    const uint32_t f = (uint32_t)R.x, end = (uint32_t)R.y + 1;
+    const uint32_t idx = P[f] + __popc(levels[f] & ((1u << lv) - 1u));
+    const uint32_t skip = end == nu ? ncells : P[end];
+    if (idx >= ncells || skip <= idx || skip > ncells) {
+        atomicOr(&stw->error, (uint32_t)ERR_TREE);
+        return;
+    }
+    const uint32_t a0 = leaf_start[f];
+    write_cell<D>(cells, idx, range_body(prefix[f], prefix[end]), lv, rw, (int32_t)skip, a0);
+    if (D == 2 && cells.bounds) write_bounds(cells, idx, sp[a0], lv, st);
+    if (t.cell_of) t.cell_of[i] = idx;
 }
 
 }  // namespace gr
