@@ -143,12 +143,14 @@ struct gr_fa2 {
     uint64_t *keys = nullptr, *ukey = nullptr;
     uint32_t *too_long = nullptr;  // count of runs of equal high key words longer than 64
     uint2 *long_runs = nullptr;    // those runs (start, length)
-    uint32_t *vals = nullptr, *sorig = nullptr, *flag = nullptr, *excl = nullptr, *uid = nullptr;
+    uint32_t *vals = nullptr, *sorig = nullptr, *uid = nullptr;
     uint32_t *leaf_start = nullptr, *levels = nullptr, *P = nullptr, *leaf_pre = nullptr;
     float4 *sp = nullptr;
     BinTree bt{};
     Body *leaf_body = nullptr, *int_body = nullptr;
-    BodyDD *dd_prefix = nullptr, *dd_bsum = nullptr;
+    DD *dd_prefix = nullptr;             // (n + 1) x (D + 1) double-doubles
+    BodyDD *dd_bsum = nullptr;           // the prefix pass's tile totals
+    uint32_t *dd_flag = nullptr;         // its tile flags and tile counter, then its tile leaf counts
     uint8_t *leaf_coinc = nullptr;
     Cells cells{};
     float *rep = nullptr, *U = nullptr;
@@ -219,8 +221,6 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
     A(h->vals, n);
     A(h->ukey, n);
     A(h->sorig, n);
-    A(h->flag, n);
-    A(h->excl, n);
     A(h->uid, n);
     A(h->leaf_start, (size_t)n + 1);
     A(h->levels, n);
@@ -239,8 +239,9 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
     A(h->leaf_body, n);
     A(h->int_body, n);
     A(h->leaf_coinc, n);
-    A(h->dd_prefix, (size_t)n + 1);
+    A(h->dd_prefix, 4 * ((size_t)n + 1));
     A(h->dd_bsum, div_up(n, AG_TILE) + 1);
+    A(h->dd_flag, 2 * ((size_t)div_up(n, AG_TILE) + 1));
     A(h->cells.A, 2 * (size_t)n);
     A(h->cells.B, 2 * (size_t)n);
     if (D == 3) A(h->cells.C, 2 * (size_t)n);
@@ -298,14 +299,15 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
     const uint32_t *conv = &st->converged;
     if (phases & PH_TREE) {
         k_bounds<D><<<h->bnd_blocks(), BND_THREADS, 0, s>>>(h->pos, n, st, h->part);
-        k_keys<D><<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals);
+        const uint32_t ab = div_up(n, AG_TILE);
+        k_keys<D><<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals, h->dd_flag, ab + 1);
         if (h->long_runs)
             sort_fast(h, s);
         else
             h->sorter.sort(h->keys, h->vals, n, 64, s, conv);
-        k_gather<<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals, h->sp, h->sorig, h->flag);
-        h->scanner.scan(h->flag, h->excl, n, nullptr, 0, &st->n_unique, nullptr, s, conv);
-        k_leaves<<<gn, 256, 0, s>>>(n, st, h->keys, h->flag, h->excl, h->leaf_start, h->ukey, h->uid, h->levels);
+        k_sorted_leaves<D><<<ab, AG_T, 0, s>>>(st, n, h->pos, h->keys, h->vals, h->sp, h->sorig, h->uid,
+                                                h->leaf_start, h->ukey, h->levels, h->dd_bsum, h->dd_flag + ab + 1,
+                                                h->dd_flag, h->dd_prefix);
         const bool adjoint = h->bt.cell_of != nullptr;  // the adjoint reads leaf and node bodies as arrays
         BinTree bt = h->bt;  // the tick itself reads only the packed records and leaf_parent
         bt.levels = h->levels;
@@ -315,14 +317,10 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
         }
         k_karras<D><<<gn, 256, 0, s>>>(st, h->ukey, bt);
         if (adjoint) k_leaf_body<D><<<gn, 256, 0, s>>>(st, h->sp, h->leaf_start, h->leaf_body, h->leaf_coinc);
-        const uint32_t ab = div_up(n, AG_TILE);
-        k_dd_reduce<D><<<ab, AG_T, 0, s>>>(st, h->sp, h->leaf_start, h->dd_bsum);
-        k_dd_blocks<D><<<1, AG_T, 0, s>>>(st, h->dd_bsum, h->dd_prefix);
-        k_dd_down<D><<<ab, AG_T, 0, s>>>(st, h->sp, h->leaf_start, h->dd_bsum, h->dd_prefix, h->leaf_coinc);
-        if (adjoint) k_node_body<<<gn, 256, 0, s>>>(st, h->bt, h->dd_prefix, h->int_body);
+        if (adjoint) k_node_body<D><<<gn, 256, 0, s>>>(st, h->bt, h->dd_prefix, h->int_body);
         h->scanner.scan_levels(h->levels, h->P, n, &st->n_unique, &st->n_cells, s, conv);
         k_assign_cells<D><<<2 * gn, 256, 0, s>>>(st, bt, gn * 256, h->sp, h->P, h->levels, h->leaf_start,
-                                                 h->dd_prefix, h->leaf_coinc, h->cells, h->leaf_pre, st);
+                                                 h->dd_prefix, h->cells, h->leaf_pre, st);
     }
     if (phases & PH_WALK) {
         WalkParams wp;
@@ -1052,8 +1050,6 @@ static int forces_static(uint32_t n, const float4 *nodes, const uint32_t *rp, co
     h.vals = cv.take<uint32_t>(n);
     h.ukey = cv.take<uint64_t>(n);
     h.sorig = cv.take<uint32_t>(n);
-    h.flag = cv.take<uint32_t>(n);
-    h.excl = cv.take<uint32_t>(n);
     h.uid = cv.take<uint32_t>(n);
     h.leaf_start = cv.take<uint32_t>((size_t)n + 1);
     h.levels = cv.take<uint32_t>(n);
@@ -1072,8 +1068,9 @@ static int forces_static(uint32_t n, const float4 *nodes, const uint32_t *rp, co
     h.leaf_body = cv.take<Body>(n);
     h.int_body = cv.take<Body>(n);
     h.leaf_coinc = cv.take<uint8_t>(n);
-    h.dd_prefix = cv.take<BodyDD>((size_t)n + 1);
+    h.dd_prefix = cv.take<DD>(4 * ((size_t)n + 1));
     h.dd_bsum = cv.take<BodyDD>(div_up(n, AG_TILE) + 1);
+    h.dd_flag = cv.take<uint32_t>(2 * ((size_t)div_up(n, AG_TILE) + 1));
     h.cells.A = cv.take<float4>(2 * (size_t)n);
     h.cells.B = cv.take<float4>(2 * (size_t)n);
     h.cells.C = D == 3 ? cv.take<int2>(2 * (size_t)n) : nullptr;

@@ -205,47 +205,18 @@ k_bounds(const float4 *__restrict__ pos, uint32_t n, DevState *st, double *__res
 
 // Morton key of every node in the root square: per axis q = floor((x - x0) *
 // 2^L / side), exact in FP64 because the side is a power of two.
+// Also zeroes zero[0, nzero) (the leaf pass's tile flags and counter; the
+// launch has at least nzero threads).
 template <int D>
 __global__ void k_keys(const float4 *__restrict__ pos, uint32_t n, const DevState *st,
-                       uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+                       uint64_t *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t *__restrict__ zero,
+                       uint32_t nzero) {
     if (st->converged) return;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nzero) zero[i] = 0;
     if (i >= n) return;
     keys[i] = morton_key<D>(pos[i], st->root0, st->root_w);
     vals[i] = i;
-}
-
-// Sorted node records and the "first of its key" flags.
-__global__ void k_gather(const float4 *__restrict__ pos, uint32_t n, const DevState *st,
-                         const uint64_t *__restrict__ keys, const uint32_t *__restrict__ perm,
-                         float4 *__restrict__ sp, uint32_t *__restrict__ sorig,
-                         uint32_t *__restrict__ flag) {
-    if (st->converged) return;
-    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    uint32_t i = perm[p];
-    sp[p] = pos[i];
-    sorig[p] = i;
-    flag[p] = (p == 0 || keys[p] != keys[p - 1]) ? 1u : 0u;
-}
-
-// Unique keys: leaf s starts at the first sorted point with its key; its cell
-// level mask starts empty.
-__global__ void k_leaves(uint32_t n, const DevState *st, const uint64_t *__restrict__ keys,
-                         const uint32_t *__restrict__ flag, const uint32_t *__restrict__ excl,
-                         uint32_t *__restrict__ leaf_start, uint64_t *__restrict__ ukey,
-                         uint32_t *__restrict__ uid, uint32_t *__restrict__ levels) {
-    if (st->converged) return;
-    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    uint32_t e = excl[p], f = flag[p];
-    uid[p] = e + f - 1;
-    if (f) {
-        leaf_start[e] = p;
-        ukey[e] = keys[p];
-        if (levels) levels[e] = 0;
-    }
-    if (p == n - 1) leaf_start[e + f] = n;
 }
 
 // Binary radix tree node arrays (Karras 2012, "Maximizing parallelism in the
@@ -553,67 +524,211 @@ __device__ __forceinline__ BodyDD thread_chunk(const float4 *__restrict__ sp, co
     return acc;
 }
 
-template <int D>
-__global__ void __launch_bounds__(AG_T) k_dd_reduce(const DevState *st, const float4 *__restrict__ sp,
-                                                    const uint32_t *__restrict__ leaf_start,
-                                                    BodyDD *__restrict__ bsum) {
-    if (st->converged) return;
-    __shared__ BodyDD s_w[2 * AG_W];
-    const uint32_t nu = st->n_unique;
-    const uint32_t base = blockIdx.x * AG_TILE;
-    if (base >= nu) return;
-    BodyDD total;
-    Body lb[AG_I];
-    uint32_t cb;
-    block_scan_bdd<D>(thread_chunk<D>(sp, leaf_start, base + threadIdx.x * AG_I, nu, lb, cb), BodyDD{}, total, s_w);
-    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+__device__ __forceinline__ DD dd_shfl_down(DD v, int o) {
+    return DD{__shfl_down_sync(GR_FULL, v.hi, o), __shfl_down_sync(GR_FULL, v.lo, o)};
 }
 
-// One block: exclusive prefix of the block sums in block order (in place); the
-// total is the prefix at nu.
+// Block total (AG_T threads) of one BodyDD per thread in a fixed shape (a
+// shuffle-down tree per warp, then over the warp totals); every thread gets it.
 template <int D>
-__global__ void __launch_bounds__(AG_T) k_dd_blocks(const DevState *st, BodyDD *__restrict__ bsum,
-                                                    BodyDD *__restrict__ prefix) {
-    if (st->converged) return;
-    __shared__ BodyDD s_w[2 * AG_W];
-    const uint32_t nu = st->n_unique;
-    const uint32_t nb = (nu + AG_TILE - 1) / AG_TILE;
-    BodyDD carry{};
-    for (uint32_t off = 0; off < nb; off += AG_T) {
-        const uint32_t b = off + threadIdx.x;
-        const BodyDD x = b < nb ? bsum[b] : BodyDD{};
-        BodyDD total;
-        const BodyDD ex = block_scan_bdd<D>(x, carry, total, s_w);
-        if (b < nb) bsum[b] = ex;
-        carry = total;
+__device__ __forceinline__ BodyDD block_total_bdd(BodyDD v, BodyDD *s_w) {
+    const int lane = threadIdx.x % GR_WARP, w = threadIdx.x / GR_WARP;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v = bdd_add<D>(v, BodyDD{dd_shfl_down(v.m, o), dd_shfl_down(v.c0, o), dd_shfl_down(v.c1, o),
+                                 D == 3 ? dd_shfl_down(v.c2, o) : DD{0.0, 0.0}});
+    if (lane == 0) s_w[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = lane < AG_W ? s_w[lane] : BodyDD{};
+#pragma unroll
+        for (int o = AG_W / 2; o > 0; o >>= 1)
+            v = bdd_add<D>(v, BodyDD{dd_shfl_down(v.m, o), dd_shfl_down(v.c0, o), dd_shfl_down(v.c1, o),
+                                     D == 3 ? dd_shfl_down(v.c2, o) : DD{0.0, 0.0}});
+        if (lane == 0) s_w[AG_W] = v;
     }
-    if (threadIdx.x == 0) prefix[nu] = carry;
+    __syncthreads();
+    const BodyDD r = s_w[AG_W];
+    __syncthreads();
+    return r;
 }
 
-// The exclusive prefix at every leaf, and every leaf's coincidence flag.
+// The stored prefix: D + 1 double-doubles per leaf (the mass, then the D mass
+// moments), 48 B in 2D and 64 B in 3D.
 template <int D>
-__global__ void __launch_bounds__(AG_T) k_dd_down(const DevState *st, const float4 *__restrict__ sp,
-                                                  const uint32_t *__restrict__ leaf_start,
-                                                  const BodyDD *__restrict__ bsum, BodyDD *__restrict__ prefix,
-                                                  uint8_t *__restrict__ leaf_coinc) {
+__device__ __forceinline__ void prefix_put(DD *__restrict__ pre, uint32_t s, const BodyDD &b) {
+    double2 *q = reinterpret_cast<double2 *>(pre + (size_t)s * (D + 1));
+    q[0] = make_double2(b.m.hi, b.m.lo);
+    q[1] = make_double2(b.c0.hi, b.c0.lo);
+    q[2] = make_double2(b.c1.hi, b.c1.lo);
+    if (D == 3) q[3] = make_double2(b.c2.hi, b.c2.lo);
+}
+
+template <int D>
+__device__ __forceinline__ BodyDD prefix_get(const DD *__restrict__ pre, uint32_t s) {
+    const double2 *q = reinterpret_cast<const double2 *>(pre + (size_t)s * (D + 1));
+    const double2 a = q[0], b = q[1], c = q[2];
+    const double2 d = D == 3 ? q[3] : make_double2(0.0, 0.0);
+    return BodyDD{{a.x, a.y}, {b.x, b.y}, {c.x, c.y}, {d.x, d.y}};
+}
+
+__device__ __forceinline__ void bdd_store(BodyDD *p, const BodyDD &b) {
+    double2 *q = reinterpret_cast<double2 *>(p);
+    q[0] = make_double2(b.m.hi, b.m.lo);
+    q[1] = make_double2(b.c0.hi, b.c0.lo);
+    q[2] = make_double2(b.c1.hi, b.c1.lo);
+    q[3] = make_double2(b.c2.hi, b.c2.lo);
+}
+
+__device__ __forceinline__ BodyDD bdd_load_cg(const BodyDD *p) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    const double2 a = __ldcg(q), b = __ldcg(q + 1), c = __ldcg(q + 2), d = __ldcg(q + 3);
+    return BodyDD{{a.x, a.y}, {b.x, b.y}, {c.x, c.y}, {d.x, d.y}};
+}
+
+constexpr uint32_t DD_SPIN_LIMIT = 1u << 22;  // x 32 ns sleeps: ~0.1 s
+
+// A point's exact FP64 terms: m and m * x per axis (a product of two FP32
+// values is exact in FP64).
+template <int D>
+__device__ __forceinline__ BodyDD point_terms(const float4 &p) {
+    const double m = (double)p.w;
+    return BodyDD{{m, 0.0}, {m * (double)p.x, 0.0}, {m * (double)p.y, 0.0}, {D == 3 ? m * (double)p.z : 0.0, 0.0}};
+}
+
+// Exclusive block scan (AG_T threads) of one count per thread; total = the
+// block's sum.
+__device__ __forceinline__ uint32_t block_excl_u32(uint32_t x, uint32_t &total, uint32_t *s_c) {
+    const int lane = threadIdx.x % GR_WARP, w = threadIdx.x / GR_WARP;
+    uint32_t inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(GR_FULL, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) s_c[w] = inc;
+    __syncthreads();
+    uint32_t before = 0;
+    total = 0;
+#pragma unroll
+    for (int k = 0; k < AG_W; k++) {
+        const uint32_t v = s_c[k];
+        before += k < w ? v : 0u;
+        total += v;
+    }
+    __syncthreads();
+    return before + inc - x;
+}
+
+// One pass over the sorted points (AG_TILE per tile, AG_I consecutive points
+// per thread; tile ids in start order from the counter at tile_flag[gridDim.x]):
+//  - the sorted point records sp[p] = pos[perm[p]], sorig[p] = perm[p];
+//  - "first of its key" flags and their exclusive count, the leaf index:
+//    uid[p], and at a leaf's first point leaf_start, ukey and an empty cell
+//    level mask; the last tile writes n_unique and leaf_start[n_unique] = n;
+//  - the exclusive double-double prefix of the point terms (point_terms) at
+//    each leaf's first point, and its total at n_unique.
+// Tile b publishes its totals (tile_sum[b], tile_cnt[b], then tile_flag[b] =
+// 1) and adds the totals of every tile before it in a fixed order: thread j
+// takes tiles j, j + AG_T, ... in turn, then block_total_bdd. So the prefix
+// does not depend on which tiles finished first and is the same every run.
+// The flags and the counter must be zero at launch. A wait that runs out sets
+// ERR_WAIT and goes on with what it read.
+template <int D>
+__global__ void __launch_bounds__(AG_T)
+k_sorted_leaves(DevState *st, uint32_t n, const float4 *__restrict__ pos, const uint64_t *__restrict__ keys,
+                const uint32_t *__restrict__ perm, float4 *__restrict__ sp, uint32_t *__restrict__ sorig,
+                uint32_t *__restrict__ uid, uint32_t *__restrict__ leaf_start, uint64_t *__restrict__ ukey,
+                uint32_t *__restrict__ levels, BodyDD *tile_sum, uint32_t *tile_cnt, uint32_t *tile_flag,
+                DD *__restrict__ prefix) {
     if (st->converged) return;
     __shared__ BodyDD s_w[2 * AG_W];
-    const uint32_t nu = st->n_unique;
-    const uint32_t base = blockIdx.x * AG_TILE;
-    if (base >= nu) return;
-    const uint32_t mine = base + threadIdx.x * AG_I;
-    BodyDD total;
-    Body lb[AG_I];
-    uint32_t cb;
-    BodyDD run = block_scan_bdd<D>(thread_chunk<D>(sp, leaf_start, mine, nu, lb, cb), bsum[blockIdx.x], total, s_w);
+    __shared__ uint32_t s_c[AG_W];
+    __shared__ uint32_t s_tile;
+    const uint32_t nt = (n + AG_TILE - 1) / AG_TILE;
+    if (threadIdx.x == 0) s_tile = atomicAdd(&tile_flag[gridDim.x], 1u);
+    __syncthreads();
+    const uint32_t b = s_tile;
+    if (b >= nt) return;
+    const uint32_t p0 = b * AG_TILE + threadIdx.x * AG_I;
+    uint64_t k[AG_I];
+    uint32_t q[AG_I];
+    float4 pt[AG_I];
 #pragma unroll
     for (int r = 0; r < AG_I; r++) {
-        const uint32_t s = mine + r;
-        if (s < nu) {
-            prefix[s] = run;
-            leaf_coinc[s] = (cb >> r) & 1u;
-            run = bdd_add<D>(run, bdd_of(lb[r]));
+        k[r] = p0 + r < n ? keys[p0 + r] : 0ull;
+        q[r] = p0 + r < n ? perm[p0 + r] : 0u;
+        if (q[r] >= n) {  // only after a sort pass gave up a wait (ERR_WAIT): keep the reads in bounds
+            atomicOr(&st->error, (uint32_t)ERR_TREE);
+            q[r] = 0;
         }
+    }
+    const uint64_t kprev = (p0 > 0 && p0 <= n) ? keys[p0 - 1] : 0ull;
+#pragma unroll
+    for (int r = 0; r < AG_I; r++) pt[r] = p0 + r < n ? pos[q[r]] : make_float4(0.f, 0.f, 0.f, 0.f);
+    uint32_t fl = 0;
+    BodyDD acc{};
+#pragma unroll
+    for (int r = 0; r < AG_I; r++) {
+        const uint32_t p = p0 + r;
+        if (p < n) {
+            const bool f = p == 0 || k[r] != (r == 0 ? kprev : k[r - 1]);
+            fl |= (f ? 1u : 0u) << r;
+            acc = bdd_add<D>(acc, point_terms<D>(pt[r]));
+            sp[p] = pt[r];
+            sorig[p] = q[r];
+        }
+    }
+    BodyDD total;
+    const BodyDD ex = block_scan_bdd<D>(acc, BodyDD{}, total, s_w);
+    uint32_t tcnt;
+    const uint32_t exc = block_excl_u32((uint32_t)__popc(fl), tcnt, s_c);
+    if (threadIdx.x == 0) {
+        bdd_store(&tile_sum[b], total);
+        tile_cnt[b] = tcnt;
+        __threadfence();
+        atomicExch(&tile_flag[b], 1u);
+    }
+    BodyDD fold{};
+    uint32_t cfold = 0;
+    volatile uint32_t *vf = tile_flag;
+    for (uint32_t j = threadIdx.x; j < b; j += AG_T) {
+        for (uint32_t spins = 0; vf[j] == 0u;) {
+            if (++spins > DD_SPIN_LIMIT) {
+                atomicOr(&st->error, (uint32_t)ERR_WAIT);
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+        fold = bdd_add<D>(fold, bdd_load_cg(&tile_sum[j]));
+        cfold += __ldcg(&tile_cnt[j]);
+    }
+    const BodyDD carry = block_total_bdd<D>(fold, s_w);
+    uint32_t ccarry;
+    block_excl_u32(cfold, ccarry, s_c);
+    BodyDD run = bdd_add<D>(carry, ex);
+    uint32_t e = ccarry + exc;  // leaves that start before this thread's first point
+#pragma unroll
+    for (int r = 0; r < AG_I; r++) {
+        const uint32_t p = p0 + r;
+        if (p < n) {
+            if (((fl >> r) & 1u) && e < n) {  // e < n unless a wait gave up
+                prefix_put<D>(prefix, e, run);
+                leaf_start[e] = p;
+                ukey[e] = k[r];
+                levels[e] = 0;
+                e++;
+            }
+            uid[p] = e - 1;
+            run = bdd_add<D>(run, point_terms<D>(pt[r]));
+        }
+    }
+    if (b == nt - 1 && threadIdx.x == 0) {
+        const uint32_t nu = min(ccarry + tcnt, n);
+        st->n_unique = nu;
+        leaf_start[nu] = n;
+        prefix_put<D>(prefix, nu, bdd_add<D>(carry, total));
     }
 }
 
@@ -625,12 +740,13 @@ __device__ __forceinline__ Body range_body(const BodyDD &a, const BodyDD &b) {
 
 // Every internal node's body as an array (the adjoint reads them; the tick's
 // own cell writer takes range_body of the cells only).
-__global__ void k_node_body(const DevState *st, BinTree t, const BodyDD *__restrict__ prefix,
+template <int D>
+__global__ void k_node_body(const DevState *st, BinTree t, const DD *__restrict__ prefix,
                             Body *__restrict__ int_body) {
     if (st->converged) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i + 1 >= st->n_unique) return;
-    body_store(&int_body[i], range_body(prefix[t.first[i]], prefix[t.last[i] + 1]));
+    body_store(&int_body[i], range_body(prefix_get<D>(prefix, t.first[i]), prefix_get<D>(prefix, t.last[i] + 1)));
 }
 
 template <int D>
@@ -747,8 +863,8 @@ __device__ __forceinline__ void assign_leaf(uint32_t s, uint32_t nu, uint32_t nc
 template <int D>
 __global__ void k_assign_cells(const DevState *st, BinTree t, uint32_t n_slots, const float4 *__restrict__ sp,
                                const uint32_t *__restrict__ P, const uint32_t *__restrict__ levels,
-                               const uint32_t *__restrict__ leaf_start, const BodyDD *__restrict__ prefix,
-                               const uint8_t *__restrict__ leaf_coinc, Cells cells, uint32_t *__restrict__ leaf_pre,
+                               const uint32_t *__restrict__ leaf_start, const DD *__restrict__ prefix,
+                               Cells cells, uint32_t *__restrict__ leaf_pre,
                                DevState *stw) {
     if (st->converged) return;
     constexpr int L = Levels<D>::L;
@@ -761,8 +877,6 @@ __global__ void k_assign_cells(const DevState *st, BinTree t, uint32_t n_slots, 
         if (s >= nu) return;
         const uint32_t idx = P[s] + __popc(levels[s]);
         const int32_t par = t.leaf_parent[s];
-        int level = 0;
-        if (par >= 0) level = leaf_coinc[s] ? t.rec[par].w / D + 1 : L;
         const uint32_t a0 = leaf_start[s], a1 = leaf_start[s + 1];
         if (idx >= ncells || a1 <= a0) {
             atomicOr(&stw->error, (uint32_t)ERR_TREE);
@@ -770,8 +884,10 @@ __global__ void k_assign_cells(const DevState *st, BinTree t, uint32_t n_slots, 
         }
         const float4 one = sp[a0];
         bool coinc;
-        write_cell<D>(cells, idx, leaf_sum<D>(sp, a0, a1, coinc), level, rw, -(int32_t)(a1 - a0), a0,
-                      a1 - a0 == 1 ? &one : nullptr);
+        const Body body = leaf_sum<D>(sp, a0, a1, coinc);
+        int level = 0;
+        if (par >= 0) level = coinc ? t.rec[par].w / D + 1 : L;
+        write_cell<D>(cells, idx, body, level, rw, -(int32_t)(a1 - a0), a0, a1 - a0 == 1 ? &one : nullptr);
         if (D == 2 && cells.bounds) write_bounds(cells, idx, one, level, st);
         leaf_pre[s] = idx;
         return;
@@ -789,7 +905,8 @@ __global__ void k_assign_cells(const DevState *st, BinTree t, uint32_t n_slots, 
         return;
     }
     const uint32_t a0 = leaf_start[f];
-    write_cell<D>(cells, idx, range_body(prefix[f], prefix[end]), lv, rw, (int32_t)skip, a0);
+    write_cell<D>(cells, idx, range_body(prefix_get<D>(prefix, f), prefix_get<D>(prefix, end)), lv, rw, (int32_t)skip,
+                  a0);
     if (D == 2 && cells.bounds) write_bounds(cells, idx, sp[a0], lv, st);
     if (t.cell_of) t.cell_of[i] = idx;
 }
