@@ -120,7 +120,7 @@ k_adj_update(uint32_t n, double jt, const DevState *st_after, const DevState *st
     if (threadIdx.x == 0) part[blockIdx.x] = acc;
     if (!last_block_done(&A->counters[0], &s_last)) return;
     double t = 0.0;
-    for (uint32_t k = threadIdx.x; k < gridDim.x; k += FRC_THREADS) t += __ldcg(&part[k]);
+    t += strided_sum_cg<FRC_THREADS>(part, gridDim.x, 1, 0);
     t = block_sum_d<FRC_THREADS>(t, s_red);
     if (threadIdx.x == 0) {
         const double Lsp = A->Lsp + t;
@@ -190,7 +190,7 @@ k_adj_node(uint32_t n, float gravity, int strong, const DevState *st, AdjScalars
     double S[3] = {0, 0, 0};
     for (int a = 0; a < D; a++) {
         double t = 0.0;
-        for (uint32_t k = threadIdx.x; k < gridDim.x; k += FRC_THREADS) t += __ldcg(&part[(size_t)k * 3 + a]);
+        t += strided_sum_cg<FRC_THREADS>(part, gridDim.x, 3, a);
         S[a] = block_sum_d<FRC_THREADS>(t, s_red);
     }
     if (threadIdx.x == 0)

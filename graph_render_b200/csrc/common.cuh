@@ -126,6 +126,26 @@ __device__ __forceinline__ double block_sum_d(double v, double *smem) {
     return r;
 }
 
+// Sum of v[k * stride + off] over this thread's k = threadIdx.x, threadIdx.x +
+// T, ... < count, added in k order; U loads are in flight at a time (the same
+// sum as one load per step, without a round trip per step).
+template <int T, int U = 8>
+__device__ __forceinline__ double strided_sum_cg(const double *v, uint32_t count, uint32_t stride, uint32_t off) {
+    double a = 0.0;
+    for (uint32_t k0 = threadIdx.x; k0 < count; k0 += T * U) {
+        double x[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint32_t k = k0 + u * T;
+            x[u] = k < count ? __ldcg(&v[(size_t)k * stride + off]) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (k0 + u * T < count) a += x[u];
+    }
+    return a;
+}
+
 // True in exactly one thread of the grid's last block to finish (threadfence
 // reduction pattern); the ticket resets itself for the next launch.
 __device__ __forceinline__ bool last_block_done(uint32_t *ticket, bool *smem_flag) {

@@ -149,8 +149,9 @@ struct gr_fa2 {
     BinTree bt{};
     Body *leaf_body = nullptr, *int_body = nullptr;
     DD *dd_prefix = nullptr;             // (n + 1) x (D + 1) double-doubles
-    BodyDD *dd_bsum = nullptr;           // the prefix pass's tile totals
-    uint32_t *dd_flag = nullptr;         // its tile flags and tile counter, then its tile leaf counts
+    Body *tile_sum = nullptr;            // per tile of AG_TILE sorted points: FP64 term sums
+    BodyDD *tile_carry = nullptr;        // and their exclusive double-double prefix
+    uint32_t *tile_cnt = nullptr;        // leaf counts per tile, then their exclusive prefix
     uint8_t *leaf_coinc = nullptr;
     Cells cells{};
     float *rep = nullptr, *U = nullptr;
@@ -163,10 +164,17 @@ struct gr_fa2 {
     cudaGraphExec_t exec = nullptr;
     uint32_t graph_kernels = 0;
     int walk_schedule = 1;  // 0: warp-cooperative union walk, 1: per-lane walk, 2: two nodes per lane
-    // the same tick as three graphs (tree, walk, forces+update) for per-phase timing
-    cudaGraph_t pgraph[3] = {nullptr, nullptr, nullptr};
-    cudaGraphExec_t pexec[3] = {nullptr, nullptr, nullptr};
+    // the same tick with event records at its phase boundaries (tick start,
+    // tree built, walk done, tick end), for per-phase timing
+    cudaGraph_t tgraph = nullptr;
+    cudaGraphExec_t texec = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool timing_events = false;  // set while the timed graph is captured
+    // the attraction branch of a captured tick: it forks after the tree build and
+    // joins before the forces, beside the walk
+    cudaStream_t aux = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    bool branch = false;  // set while a whole tick is captured
     void *flush = nullptr;
     size_t flush_bytes = 0;
 
@@ -186,18 +194,19 @@ struct gr_fa2 {
         if (graph) cudaGraphDestroy(graph);
         exec = nullptr;
         graph = nullptr;
-        for (int i = 0; i < 3; i++) {
-            if (pexec[i]) cudaGraphExecDestroy(pexec[i]);
-            if (pgraph[i]) cudaGraphDestroy(pgraph[i]);
-            pexec[i] = nullptr;
-            pgraph[i] = nullptr;
-        }
+        if (texec) cudaGraphExecDestroy(texec);
+        if (tgraph) cudaGraphDestroy(tgraph);
+        texec = nullptr;
+        tgraph = nullptr;
     }
     ~gr_fa2() {
         if (adj) adjoint_release(adj);
         drop_graphs();
         for (int i = 0; i < 4; i++)
             if (ev[i]) cudaEventDestroy(ev[i]);
+        if (fork_ev) cudaEventDestroy(fork_ev);
+        if (join_ev) cudaEventDestroy(join_ev);
+        if (aux) cudaStreamDestroy(aux);
         if (flush) cudaFree(flush);
         for (void *p : allocs) cudaFreeAsync(p, stream);
         sorter.release();
@@ -240,8 +249,9 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
     A(h->int_body, n);
     A(h->leaf_coinc, n);
     A(h->dd_prefix, 4 * ((size_t)n + 1));
-    A(h->dd_bsum, div_up(n, AG_TILE) + 1);
-    A(h->dd_flag, 2 * ((size_t)div_up(n, AG_TILE) + 1));
+    A(h->tile_sum, div_up(n, AG_TILE) + 1);
+    A(h->tile_carry, div_up(n, AG_TILE) + 1);
+    A(h->tile_cnt, 2 * ((size_t)div_up(n, AG_TILE) + 1));
     A(h->cells.A, 2 * (size_t)n);
     A(h->cells.B, 2 * (size_t)n);
     if (D == 3) A(h->cells.C, 2 * (size_t)n);
@@ -297,17 +307,39 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
     const uint32_t gn = div_up(n, 256);
     DevState *st = h->st;
     const uint32_t *conv = &st->converged;
+    const int lin_log = (int)h->prm[P_LINLOG];
+    // the attraction of every node into U (k_forces reads it there): the heavy
+    // rows' segment sums, then every row
+    auto attraction_seg = [&](cudaStream_t q) {
+        if (h->nseg)
+            k_attract_seg<D><<<div_up((uint64_t)h->nseg * GR_WARP, FRC_THREADS), FRC_THREADS, 0, q>>>(
+                h->nseg, lin_log, st, h->pos, h->rp, h->col, h->wt, h->seg_row, h->seg_first, h->seg_out);
+    };
+    auto attraction_rows = [&](cudaStream_t q) {
+        k_attract<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, q>>>(n, lin_log, st, h->pos, h->rp, h->col, h->wt,
+                                                                     h->nseg ? h->seg_first : nullptr, h->seg_out,
+                                                                     h->U);
+    };
+    // In a captured whole tick the attraction runs on its own branch beside the
+    // walk (which is bound by instruction issue, the attraction by memory
+    // latency); beside the tree build it slowed the latency-bound tree kernels
+    // by about as much as it saved.
+    const bool branch = h->branch && phases == PH_ALL;
+    if (h->timing_events) cudaEventRecordWithFlags(h->ev[0], s, cudaEventRecordExternal);
     if (phases & PH_TREE) {
         k_bounds<D><<<h->bnd_blocks(), BND_THREADS, 0, s>>>(h->pos, n, st, h->part);
         const uint32_t ab = div_up(n, AG_TILE);
-        k_keys<D><<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals, h->dd_flag, ab + 1);
+        k_keys<D><<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals);
         if (h->long_runs)
             sort_fast(h, s);
         else
             h->sorter.sort(h->keys, h->vals, n, 64, s, conv);
-        k_sorted_leaves<D><<<ab, AG_T, 0, s>>>(st, n, h->pos, h->keys, h->vals, h->sp, h->sorig, h->uid,
-                                                h->leaf_start, h->ukey, h->levels, h->dd_bsum, h->dd_flag + ab + 1,
-                                                h->dd_flag, h->dd_prefix);
+        k_leaf_tiles<D><<<ab, AG_T, 0, s>>>(st, n, h->pos, h->keys, h->vals, h->sp, h->sorig, h->tile_sum,
+                                             h->tile_cnt);
+        k_leaf_carry<D><<<1, CARRY_T, 0, s>>>(st, n, h->tile_sum, h->tile_cnt, h->tile_carry, h->tile_cnt + ab,
+                                              h->leaf_start, h->dd_prefix);
+        k_leaf_prefix<D><<<ab, AG_T, 0, s>>>(st, n, h->sp, h->keys, h->tile_carry, h->tile_cnt + ab, h->uid,
+                                              h->leaf_start, h->ukey, h->levels, h->dd_prefix);
         const bool adjoint = h->bt.cell_of != nullptr;  // the adjoint reads leaf and node bodies as arrays
         BinTree bt = h->bt;  // the tick itself reads only the packed records and leaf_parent
         bt.levels = h->levels;
@@ -321,6 +353,14 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
         h->scanner.scan_levels(h->levels, h->P, n, &st->n_unique, &st->n_cells, s, conv);
         k_assign_cells<D><<<2 * gn, 256, 0, s>>>(st, bt, gn * 256, h->sp, h->P, h->levels, h->leaf_start,
                                                  h->dd_prefix, h->cells, h->leaf_pre, st);
+    }
+    if (h->timing_events) cudaEventRecordWithFlags(h->ev[1], s, cudaEventRecordExternal);
+    if (branch) {
+        cudaEventRecord(h->fork_ev, s);
+        cudaStreamWaitEvent(h->aux, h->fork_ev, 0);
+        attraction_seg(h->aux);
+        attraction_rows(h->aux);
+        cudaEventRecord(h->join_ev, h->aux);
     }
     if (phases & PH_WALK) {
         WalkParams wp;
@@ -338,23 +378,27 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
             k_walk_s<D, 0><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig, h->uid,
                                                                            h->leaf_pre, h->rep, st);
     }
+    if (h->timing_events) cudaEventRecordWithFlags(h->ev[2], s, cudaEventRecordExternal);
     if (phases & PH_FINISH) {
         ForceParams fp;
         fp.n = n;
         fp.gravity = (float)h->prm[P_GRAVITY];
-        fp.lin_log = (int)h->prm[P_LINLOG];
+        fp.lin_log = lin_log;
         fp.strong_gravity = (int)h->prm[P_STRONG];
         fp.dissuade_hubs = (int)h->prm[P_DISSUADE];
         fp.jitter_tolerance = h->prm[P_JT];
-        if (h->nseg)
-            k_attract_seg<D><<<div_up((uint64_t)h->nseg * GR_WARP, FRC_THREADS), FRC_THREADS, 0, s>>>(
-                h->nseg, fp.lin_log, st, h->pos, h->rp, h->col, h->wt, h->seg_row, h->seg_first, h->seg_out);
-        k_forces<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(fp, st, h->pos, h->rp, h->col, h->wt,
-                                                                    h->seg_first, h->seg_out, h->rep, h->U,
-                                                                    h->part, forces_only ? 0 : 1);
+        if (branch) {
+            cudaStreamWaitEvent(s, h->join_ev, 0);
+        } else {
+            attraction_seg(s);
+            attraction_rows(s);
+        }
+        k_forces<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(fp, st, h->pos, h->rep, h->U, h->part,
+                                                                    forces_only ? 0 : 1);
         if (!forces_only)
             k_update<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(n, st, h->pos, h->U, h->part);
     }
+    if (h->timing_events) cudaEventRecordWithFlags(h->ev[3], s, cudaEventRecordExternal);
 }
 
 static void enqueue(gr_fa2 *h, bool forces_only, int phases = PH_ALL) {
@@ -364,18 +408,56 @@ static void enqueue(gr_fa2 *h, bool forces_only, int phases = PH_ALL) {
         enqueue_tick<2>(h, forces_only, phases);
 }
 
-static int capture(gr_fa2 *h, int phases, cudaGraph_t *g, cudaGraphExec_t *x) {
+// Captures one whole tick (with the attraction on its own branch), and with
+// timing the event records at its phase boundaries.
+static int capture(gr_fa2 *h, bool timing, cudaGraph_t *g, cudaGraphExec_t *x) {
+    if (!h->aux) {
+        CU(cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking));
+        CU(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
+        CU(cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming));
+    }
+    if (timing)
+        for (int i = 0; i < 4; i++)
+            if (!h->ev[i]) CU(cudaEventCreate(&h->ev[i]));
     CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue(h, false, phases);
+    h->branch = true;
+    h->timing_events = timing;
+    enqueue(h, false, PH_ALL);
+    h->branch = false;
+    h->timing_events = false;
     cudaError_t e = cudaStreamEndCapture(h->stream, g);
     if (e != cudaSuccess) return set_err(GR_CUDA_ERROR, cudaGetErrorString(e));
+    // The attraction branch fills what the tree build leaves idle: its kernels
+    // run at the lowest priority, the tick's own path at the highest, so a free
+    // SM slot goes to the tree's next block first.
+    int least = 0, greatest = 0;
+    CU(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    size_t nn = 0;
+    CU(cudaGraphGetNodes(*g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    CU(cudaGraphGetNodes(*g, nodes.data(), &nn));
+    const void *side[4] = {(const void *)k_attract<2>, (const void *)k_attract<3>, (const void *)k_attract_seg<2>,
+                           (const void *)k_attract_seg<3>};
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        CU(cudaGraphNodeGetType(nd, &t));
+        if (t != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp;
+        CU(cudaGraphKernelNodeGetParams(nd, &kp));
+        bool low = false;
+        for (const void *f : side) low = low || kp.func == f;
+        cudaLaunchAttributeValue v;
+        memset(&v, 0, sizeof v);
+        v.priority = low ? least : greatest;
+        CU(cudaGraphKernelNodeSetAttribute(nd, cudaLaunchAttributePriority, &v));
+    }
     CU(cudaGraphInstantiate(x, *g, 0));
     return GR_OK;
 }
 
 static int build_graph(gr_fa2 *h) {
     if (h->exec) return GR_OK;
-    if (int c = capture(h, PH_ALL, &h->graph, &h->exec)) return c;
+    if (int c = capture(h, false, &h->graph, &h->exec)) return c;
     size_t nn = 0;
     CU(cudaGraphGetNodes(h->graph, nullptr, &nn));
     std::vector<cudaGraphNode_t> nodes(nn);
@@ -389,12 +471,9 @@ static int build_graph(gr_fa2 *h) {
     return GR_OK;
 }
 
-static int build_phase_graphs(gr_fa2 *h) {
-    if (h->pexec[0]) return GR_OK;
-    const int ph[3] = {PH_TREE, PH_WALK, PH_FINISH};
-    for (int i = 0; i < 3; i++)
-        if (int c = capture(h, ph[i], &h->pgraph[i], &h->pexec[i])) return c;
-    return GR_OK;
+static int build_timed_graph(gr_fa2 *h) {
+    if (h->texec) return GR_OK;
+    return capture(h, true, &h->tgraph, &h->texec);
 }
 
 static int read_state(gr_fa2 *h, DevState *out) {
@@ -713,10 +792,7 @@ int gr_fa2_tick_timed(gr_fa2 *h, uint32_t ticks, size_t l2_flush_bytes, float *m
     DevState s0;
     if (int c = read_state(h, &s0)) return c;
     if (h->n && ticks) {
-        if (int c = build_phase_graphs(h)) return c;
-        if (int c = build_graph(h)) return c;
-        for (int i = 0; i < 4; i++)
-            if (!h->ev[i]) CU(cudaEventCreate(&h->ev[i]));
+        if (int c = build_timed_graph(h)) return c;
         if (l2_flush_bytes && l2_flush_bytes != h->flush_bytes) {
             if (h->flush) cudaFree(h->flush);
             h->flush = nullptr;
@@ -725,14 +801,8 @@ int gr_fa2_tick_timed(gr_fa2 *h, uint32_t ticks, size_t l2_flush_bytes, float *m
         }
         for (uint32_t t = 0; t < ticks; t++) {
             if (l2_flush_bytes) CU(cudaMemsetAsync(h->flush, (int)(t & 0xff), l2_flush_bytes, h->stream));
-            CU(cudaEventRecord(h->ev[0], h->stream));
-            CU(cudaGraphLaunch(h->pexec[0], h->stream));
-            CU(cudaEventRecord(h->ev[1], h->stream));
-            CU(cudaGraphLaunch(h->pexec[1], h->stream));
-            CU(cudaEventRecord(h->ev[2], h->stream));
-            CU(cudaGraphLaunch(h->pexec[2], h->stream));
-            CU(cudaEventRecord(h->ev[3], h->stream));
-            CU(cudaEventSynchronize(h->ev[3]));
+            CU(cudaGraphLaunch(h->texec, h->stream));
+            CU(cudaStreamSynchronize(h->stream));
             float a = 0.f, b = 0.f, c = 0.f, d = 0.f;
             CU(cudaEventElapsedTime(&a, h->ev[0], h->ev[1]));
             CU(cudaEventElapsedTime(&b, h->ev[1], h->ev[2]));
@@ -1069,8 +1139,9 @@ static int forces_static(uint32_t n, const float4 *nodes, const uint32_t *rp, co
     h.int_body = cv.take<Body>(n);
     h.leaf_coinc = cv.take<uint8_t>(n);
     h.dd_prefix = cv.take<DD>(4 * ((size_t)n + 1));
-    h.dd_bsum = cv.take<BodyDD>(div_up(n, AG_TILE) + 1);
-    h.dd_flag = cv.take<uint32_t>(2 * ((size_t)div_up(n, AG_TILE) + 1));
+    h.tile_sum = cv.take<Body>(div_up(n, AG_TILE) + 1);
+    h.tile_carry = cv.take<BodyDD>(div_up(n, AG_TILE) + 1);
+    h.tile_cnt = cv.take<uint32_t>(2 * ((size_t)div_up(n, AG_TILE) + 1));
     h.cells.A = cv.take<float4>(2 * (size_t)n);
     h.cells.B = cv.take<float4>(2 * (size_t)n);
     h.cells.C = D == 3 ? cv.take<int2>(2 * (size_t)n) : nullptr;
@@ -1555,8 +1626,9 @@ static void adjoint_tick(gr_fa2 *h, Adjoint *a, const DevState *before) {
     if (h->nseg)
         k_attract_seg<D><<<div_up((uint64_t)h->nseg * GR_WARP, FRC_THREADS), FRC_THREADS, 0, s>>>(
             h->nseg, fp.lin_log, st, h->pos, h->rp, h->col, h->wt, h->seg_row, h->seg_first, h->seg_out);
-    k_forces<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(fp, st, h->pos, h->rp, h->col, h->wt, h->seg_first,
-                                                                h->seg_out, h->rep, h->U, h->part, 1);
+    k_attract<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(n, fp.lin_log, st, h->pos, h->rp, h->col, h->wt,
+                                                                 h->nseg ? h->seg_first : nullptr, h->seg_out, h->U);
+    k_forces<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(fp, st, h->pos, h->rep, h->U, h->part, 1);
     const uint32_t gb = div_up(n, FRC_THREADS);
     k_adj_update<D><<<gb, FRC_THREADS, 0, s>>>(n, h->prm[P_JT], st, before, a->A, h->pos, h->U, a->lam1, a->lam, a->ub,
                                                 a->part);

@@ -107,8 +107,8 @@ __device__ __forceinline__ void estimate_factor(DevState *st, double n, double j
 // and returns the node's FP64 swing and traction terms (schedule.rs:16-30).
 template <int D>
 __device__ __forceinline__ void node_force(const ForceParams &P, const float4 &p, float a0, float a1, float a2,
-                                           float r0, float r1, float r2, const double *mean, float *__restrict__ u,
-                                           double &sw, double &tr) {
+                                           float r0, float r1, float r2, const double *mean, float *u, double &sw,
+                                           double &tr) {
     if (P.dissuade_hubs) {
         a0 /= p.w;
         a1 /= p.w;
@@ -180,14 +180,30 @@ __device__ __forceinline__ void node_attraction(uint32_t i, const float4 &p, int
     }
 }
 
-// u_i for every node; per-block FP64 swing and traction; the last block
-// accumulates them into the state (cumulative, state.rs:141-143) and runs
-// estimate_factor.
+// Every node's attraction (node_attraction) into att (n x D). It reads only the
+// positions and the graph, so it can run beside the tree build and the walk.
 template <int D>
 __global__ void __launch_bounds__(FRC_THREADS)
-k_forces(ForceParams P, DevState *st, const float4 *__restrict__ pos, const uint32_t *__restrict__ rp,
-         const uint32_t *__restrict__ col, const float *__restrict__ wt, const uint32_t *__restrict__ seg_first,
-         const float *__restrict__ seg_out, const float *__restrict__ rep, float *__restrict__ U,
+k_attract(uint32_t n, int lin_log, const DevState *st, const float4 *__restrict__ pos,
+          const uint32_t *__restrict__ rp, const uint32_t *__restrict__ col, const float *__restrict__ wt,
+          const uint32_t *__restrict__ seg_first, const float *__restrict__ seg_out, float *__restrict__ att) {
+    if (st->converged) return;
+    const uint32_t i = blockIdx.x * FRC_THREADS + threadIdx.x;
+    if (i >= n) return;
+    float a0, a1, a2;
+    node_attraction<D>(i, pos[i], lin_log, pos, rp, col, wt, seg_first, seg_out, a0, a1, a2);
+    att[(size_t)i * D] = a0;
+    att[(size_t)i * D + 1] = a1;
+    if (D == 3) att[(size_t)i * D + 2] = a2;
+}
+
+// u_i for every node from its attraction (read from U, where k_attract put it;
+// each thread reads and then overwrites only its own node's entries) and its
+// repulsion; per-block FP64 swing and traction; the last block accumulates
+// them into the state (cumulative, state.rs:141-143) and runs estimate_factor.
+template <int D>
+__global__ void __launch_bounds__(FRC_THREADS)
+k_forces(ForceParams P, DevState *st, const float4 *__restrict__ pos, const float *__restrict__ rep, float *U,
          double *__restrict__ part, int speed_update) {
     if (st->converged) return;
     __shared__ double s_red[32];
@@ -196,10 +212,10 @@ k_forces(ForceParams P, DevState *st, const float4 *__restrict__ pos, const uint
     double sw = 0.0, tr = 0.0;
     if (i < P.n) {
         const float4 p = pos[i];
-        float a0, a1, a2;
-        node_attraction<D>(i, p, P.lin_log, pos, rp, col, wt, seg_first, seg_out, a0, a1, a2);
+        float *u = U + (size_t)i * D;
+        const float a0 = u[0], a1 = u[1], a2 = D == 3 ? u[2] : 0.f;
         node_force<D>(P, p, a0, a1, a2, rep[(size_t)i * D + 0], rep[(size_t)i * D + 1],
-                      D == 3 ? rep[(size_t)i * D + 2] : 0.f, st->mean, U + (size_t)i * D, sw, tr);
+                      D == 3 ? rep[(size_t)i * D + 2] : 0.f, st->mean, u, sw, tr);
     }
     if (!speed_update) return;
     sw = block_sum_d<FRC_THREADS>(sw, s_red);
@@ -209,11 +225,8 @@ k_forces(ForceParams P, DevState *st, const float4 *__restrict__ pos, const uint
         part[2 * blockIdx.x + 1] = tr;
     }
     if (!last_block_done(&st->counters[1], &s_last)) return;
-    double a = 0.0, b = 0.0;
-    for (uint32_t k = threadIdx.x; k < gridDim.x; k += FRC_THREADS) {
-        a += __ldcg(&part[2 * k]);
-        b += __ldcg(&part[2 * k + 1]);
-    }
+    double a = strided_sum_cg<FRC_THREADS>(part, gridDim.x, 2, 0);
+    double b = strided_sum_cg<FRC_THREADS>(part, gridDim.x, 2, 1);
     a = block_sum_d<FRC_THREADS>(a, s_red);
     b = block_sum_d<FRC_THREADS>(b, s_red);
     if (threadIdx.x == 0) {
@@ -244,8 +257,7 @@ k_update(uint32_t n, DevState *st, float4 *__restrict__ pos, const float *__rest
     step = block_sum_d<FRC_THREADS>(step, s_red);
     if (threadIdx.x == 0) part[blockIdx.x] = step;
     if (!last_block_done(&st->counters[2], &s_last)) return;
-    double a = 0.0;
-    for (uint32_t k = threadIdx.x; k < gridDim.x; k += FRC_THREADS) a += __ldcg(&part[k]);
+    double a = strided_sum_cg<FRC_THREADS>(part, gridDim.x, 1, 0);
     a = block_sum_d<FRC_THREADS>(a, s_red);
     if (threadIdx.x == 0) {
         st->moved = a;

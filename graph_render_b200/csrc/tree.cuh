@@ -113,15 +113,27 @@ k_bounds(const float4 *__restrict__ pos, uint32_t n, DevState *st, double *__res
         sum[a] = 0.0;
     }
     bool bad = false;
-    for (uint32_t i = blockIdx.x * BND_THREADS + threadIdx.x; i < n; i += gridDim.x * BND_THREADS) {
-        float4 p = pos[i];
-        float c[3] = {p.x, p.y, p.z};
+    // this thread's points i0, i0 + stride, ... in order, BND_U loads in flight
+    constexpr int BND_U = 4;
+    const uint64_t stride = (uint64_t)gridDim.x * BND_THREADS;
+    for (uint64_t i0 = blockIdx.x * BND_THREADS + threadIdx.x; i0 < n; i0 += stride * BND_U) {
+        float4 pv[BND_U];
 #pragma unroll
-        for (int a = 0; a < D; a++) {
-            if (!isfinite(c[a])) bad = true;
-            lo[a] = fminf(lo[a], c[a]);
-            hi[a] = fmaxf(hi[a], c[a]);
-            sum[a] += (double)c[a];
+        for (int u = 0; u < BND_U; u++) {
+            const uint64_t i = i0 + u * stride;
+            pv[u] = i < n ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < BND_U; u++) {
+            if (i0 + u * stride >= n) break;
+            const float c[3] = {pv[u].x, pv[u].y, pv[u].z};
+#pragma unroll
+            for (int a = 0; a < D; a++) {
+                if (!isfinite(c[a])) bad = true;
+                lo[a] = fminf(lo[a], c[a]);
+                hi[a] = fmaxf(hi[a], c[a]);
+                sum[a] += (double)c[a];
+            }
         }
     }
     if (__syncthreads_or(bad)) {
@@ -175,11 +187,20 @@ k_bounds(const float4 *__restrict__ pos, uint32_t n, DevState *st, double *__res
             gs[a] += __ldcg(q + 2 * D + a);
         }
     }
-    __shared__ double s_l[D][BND_THREADS], s_h[D][BND_THREADS];
+    // min / max are exact in any order: warp shuffles, then the warp results
+    __shared__ double s_l[D][BND_THREADS / GR_WARP], s_h[D][BND_THREADS / GR_WARP];
 #pragma unroll
     for (int a = 0; a < D; a++) {
-        s_l[a][threadIdx.x] = gl[a];
-        s_h[a][threadIdx.x] = gh[a];
+        double l = gl[a], h = gh[a];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            l = fmin(l, __shfl_xor_sync(GR_FULL, l, o));
+            h = fmax(h, __shfl_xor_sync(GR_FULL, h, o));
+        }
+        if (lane == 0) {
+            s_l[a][w] = l;
+            s_h[a][w] = h;
+        }
     }
     double S[D];
 #pragma unroll
@@ -189,7 +210,7 @@ k_bounds(const float4 *__restrict__ pos, uint32_t n, DevState *st, double *__res
         for (int a = 0; a < D; a++) {
             mn[a] = INFINITY;
             mx[a] = -INFINITY;
-            for (int k = 0; k < BND_THREADS; k++) {
+            for (int k = 0; k < BND_THREADS / GR_WARP; k++) {
                 mn[a] = fmin(mn[a], s_l[a][k]);
                 mx[a] = fmax(mx[a], s_h[a][k]);
             }
@@ -205,15 +226,11 @@ k_bounds(const float4 *__restrict__ pos, uint32_t n, DevState *st, double *__res
 
 // Morton key of every node in the root square: per axis q = floor((x - x0) *
 // 2^L / side), exact in FP64 because the side is a power of two.
-// Also zeroes zero[0, nzero) (the leaf pass's tile flags and counter; the
-// launch has at least nzero threads).
 template <int D>
 __global__ void k_keys(const float4 *__restrict__ pos, uint32_t n, const DevState *st,
-                       uint64_t *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t *__restrict__ zero,
-                       uint32_t nzero) {
+                       uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
     if (st->converged) return;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nzero) zero[i] = 0;
     if (i >= n) return;
     keys[i] = morton_key<D>(pos[i], st->root0, st->root_w);
     vals[i] = i;
@@ -393,11 +410,14 @@ __global__ void k_aggregate(DevState *st, const float4 *__restrict__ sp,
     aggregate_leaf<D>(s, sp, leaf_start, t, leaf_body, int_body, leaf_coinc, &st->error);
 }
 
-// ---- bodies without atomics: leaf sums, a double-double prefix over the
-// leaves in key order, and every internal node's body as the difference of the
-// prefixes at its range ends. The prefix is exact to ~1e-32 of its magnitude,
-// so a node's sums are as exact as a direct FP64 sum; the scan's decomposition
-// is fixed, so the result is the same every run.
+// ---- bodies without atomics: a prefix of the point terms (m, m x per axis;
+// each an exact FP64 product of two FP32 values) over the sorted points, read
+// at every leaf's first point, and every internal node's body as the
+// difference of the prefixes at its range ends. Inside a tile of AG_TILE
+// points the prefix is an FP64 scan (error ~1e-16 of the tile's sums); across
+// tiles it is a double-double carry (exact to ~1e-32 of the whole sum), so a
+// node's sums are as exact as a direct FP64 sum over its points. Every
+// decomposition is fixed, so the result is the same every run.
 
 struct DD {
     double hi, lo;
@@ -466,91 +486,100 @@ __device__ __forceinline__ DD dd_shfl_up(DD v, int o) {
     return DD{__shfl_up_sync(GR_FULL, v.hi, o), __shfl_up_sync(GR_FULL, v.lo, o)};
 }
 
-// Inclusive warp scan of BodyDD, a fixed Hillis-Steele shape.
 template <int D>
-__device__ __forceinline__ BodyDD warp_scan_bdd(BodyDD v) {
-    const int lane = threadIdx.x % GR_WARP;
+__device__ __forceinline__ BodyDD bdd_shfl_up(const BodyDD &v, int o) {
+    return BodyDD{dd_shfl_up(v.m, o), dd_shfl_up(v.c0, o), dd_shfl_up(v.c1, o),
+                  D == 3 ? dd_shfl_up(v.c2, o) : DD{0.0, 0.0}};
+}
+
+// a + b for a double-double a and a double b (two-sum, renormalised).
+__device__ __forceinline__ DD dd_add_d(DD a, double b) {
+    const double s = a.hi + b;
+    const double bb = s - a.hi;
+    double e = (a.hi - (s - bb)) + (b - bb);
+    e += a.lo;
+    const double hi = s + e;
+    return DD{hi, e - (hi - s)};
+}
+
+template <int D>
+__device__ __forceinline__ BodyDD bdd_add_body(const BodyDD &a, const Body &b) {
+    return BodyDD{dd_add_d(a.m, b.m), dd_add_d(a.c0, b.c0), dd_add_d(a.c1, b.c1),
+                  D == 3 ? dd_add_d(a.c2, b.c2) : DD{0.0, 0.0}};
+}
+
+// A point's exact FP64 terms: m and m * x per axis (a product of two FP32
+// values is exact in FP64).
+template <int D>
+__device__ __forceinline__ Body point_body(const float4 &p) {
+    const double m = (double)p.w;
+    return Body{m, m * (double)p.x, m * (double)p.y, D == 3 ? m * (double)p.z : 0.0};
+}
+
+template <int D>
+__device__ __forceinline__ Body body_sum(const Body &a, const Body &b) {
+    return Body{a.m + b.m, a.c0 + b.c0, a.c1 + b.c1, D == 3 ? a.c2 + b.c2 : 0.0};
+}
+
+__device__ __forceinline__ double shfl_up_d(double v, int o) { return __shfl_up_sync(GR_FULL, v, o); }
+
+// Exclusive block scan (AG_T threads) of one (FP64 Body, count) per thread in
+// a fixed shape: Hillis-Steele warp scans, then a scan of the warp totals.
+// Gives this thread's exclusive prefixes and the block totals (the same values
+// for the same inputs, whichever kernel asks). s_w and s_c hold 2 AG_W entries.
+template <int D>
+__device__ __forceinline__ void block_scan_body(const Body &x, uint32_t c, Body &ex, uint32_t &exc, Body &total,
+                                                uint32_t &tcnt, Body *s_w, uint32_t *s_c) {
+    const int lane = threadIdx.x % GR_WARP, w = threadIdx.x / GR_WARP;
+    Body inc = x;
+    uint32_t ci = c;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const BodyDD u{dd_shfl_up(v.m, o), dd_shfl_up(v.c0, o), dd_shfl_up(v.c1, o),
-                       D == 3 ? dd_shfl_up(v.c2, o) : DD{0.0, 0.0}};
-        if (lane >= o) v = bdd_add<D>(u, v);
-    }
-    return v;
-}
-
-// Exclusive block scan (AG_T threads) of one BodyDD per thread, offset by
-// `carry`; returns this thread's exclusive prefix and the block total.
-template <int D>
-__device__ __forceinline__ BodyDD block_scan_bdd(const BodyDD &x, const BodyDD &carry, BodyDD &total,
-                                                 BodyDD *s_w) {
-    const int lane = threadIdx.x % GR_WARP, w = threadIdx.x / GR_WARP;
-    const BodyDD inc = warp_scan_bdd<D>(x);
-    if (lane == 31) s_w[w] = inc;
-    __syncthreads();
-    if (w == 0) {  // scan the warp totals (one per lane < AG_W)
-        BodyDD t = lane < AG_W ? s_w[lane] : BodyDD{};
-        t = warp_scan_bdd<D>(t);
-        if (lane < AG_W) s_w[AG_W + lane] = t;
-    }
-    __syncthreads();
-    const BodyDD before = w > 0 ? s_w[AG_W + w - 1] : BodyDD{};
-    total = bdd_add<D>(carry, s_w[AG_W + AG_W - 1]);
-    // exclusive prefix: carry + warps before + lanes before (inc - x recomputed as a shifted scan)
-    BodyDD lanes_before{dd_shfl_up(inc.m, 1), dd_shfl_up(inc.c0, 1), dd_shfl_up(inc.c1, 1),
-                        D == 3 ? dd_shfl_up(inc.c2, 1) : DD{0.0, 0.0}};
-    if (lane == 0) lanes_before = BodyDD{};
-    __syncthreads();
-    return bdd_add<D>(bdd_add<D>(carry, before), lanes_before);
-}
-
-// This thread's AG_I leaf bodies (leaf_sum over the sorted points) and their
-// sequential double-double sum.
-template <int D>
-__device__ __forceinline__ BodyDD thread_chunk(const float4 *__restrict__ sp, const uint32_t *__restrict__ leaf_start,
-                                               uint32_t base, uint32_t nu, Body *lb, uint32_t &coinc_bits) {
-    BodyDD acc{};
-    coinc_bits = 0;
-#pragma unroll
-    for (int r = 0; r < AG_I; r++) {
-        const uint32_t s = base + r;
-        if (s < nu) {
-            bool c;
-            lb[r] = leaf_sum<D>(sp, leaf_start[s], leaf_start[s + 1], c);
-            coinc_bits |= (c ? 1u : 0u) << r;
-            acc = bdd_add<D>(acc, bdd_of(lb[r]));
+        const Body u{shfl_up_d(inc.m, o), shfl_up_d(inc.c0, o), shfl_up_d(inc.c1, o),
+                     D == 3 ? shfl_up_d(inc.c2, o) : 0.0};
+        const uint32_t cu = __shfl_up_sync(GR_FULL, ci, o);
+        if (lane >= o) {
+            inc = body_sum<D>(u, inc);
+            ci += cu;
         }
     }
-    return acc;
-}
-
-__device__ __forceinline__ DD dd_shfl_down(DD v, int o) {
-    return DD{__shfl_down_sync(GR_FULL, v.hi, o), __shfl_down_sync(GR_FULL, v.lo, o)};
-}
-
-// Block total (AG_T threads) of one BodyDD per thread in a fixed shape (a
-// shuffle-down tree per warp, then over the warp totals); every thread gets it.
-template <int D>
-__device__ __forceinline__ BodyDD block_total_bdd(BodyDD v, BodyDD *s_w) {
-    const int lane = threadIdx.x % GR_WARP, w = threadIdx.x / GR_WARP;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-        v = bdd_add<D>(v, BodyDD{dd_shfl_down(v.m, o), dd_shfl_down(v.c0, o), dd_shfl_down(v.c1, o),
-                                 D == 3 ? dd_shfl_down(v.c2, o) : DD{0.0, 0.0}});
-    if (lane == 0) s_w[w] = v;
-    __syncthreads();
-    if (w == 0) {
-        v = lane < AG_W ? s_w[lane] : BodyDD{};
-#pragma unroll
-        for (int o = AG_W / 2; o > 0; o >>= 1)
-            v = bdd_add<D>(v, BodyDD{dd_shfl_down(v.m, o), dd_shfl_down(v.c0, o), dd_shfl_down(v.c1, o),
-                                     D == 3 ? dd_shfl_down(v.c2, o) : DD{0.0, 0.0}});
-        if (lane == 0) s_w[AG_W] = v;
+    if (lane == 31) {
+        s_w[w] = inc;
+        s_c[w] = ci;
     }
     __syncthreads();
-    const BodyDD r = s_w[AG_W];
+    if (w == 0) {
+        Body t = lane < AG_W ? s_w[lane] : Body{0.0, 0.0, 0.0, 0.0};
+        uint32_t tc = lane < AG_W ? s_c[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < AG_W; o <<= 1) {
+            const Body u{shfl_up_d(t.m, o), shfl_up_d(t.c0, o), shfl_up_d(t.c1, o), D == 3 ? shfl_up_d(t.c2, o) : 0.0};
+            const uint32_t cu = __shfl_up_sync(GR_FULL, tc, o);
+            if (lane >= o) {
+                t = body_sum<D>(u, t);
+                tc += cu;
+            }
+        }
+        if (lane < AG_W) {
+            s_w[AG_W + lane] = t;
+            s_c[AG_W + lane] = tc;
+        }
+    }
     __syncthreads();
-    return r;
+    const Body before = w > 0 ? s_w[AG_W + w - 1] : Body{0.0, 0.0, 0.0, 0.0};
+    const uint32_t cbefore = w > 0 ? s_c[AG_W + w - 1] : 0u;
+    total = s_w[2 * AG_W - 1];
+    tcnt = s_c[2 * AG_W - 1];
+    Body lanes_before{shfl_up_d(inc.m, 1), shfl_up_d(inc.c0, 1), shfl_up_d(inc.c1, 1),
+                      D == 3 ? shfl_up_d(inc.c2, 1) : 0.0};  // inclusive scan of the lane before
+    uint32_t clb = __shfl_up_sync(GR_FULL, ci, 1);
+    if (lane == 0) {
+        lanes_before = Body{0.0, 0.0, 0.0, 0.0};
+        clb = 0;
+    }
+    __syncthreads();
+    ex = body_sum<D>(before, lanes_before);
+    exc = cbefore + clb;
 }
 
 // The stored prefix: D + 1 double-doubles per leaf (the mass, then the D mass
@@ -572,163 +601,191 @@ __device__ __forceinline__ BodyDD prefix_get(const DD *__restrict__ pre, uint32_
     return BodyDD{{a.x, a.y}, {b.x, b.y}, {c.x, c.y}, {d.x, d.y}};
 }
 
-__device__ __forceinline__ void bdd_store(BodyDD *p, const BodyDD &b) {
-    double2 *q = reinterpret_cast<double2 *>(p);
-    q[0] = make_double2(b.m.hi, b.m.lo);
-    q[1] = make_double2(b.c0.hi, b.c0.lo);
-    q[2] = make_double2(b.c1.hi, b.c1.lo);
-    q[3] = make_double2(b.c2.hi, b.c2.lo);
-}
-
-__device__ __forceinline__ BodyDD bdd_load_cg(const BodyDD *p) {
-    const double2 *q = reinterpret_cast<const double2 *>(p);
-    const double2 a = __ldcg(q), b = __ldcg(q + 1), c = __ldcg(q + 2), d = __ldcg(q + 3);
-    return BodyDD{{a.x, a.y}, {b.x, b.y}, {c.x, c.y}, {d.x, d.y}};
-}
-
-constexpr uint32_t DD_SPIN_LIMIT = 1u << 22;  // x 32 ns sleeps: ~0.1 s
-
-// A point's exact FP64 terms: m and m * x per axis (a product of two FP32
-// values is exact in FP64).
+// This thread's AG_I consecutive sorted points p0 .. p0 + AG_I - 1 (< n): their
+// keys, the "first of its key" bits (fl) and their FP64 terms summed in order.
 template <int D>
-__device__ __forceinline__ BodyDD point_terms(const float4 &p) {
-    const double m = (double)p.w;
-    return BodyDD{{m, 0.0}, {m * (double)p.x, 0.0}, {m * (double)p.y, 0.0}, {D == 3 ? m * (double)p.z : 0.0, 0.0}};
-}
-
-// Exclusive block scan (AG_T threads) of one count per thread; total = the
-// block's sum.
-__device__ __forceinline__ uint32_t block_excl_u32(uint32_t x, uint32_t &total, uint32_t *s_c) {
-    const int lane = threadIdx.x % GR_WARP, w = threadIdx.x / GR_WARP;
-    uint32_t inc = x;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(GR_FULL, inc, o);
-        if (lane >= o) inc += y;
-    }
-    if (lane == 31) s_c[w] = inc;
-    __syncthreads();
-    uint32_t before = 0;
-    total = 0;
-#pragma unroll
-    for (int k = 0; k < AG_W; k++) {
-        const uint32_t v = s_c[k];
-        before += k < w ? v : 0u;
-        total += v;
-    }
-    __syncthreads();
-    return before + inc - x;
-}
-
-// One pass over the sorted points (AG_TILE per tile, AG_I consecutive points
-// per thread; tile ids in start order from the counter at tile_flag[gridDim.x]):
-//  - the sorted point records sp[p] = pos[perm[p]], sorig[p] = perm[p];
-//  - "first of its key" flags and their exclusive count, the leaf index:
-//    uid[p], and at a leaf's first point leaf_start, ukey and an empty cell
-//    level mask; the last tile writes n_unique and leaf_start[n_unique] = n;
-//  - the exclusive double-double prefix of the point terms (point_terms) at
-//    each leaf's first point, and its total at n_unique.
-// Tile b publishes its totals (tile_sum[b], tile_cnt[b], then tile_flag[b] =
-// 1) and adds the totals of every tile before it in a fixed order: thread j
-// takes tiles j, j + AG_T, ... in turn, then block_total_bdd. So the prefix
-// does not depend on which tiles finished first and is the same every run.
-// The flags and the counter must be zero at launch. A wait that runs out sets
-// ERR_WAIT and goes on with what it read.
-template <int D>
-__global__ void __launch_bounds__(AG_T)
-k_sorted_leaves(DevState *st, uint32_t n, const float4 *__restrict__ pos, const uint64_t *__restrict__ keys,
-                const uint32_t *__restrict__ perm, float4 *__restrict__ sp, uint32_t *__restrict__ sorig,
-                uint32_t *__restrict__ uid, uint32_t *__restrict__ leaf_start, uint64_t *__restrict__ ukey,
-                uint32_t *__restrict__ levels, BodyDD *tile_sum, uint32_t *tile_cnt, uint32_t *tile_flag,
-                DD *__restrict__ prefix) {
-    if (st->converged) return;
-    __shared__ BodyDD s_w[2 * AG_W];
-    __shared__ uint32_t s_c[AG_W];
-    __shared__ uint32_t s_tile;
-    const uint32_t nt = (n + AG_TILE - 1) / AG_TILE;
-    if (threadIdx.x == 0) s_tile = atomicAdd(&tile_flag[gridDim.x], 1u);
-    __syncthreads();
-    const uint32_t b = s_tile;
-    if (b >= nt) return;
-    const uint32_t p0 = b * AG_TILE + threadIdx.x * AG_I;
-    uint64_t k[AG_I];
-    uint32_t q[AG_I];
-    float4 pt[AG_I];
-#pragma unroll
-    for (int r = 0; r < AG_I; r++) {
-        k[r] = p0 + r < n ? keys[p0 + r] : 0ull;
-        q[r] = p0 + r < n ? perm[p0 + r] : 0u;
-        if (q[r] >= n) {  // only after a sort pass gave up a wait (ERR_WAIT): keep the reads in bounds
-            atomicOr(&st->error, (uint32_t)ERR_TREE);
-            q[r] = 0;
-        }
-    }
+__device__ __forceinline__ Body point_chunk(uint32_t n, uint32_t p0, const float4 *__restrict__ pts,
+                                            const uint64_t *__restrict__ keys, uint64_t *k, uint32_t &fl) {
     const uint64_t kprev = (p0 > 0 && p0 <= n) ? keys[p0 - 1] : 0ull;
 #pragma unroll
-    for (int r = 0; r < AG_I; r++) pt[r] = p0 + r < n ? pos[q[r]] : make_float4(0.f, 0.f, 0.f, 0.f);
-    uint32_t fl = 0;
-    BodyDD acc{};
+    for (int r = 0; r < AG_I; r++) k[r] = p0 + r < n ? keys[p0 + r] : 0ull;
+    Body acc{0.0, 0.0, 0.0, 0.0};
+    fl = 0;
 #pragma unroll
     for (int r = 0; r < AG_I; r++) {
         const uint32_t p = p0 + r;
         if (p < n) {
             const bool f = p == 0 || k[r] != (r == 0 ? kprev : k[r - 1]);
             fl |= (f ? 1u : 0u) << r;
-            acc = bdd_add<D>(acc, point_terms<D>(pt[r]));
-            sp[p] = pt[r];
-            sorig[p] = q[r];
+            acc = body_sum<D>(acc, point_body<D>(pts[r]));
         }
     }
-    BodyDD total;
-    const BodyDD ex = block_scan_bdd<D>(acc, BodyDD{}, total, s_w);
-    uint32_t tcnt;
-    const uint32_t exc = block_excl_u32((uint32_t)__popc(fl), tcnt, s_c);
+    return acc;
+}
+
+// (1 of 3) Tile b of AG_TILE sorted points: the sorted point records sp[p] =
+// pos[perm[p]], sorig[p] = perm[p]; the tile's FP64 term sums and its count of
+// leaves (points that start a key), as block_scan_body totals them.
+template <int D>
+__global__ void __launch_bounds__(AG_T)
+k_leaf_tiles(DevState *st, uint32_t n, const float4 *__restrict__ pos, const uint64_t *__restrict__ keys,
+             const uint32_t *__restrict__ perm, float4 *__restrict__ sp, uint32_t *__restrict__ sorig,
+             Body *__restrict__ tile_sum, uint32_t *__restrict__ tile_cnt) {
+    if (st->converged) return;
+    __shared__ Body s_w[2 * AG_W];
+    __shared__ uint32_t s_c[2 * AG_W];
+    const uint32_t b = blockIdx.x;
+    const uint32_t p0 = b * AG_TILE + threadIdx.x * AG_I;
+    uint32_t q[AG_I];
+    float4 pt[AG_I];
+#pragma unroll
+    for (int r = 0; r < AG_I; r++) {
+        q[r] = p0 + r < n ? perm[p0 + r] : 0u;
+        if (q[r] >= n) {  // only after a sort pass gave up a wait (ERR_WAIT): keep the reads in bounds
+            atomicOr(&st->error, (uint32_t)ERR_TREE);
+            q[r] = 0;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < AG_I; r++) pt[r] = p0 + r < n ? pos[q[r]] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int r = 0; r < AG_I; r++)
+        if (p0 + r < n) {
+            sp[p0 + r] = pt[r];
+            sorig[p0 + r] = q[r];
+        }
+    uint64_t k[AG_I];
+    uint32_t fl;
+    const Body acc = point_chunk<D>(n, p0, pt, keys, k, fl);
+    Body ex, total;
+    uint32_t exc, tcnt;
+    block_scan_body<D>(acc, (uint32_t)__popc(fl), ex, exc, total, tcnt, s_w, s_c);
     if (threadIdx.x == 0) {
-        bdd_store(&tile_sum[b], total);
+        tile_sum[b] = total;
         tile_cnt[b] = tcnt;
-        __threadfence();
-        atomicExch(&tile_flag[b], 1u);
     }
-    BodyDD fold{};
-    uint32_t cfold = 0;
-    volatile uint32_t *vf = tile_flag;
-    for (uint32_t j = threadIdx.x; j < b; j += AG_T) {
-        for (uint32_t spins = 0; vf[j] == 0u;) {
-            if (++spins > DD_SPIN_LIMIT) {
-                atomicOr(&st->error, (uint32_t)ERR_WAIT);
-                break;
-            }
-            __nanosleep(32);
+}
+
+constexpr int CARRY_T = 1024;
+
+// (2 of 3) One block: the exclusive double-double prefix of the tile sums and
+// the exclusive prefix of the tile leaf counts, in a fixed order (thread t
+// folds tiles [t c, t c + c) in turn, then a fixed-shape scan over the
+// threads). Writes n_unique, leaf_start[n_unique] = n and the total prefix at
+// n_unique.
+template <int D>
+__global__ void __launch_bounds__(CARRY_T)
+k_leaf_carry(DevState *st, uint32_t n, const Body *__restrict__ tile_sum, const uint32_t *__restrict__ tile_cnt,
+             BodyDD *__restrict__ carry, uint32_t *__restrict__ ccarry, uint32_t *__restrict__ leaf_start,
+             DD *__restrict__ prefix) {
+    if (st->converged) return;
+    constexpr int W = CARRY_T / GR_WARP;
+    __shared__ BodyDD s_w[W];
+    __shared__ uint32_t s_c[W];
+    const uint32_t nt = (n + AG_TILE - 1) / AG_TILE;
+    const uint32_t per = (nt + CARRY_T - 1) / CARRY_T;
+    const uint32_t t0 = threadIdx.x * per, t1 = min(t0 + per, nt);
+    BodyDD acc{};
+    uint32_t cacc = 0;
+    for (uint32_t j = t0; j < t1; j++) {
+        acc = bdd_add_body<D>(acc, tile_sum[j]);
+        cacc += tile_cnt[j];
+    }
+    const int lane = threadIdx.x % GR_WARP, w = threadIdx.x / GR_WARP;
+    BodyDD inc = acc;
+    uint32_t ci = cacc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const BodyDD u = bdd_shfl_up<D>(inc, o);
+        const uint32_t cu = __shfl_up_sync(GR_FULL, ci, o);
+        if (lane >= o) {
+            inc = bdd_add<D>(u, inc);
+            ci += cu;
         }
-        __threadfence();
-        fold = bdd_add<D>(fold, bdd_load_cg(&tile_sum[j]));
-        cfold += __ldcg(&tile_cnt[j]);
     }
-    const BodyDD carry = block_total_bdd<D>(fold, s_w);
-    uint32_t ccarry;
-    block_excl_u32(cfold, ccarry, s_c);
-    BodyDD run = bdd_add<D>(carry, ex);
-    uint32_t e = ccarry + exc;  // leaves that start before this thread's first point
+    if (lane == 31) {
+        s_w[w] = inc;
+        s_c[w] = ci;
+    }
+    __syncthreads();
+    if (w == 0) {
+        BodyDD t = s_w[lane];
+        uint32_t tc = s_c[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const BodyDD u = bdd_shfl_up<D>(t, o);
+            const uint32_t cu = __shfl_up_sync(GR_FULL, tc, o);
+            if (lane >= o) {
+                t = bdd_add<D>(u, t);
+                tc += cu;
+            }
+        }
+        s_w[lane] = t;  // inclusive over warps 0 .. lane
+        s_c[lane] = tc;
+    }
+    __syncthreads();
+    BodyDD lanes_before = bdd_shfl_up<D>(inc, 1);
+    uint32_t clb = __shfl_up_sync(GR_FULL, ci, 1);
+    if (lane == 0) {
+        lanes_before = BodyDD{};
+        clb = 0;
+    }
+    BodyDD run = bdd_add<D>(w > 0 ? s_w[w - 1] : BodyDD{}, lanes_before);
+    uint32_t crun = (w > 0 ? s_c[w - 1] : 0u) + clb;
+    for (uint32_t j = t0; j < t1; j++) {
+        carry[j] = run;
+        ccarry[j] = crun;
+        run = bdd_add_body<D>(run, tile_sum[j]);
+        crun += tile_cnt[j];
+    }
+    if (threadIdx.x == CARRY_T - 1) {  // the last thread's run is the grand total
+        const uint32_t nu = min(crun, n);
+        st->n_unique = nu;
+        leaf_start[nu] = n;
+        prefix_put<D>(prefix, nu, run);
+    }
+}
+
+// (3 of 3) Tile b again: every point's leaf index uid[p]; at a leaf's first
+// point leaf_start, ukey, an empty cell level mask and the prefix: the tile's
+// double-double carry plus the FP64 in-tile exclusive prefix of the terms.
+template <int D>
+__global__ void __launch_bounds__(AG_T)
+k_leaf_prefix(const DevState *st, uint32_t n, const float4 *__restrict__ sp, const uint64_t *__restrict__ keys,
+              const BodyDD *__restrict__ carry, const uint32_t *__restrict__ ccarry, uint32_t *__restrict__ uid,
+              uint32_t *__restrict__ leaf_start, uint64_t *__restrict__ ukey, uint32_t *__restrict__ levels,
+              DD *__restrict__ prefix) {
+    if (st->converged) return;
+    __shared__ Body s_w[2 * AG_W];
+    __shared__ uint32_t s_c[2 * AG_W];
+    const uint32_t b = blockIdx.x;
+    const uint32_t p0 = b * AG_TILE + threadIdx.x * AG_I;
+    float4 pt[AG_I];
+#pragma unroll
+    for (int r = 0; r < AG_I; r++) pt[r] = p0 + r < n ? sp[p0 + r] : make_float4(0.f, 0.f, 0.f, 0.f);
+    uint64_t k[AG_I];
+    uint32_t fl;
+    const Body acc = point_chunk<D>(n, p0, pt, keys, k, fl);
+    Body ex, total;
+    uint32_t exc, tcnt;
+    block_scan_body<D>(acc, (uint32_t)__popc(fl), ex, exc, total, tcnt, s_w, s_c);
+    const BodyDD c = carry[b];
+    uint32_t e = ccarry[b] + exc;  // leaves that start before this thread's first point
+    Body run = ex;
 #pragma unroll
     for (int r = 0; r < AG_I; r++) {
         const uint32_t p = p0 + r;
         if (p < n) {
-            if (((fl >> r) & 1u) && e < n) {  // e < n unless a wait gave up
-                prefix_put<D>(prefix, e, run);
+            if (((fl >> r) & 1u) && e < n) {  // e < n unless a sort pass gave up a wait
+                prefix_put<D>(prefix, e, bdd_add_body<D>(c, run));
                 leaf_start[e] = p;
                 ukey[e] = k[r];
                 levels[e] = 0;
                 e++;
             }
             uid[p] = e - 1;
-            run = bdd_add<D>(run, point_terms<D>(pt[r]));
+            run = body_sum<D>(run, point_body<D>(pt[r]));
         }
-    }
-    if (b == nt - 1 && threadIdx.x == 0) {
-        const uint32_t nu = min(ccarry + tcnt, n);
-        st->n_unique = nu;
-        leaf_start[nu] = n;
-        prefix_put<D>(prefix, nu, bdd_add<D>(carry, total));
     }
 }
 
