@@ -145,10 +145,11 @@ struct gr_fa2 {
     uint2 *long_runs = nullptr;    // those runs (start, length)
     uint32_t *vals = nullptr, *sorig = nullptr, *uid = nullptr;
     uint32_t *leaf_start = nullptr, *levels = nullptr, *P = nullptr, *leaf_pre = nullptr;
+    uint8_t *cell_flag = nullptr;  // internal node -> 1 when it is a cell
     float4 *sp = nullptr;
     BinTree bt{};
     Body *leaf_body = nullptr, *int_body = nullptr;
-    DD *dd_prefix = nullptr;             // (n + 1) x (D + 1) double-doubles
+    double *pre_local = nullptr;         // (n + 1) x (D + 1): the in-tile part of every leaf's prefix
     Body *tile_sum = nullptr;            // per tile of AG_TILE sorted points: FP64 term sums
     BodyDD *tile_carry = nullptr;        // and their exclusive double-double prefix
     uint32_t *tile_cnt = nullptr;        // leaf counts per tile, then their exclusive prefix
@@ -233,6 +234,7 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
     A(h->uid, n);
     A(h->leaf_start, (size_t)n + 1);
     A(h->levels, n);
+    A(h->cell_flag, n);
     A(h->P, (size_t)n + 1);
     A(h->leaf_pre, n);
     A(h->sp, n);
@@ -248,7 +250,7 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
     A(h->leaf_body, n);
     A(h->int_body, n);
     A(h->leaf_coinc, n);
-    A(h->dd_prefix, 4 * ((size_t)n + 1));
+    A(h->pre_local, 4 * ((size_t)n + 1));
     A(h->tile_sum, div_up(n, AG_TILE) + 1);
     A(h->tile_carry, div_up(n, AG_TILE) + 1);
     A(h->tile_cnt, 2 * ((size_t)div_up(n, AG_TILE) + 1));
@@ -337,22 +339,24 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
         k_leaf_tiles<D><<<ab, AG_T, 0, s>>>(st, n, h->pos, h->keys, h->vals, h->sp, h->sorig, h->tile_sum,
                                              h->tile_cnt);
         k_leaf_carry<D><<<1, CARRY_T, 0, s>>>(st, n, h->tile_sum, h->tile_cnt, h->tile_carry, h->tile_cnt + ab,
-                                              h->leaf_start, h->dd_prefix);
-        k_leaf_prefix<D><<<ab, AG_T, 0, s>>>(st, n, h->sp, h->keys, h->tile_carry, h->tile_cnt + ab, h->uid,
-                                              h->leaf_start, h->ukey, h->levels, h->dd_prefix);
+                                              h->leaf_start, h->pre_local);
+        k_leaf_prefix<D><<<ab, AG_T, 0, s>>>(st, n, h->sp, h->keys, h->tile_cnt + ab, h->uid, h->leaf_start,
+                                              h->ukey, h->levels, h->pre_local);
+        const Prefix pre{h->pre_local, h->tile_carry, h->leaf_start, 0u, ab};  // nu: read on the device
         const bool adjoint = h->bt.cell_of != nullptr;  // the adjoint reads leaf and node bodies as arrays
         BinTree bt = h->bt;  // the tick itself reads only the packed records and leaf_parent
         bt.levels = h->levels;
+        bt.cell_flag = h->cell_flag;
         if (!adjoint) {
             bt.first = bt.last = bt.left = bt.right = bt.visit = nullptr;
             bt.delta = bt.int_parent = nullptr;
         }
         k_karras<D><<<gn, 256, 0, s>>>(st, h->ukey, bt);
         if (adjoint) k_leaf_body<D><<<gn, 256, 0, s>>>(st, h->sp, h->leaf_start, h->leaf_body, h->leaf_coinc);
-        if (adjoint) k_node_body<D><<<gn, 256, 0, s>>>(st, h->bt, h->dd_prefix, h->int_body);
+        if (adjoint) k_node_body<D><<<gn, 256, 0, s>>>(st, h->bt, pre, h->int_body);
         h->scanner.scan_levels(h->levels, h->P, n, &st->n_unique, &st->n_cells, s, conv);
         k_assign_cells<D><<<2 * gn, 256, 0, s>>>(st, bt, gn * 256, h->sp, h->P, h->levels, h->leaf_start,
-                                                 h->dd_prefix, h->cells, h->leaf_pre, st);
+                                                 pre, h->cells, h->leaf_pre, st);
     }
     if (h->timing_events) cudaEventRecordWithFlags(h->ev[1], s, cudaEventRecordExternal);
     if (branch) {
@@ -1123,6 +1127,7 @@ static int forces_static(uint32_t n, const float4 *nodes, const uint32_t *rp, co
     h.uid = cv.take<uint32_t>(n);
     h.leaf_start = cv.take<uint32_t>((size_t)n + 1);
     h.levels = cv.take<uint32_t>(n);
+    h.cell_flag = cv.take<uint8_t>(n);
     h.P = cv.take<uint32_t>((size_t)n + 1);
     h.leaf_pre = cv.take<uint32_t>(n);
     h.sp = cv.take<float4>(n);
@@ -1138,7 +1143,7 @@ static int forces_static(uint32_t n, const float4 *nodes, const uint32_t *rp, co
     h.leaf_body = cv.take<Body>(n);
     h.int_body = cv.take<Body>(n);
     h.leaf_coinc = cv.take<uint8_t>(n);
-    h.dd_prefix = cv.take<DD>(4 * ((size_t)n + 1));
+    h.pre_local = cv.take<double>(4 * ((size_t)n + 1));
     h.tile_sum = cv.take<Body>(div_up(n, AG_TILE) + 1);
     h.tile_carry = cv.take<BodyDD>(div_up(n, AG_TILE) + 1);
     h.tile_cnt = cv.take<uint32_t>(2 * ((size_t)div_up(n, AG_TILE) + 1));

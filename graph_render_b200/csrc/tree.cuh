@@ -250,6 +250,7 @@ struct BinTree {
     uint32_t *cell_of;    // internal node -> its cell's preorder index, when it is a cell (nullable)
     int4 *rec;            // internal node -> {first, last, parent, delta} in one load (nullable)
     uint32_t *levels;     // unique leaf s -> bit l set when a cell of level l begins at s (nullable)
+    uint8_t *cell_flag;   // internal node -> 1 when it is a cell (written with levels)
 };
 
 // What karras_node found for internal node i: its leaf range, split and
@@ -333,16 +334,22 @@ __device__ __forceinline__ KarrasNode karras_node(int32_t i, int32_t nu, const u
 // (3D, 63-bit keys).
 template <int D>
 __device__ __forceinline__ void mark_cells(int32_t i, int32_t nu, const uint64_t *__restrict__ k,
-                                           const KarrasNode &q, uint32_t *__restrict__ levels) {
+                                           const KarrasNode &q, uint32_t *__restrict__ levels,
+                                           uint8_t *__restrict__ cell_flag) {
     const int lv = q.delta / D;
-    if (i == 0) atomicOr(&levels[0], 1u << lv);
-    if (q.first != q.gamma) {  // left child [first, gamma]
+    if (i == 0) {
+        atomicOr(&levels[0], 1u << lv);
+        cell_flag[0] = 1;
+    }
+    if (q.first != q.gamma) {  // left child [first, gamma], internal node gamma
         const int c = kdelta(k, q.first, q.gamma, nu) / D;
         if (c != lv) atomicOr(&levels[q.first], 1u << c);
+        cell_flag[q.gamma] = c != lv ? 1 : 0;
     }
-    if (q.last != q.gamma + 1) {  // right child [gamma + 1, last]
+    if (q.last != q.gamma + 1) {  // right child [gamma + 1, last], internal node gamma + 1
         const int c = kdelta(k, q.gamma + 1, q.last, nu) / D;
         if (c != lv) atomicOr(&levels[q.gamma + 1], 1u << c);
+        cell_flag[q.gamma + 1] = c != lv ? 1 : 0;
     }
 }
 
@@ -354,7 +361,7 @@ __global__ void k_karras(const DevState *st, const uint64_t *__restrict__ k, Bin
     if (i == 0 && nu == 1) t.leaf_parent[0] = -1;
     if (i >= nu - 1) return;
     const KarrasNode q = karras_node(i, nu, k, t);
-    if (t.levels) mark_cells<D>(i, nu, k, q, t.levels);
+    if (t.levels) mark_cells<D>(i, nu, k, q, t.levels, t.cell_flag);
 }
 
 // Leaf s's FP64 sums, then the bottom-up pass: the second thread to reach a
@@ -582,23 +589,32 @@ __device__ __forceinline__ void block_scan_body(const Body &x, uint32_t c, Body 
     exc = cbefore + clb;
 }
 
-// The stored prefix: D + 1 double-doubles per leaf (the mass, then the D mass
-// moments), 48 B in 2D and 64 B in 3D.
+// The stored prefix of leaf s: the FP64 in-tile part, D + 1 doubles (the mass,
+// then the D mass moments; 24 B in 2D), beside the double-double carry of the
+// tile that holds the leaf's first point (carry[nt] is the grand total, and
+// leaf nu has in-tile part 0). The prefix is carry + in-tile part.
+struct Prefix {
+    const double *local;  // (nu + 1) x (D + 1)
+    const BodyDD *carry;  // nt + 1
+    const uint32_t *leaf_start;
+    uint32_t nu, nt;
+};
+
 template <int D>
-__device__ __forceinline__ void prefix_put(DD *__restrict__ pre, uint32_t s, const BodyDD &b) {
-    double2 *q = reinterpret_cast<double2 *>(pre + (size_t)s * (D + 1));
-    q[0] = make_double2(b.m.hi, b.m.lo);
-    q[1] = make_double2(b.c0.hi, b.c0.lo);
-    q[2] = make_double2(b.c1.hi, b.c1.lo);
-    if (D == 3) q[3] = make_double2(b.c2.hi, b.c2.lo);
+__device__ __forceinline__ void local_put(double *__restrict__ pre, uint32_t s, const Body &b) {
+    double *q = pre + (size_t)s * (D + 1);
+    q[0] = b.m;
+    q[1] = b.c0;
+    q[2] = b.c1;
+    if (D == 3) q[3] = b.c2;
 }
 
 template <int D>
-__device__ __forceinline__ BodyDD prefix_get(const DD *__restrict__ pre, uint32_t s) {
-    const double2 *q = reinterpret_cast<const double2 *>(pre + (size_t)s * (D + 1));
-    const double2 a = q[0], b = q[1], c = q[2];
-    const double2 d = D == 3 ? q[3] : make_double2(0.0, 0.0);
-    return BodyDD{{a.x, a.y}, {b.x, b.y}, {c.x, c.y}, {d.x, d.y}};
+__device__ __forceinline__ BodyDD prefix_at(const Prefix &P, uint32_t s) {
+    const double *q = P.local + (size_t)s * (D + 1);
+    const Body b{q[0], q[1], q[2], D == 3 ? q[3] : 0.0};
+    const uint32_t tile = s >= P.nu ? P.nt : P.leaf_start[s] / AG_TILE;
+    return bdd_add_body<D>(P.carry[tile], b);
 }
 
 // This thread's AG_I consecutive sorted points p0 .. p0 + AG_I - 1 (< n): their
@@ -671,13 +687,13 @@ constexpr int CARRY_T = 1024;
 // (2 of 3) One block: the exclusive double-double prefix of the tile sums and
 // the exclusive prefix of the tile leaf counts, in a fixed order (thread t
 // folds tiles [t c, t c + c) in turn, then a fixed-shape scan over the
-// threads). Writes n_unique, leaf_start[n_unique] = n and the total prefix at
-// n_unique.
+// threads). Writes n_unique, leaf_start[n_unique] = n, the grand total as
+// carry[nt] and a zero in-tile part for leaf n_unique.
 template <int D>
 __global__ void __launch_bounds__(CARRY_T)
 k_leaf_carry(DevState *st, uint32_t n, const Body *__restrict__ tile_sum, const uint32_t *__restrict__ tile_cnt,
              BodyDD *__restrict__ carry, uint32_t *__restrict__ ccarry, uint32_t *__restrict__ leaf_start,
-             DD *__restrict__ prefix) {
+             double *__restrict__ pre) {
     if (st->converged) return;
     constexpr int W = CARRY_T / GR_WARP;
     __shared__ BodyDD s_w[W];
@@ -742,19 +758,19 @@ k_leaf_carry(DevState *st, uint32_t n, const Body *__restrict__ tile_sum, const 
         const uint32_t nu = min(crun, n);
         st->n_unique = nu;
         leaf_start[nu] = n;
-        prefix_put<D>(prefix, nu, run);
+        carry[nt] = run;
+        local_put<D>(pre, nu, Body{0.0, 0.0, 0.0, 0.0});
     }
 }
 
 // (3 of 3) Tile b again: every point's leaf index uid[p]; at a leaf's first
-// point leaf_start, ukey, an empty cell level mask and the prefix: the tile's
-// double-double carry plus the FP64 in-tile exclusive prefix of the terms.
+// point leaf_start, ukey, an empty cell level mask and the in-tile part of its
+// prefix (the FP64 in-tile exclusive prefix of the terms).
 template <int D>
 __global__ void __launch_bounds__(AG_T)
 k_leaf_prefix(const DevState *st, uint32_t n, const float4 *__restrict__ sp, const uint64_t *__restrict__ keys,
-              const BodyDD *__restrict__ carry, const uint32_t *__restrict__ ccarry, uint32_t *__restrict__ uid,
-              uint32_t *__restrict__ leaf_start, uint64_t *__restrict__ ukey, uint32_t *__restrict__ levels,
-              DD *__restrict__ prefix) {
+              const uint32_t *__restrict__ ccarry, uint32_t *__restrict__ uid, uint32_t *__restrict__ leaf_start,
+              uint64_t *__restrict__ ukey, uint32_t *__restrict__ levels, double *__restrict__ pre) {
     if (st->converged) return;
     __shared__ Body s_w[2 * AG_W];
     __shared__ uint32_t s_c[2 * AG_W];
@@ -769,7 +785,6 @@ k_leaf_prefix(const DevState *st, uint32_t n, const float4 *__restrict__ sp, con
     Body ex, total;
     uint32_t exc, tcnt;
     block_scan_body<D>(acc, (uint32_t)__popc(fl), ex, exc, total, tcnt, s_w, s_c);
-    const BodyDD c = carry[b];
     uint32_t e = ccarry[b] + exc;  // leaves that start before this thread's first point
     Body run = ex;
 #pragma unroll
@@ -777,7 +792,7 @@ k_leaf_prefix(const DevState *st, uint32_t n, const float4 *__restrict__ sp, con
         const uint32_t p = p0 + r;
         if (p < n) {
             if (((fl >> r) & 1u) && e < n) {  // e < n unless a sort pass gave up a wait
-                prefix_put<D>(prefix, e, bdd_add_body<D>(c, run));
+                local_put<D>(pre, e, run);
                 leaf_start[e] = p;
                 ukey[e] = k[r];
                 levels[e] = 0;
@@ -798,12 +813,12 @@ __device__ __forceinline__ Body range_body(const BodyDD &a, const BodyDD &b) {
 // Every internal node's body as an array (the adjoint reads them; the tick's
 // own cell writer takes range_body of the cells only).
 template <int D>
-__global__ void k_node_body(const DevState *st, BinTree t, const DD *__restrict__ prefix,
-                            Body *__restrict__ int_body) {
+__global__ void k_node_body(const DevState *st, BinTree t, Prefix pre, Body *__restrict__ int_body) {
     if (st->converged) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i + 1 >= st->n_unique) return;
-    body_store(&int_body[i], range_body(prefix_get<D>(prefix, t.first[i]), prefix_get<D>(prefix, t.last[i] + 1)));
+    pre.nu = st->n_unique;
+    if (i + 1 >= pre.nu) return;
+    body_store(&int_body[i], range_body(prefix_at<D>(pre, t.first[i]), prefix_at<D>(pre, t.last[i] + 1)));
 }
 
 template <int D>
@@ -920,7 +935,7 @@ __device__ __forceinline__ void assign_leaf(uint32_t s, uint32_t nu, uint32_t nc
 template <int D>
 __global__ void k_assign_cells(const DevState *st, BinTree t, uint32_t n_slots, const float4 *__restrict__ sp,
                                const uint32_t *__restrict__ P, const uint32_t *__restrict__ levels,
-                               const uint32_t *__restrict__ leaf_start, const DD *__restrict__ prefix,
+                               const uint32_t *__restrict__ leaf_start, Prefix pre,
                                Cells cells, uint32_t *__restrict__ leaf_pre,
                                DevState *stw) {
     if (st->converged) return;
@@ -933,7 +948,6 @@ __global__ void k_assign_cells(const DevState *st, BinTree t, uint32_t n_slots, 
         const uint32_t s = g;
         if (s >= nu) return;
         const uint32_t idx = P[s] + __popc(levels[s]);
-        const int32_t par = t.leaf_parent[s];
         const uint32_t a0 = leaf_start[s], a1 = leaf_start[s + 1];
         if (idx >= ncells || a1 <= a0) {
             atomicOr(&stw->error, (uint32_t)ERR_TREE);
@@ -942,17 +956,16 @@ __global__ void k_assign_cells(const DevState *st, BinTree t, uint32_t n_slots, 
         const float4 one = sp[a0];
         bool coinc;
         const Body body = leaf_sum<D>(sp, a0, a1, coinc);
-        int level = 0;
-        if (par >= 0) level = coinc ? t.rec[par].w / D + 1 : L;
+        // the parent's record only for coincident points (one leaf alone is the root)
+        const int level = nu == 1 ? 0 : coinc ? t.rec[t.leaf_parent[s]].w / D + 1 : L;
         write_cell<D>(cells, idx, body, level, rw, -(int32_t)(a1 - a0), a0, a1 - a0 == 1 ? &one : nullptr);
         if (D == 2 && cells.bounds) write_bounds(cells, idx, one, level, st);
         leaf_pre[s] = idx;
         return;
     }
     const uint32_t i = g - n_slots;
-    if (i + 1 >= nu) return;
+    if (i + 1 >= nu || !t.cell_flag[i]) return;
     const int4 R = t.rec[i];
-    if (R.z >= 0 && R.w / D == t.rec[R.z].w / D) return;  // not a cell: its parent has its level
     const int lv = R.w / D;
     const uint32_t f = (uint32_t)R.x, end = (uint32_t)R.y + 1;
     const uint32_t idx = P[f] + __popc(levels[f] & ((1u << lv) - 1u));
@@ -962,8 +975,8 @@ __global__ void k_assign_cells(const DevState *st, BinTree t, uint32_t n_slots, 
         return;
     }
     const uint32_t a0 = leaf_start[f];
-    write_cell<D>(cells, idx, range_body(prefix_get<D>(prefix, f), prefix_get<D>(prefix, end)), lv, rw, (int32_t)skip,
-                  a0);
+    pre.nu = nu;
+    write_cell<D>(cells, idx, range_body(prefix_at<D>(pre, f), prefix_at<D>(pre, end)), lv, rw, (int32_t)skip, a0);
     if (D == 2 && cells.bounds) write_bounds(cells, idx, sp[a0], lv, st);
     if (t.cell_of) t.cell_of[i] = idx;
 }
