@@ -397,10 +397,10 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
             attraction_seg(s);
             attraction_rows(s);
         }
-        k_forces<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(fp, st, h->pos, h->rep, h->U, h->part,
+        k_forces<D><<<frc_blocks(n), FRC_THREADS, 0, s>>>(fp, st, h->pos, h->rep, h->U, h->part,
                                                                     forces_only ? 0 : 1);
         if (!forces_only)
-            k_update<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(n, st, h->pos, h->U, h->part);
+            k_update<D><<<frc_blocks(n), FRC_THREADS, 0, s>>>(n, st, h->pos, h->U, h->part);
     }
     if (h->timing_events) cudaEventRecordWithFlags(h->ev[3], s, cudaEventRecordExternal);
 }
@@ -1633,7 +1633,7 @@ static void adjoint_tick(gr_fa2 *h, Adjoint *a, const DevState *before) {
             h->nseg, fp.lin_log, st, h->pos, h->rp, h->col, h->wt, h->seg_row, h->seg_first, h->seg_out);
     k_attract<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(n, fp.lin_log, st, h->pos, h->rp, h->col, h->wt,
                                                                  h->nseg ? h->seg_first : nullptr, h->seg_out, h->U);
-    k_forces<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, s>>>(fp, st, h->pos, h->rep, h->U, h->part, 1);
+    k_forces<D><<<frc_blocks(n), FRC_THREADS, 0, s>>>(fp, st, h->pos, h->rep, h->U, h->part, 1);
     const uint32_t gb = div_up(n, FRC_THREADS);
     k_adj_update<D><<<gb, FRC_THREADS, 0, s>>>(n, h->prm[P_JT], st, before, a->A, h->pos, h->U, a->lam1, a->lam, a->ub,
                                                 a->part);

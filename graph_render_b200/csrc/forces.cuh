@@ -18,6 +18,14 @@
 namespace gr {
 
 constexpr int FRC_THREADS = 256;
+// k_forces and k_update stride over the nodes with at most FRC_MAX_BLOCKS
+// blocks (8 per SM): fewer per-block partials and last-block tickets.
+constexpr uint32_t FRC_MAX_BLOCKS = 8 * 148;
+
+__host__ __device__ inline uint32_t frc_blocks(uint32_t n) {
+    const uint32_t b = (n + FRC_THREADS - 1) / FRC_THREADS;
+    return b < 1 ? 1 : (b > FRC_MAX_BLOCKS ? FRC_MAX_BLOCKS : b);
+}
 // Rows longer than LIGHT_MAX are summed in SEG-entry segments, one warp each,
 // so a hub of 30k neighbours costs ~120 warps instead of one thread's 30k steps.
 constexpr uint32_t LIGHT_MAX = 32;
@@ -208,14 +216,17 @@ k_forces(ForceParams P, DevState *st, const float4 *__restrict__ pos, const floa
     if (st->converged) return;
     __shared__ double s_red[32];
     __shared__ bool s_last;
-    const uint32_t i = blockIdx.x * FRC_THREADS + threadIdx.x;
     double sw = 0.0, tr = 0.0;
-    if (i < P.n) {
+    const double mean[3] = {st->mean[0], st->mean[1], st->mean[2]};
+    for (uint32_t i = blockIdx.x * FRC_THREADS + threadIdx.x; i < P.n; i += gridDim.x * FRC_THREADS) {
         const float4 p = pos[i];
         float *u = U + (size_t)i * D;
         const float a0 = u[0], a1 = u[1], a2 = D == 3 ? u[2] : 0.f;
+        double s1, t1;
         node_force<D>(P, p, a0, a1, a2, rep[(size_t)i * D + 0], rep[(size_t)i * D + 1],
-                      D == 3 ? rep[(size_t)i * D + 2] : 0.f, st->mean, u, sw, tr);
+                      D == 3 ? rep[(size_t)i * D + 2] : 0.f, mean, u, s1, t1);
+        sw += s1;
+        tr += t1;
     }
     if (!speed_update) return;
     sw = block_sum_d<FRC_THREADS>(sw, s_red);
@@ -245,12 +256,14 @@ k_update(uint32_t n, DevState *st, float4 *__restrict__ pos, const float *__rest
     if (st->converged) return;
     __shared__ double s_red[32];
     __shared__ bool s_last;
-    const uint32_t i = blockIdx.x * FRC_THREADS + threadIdx.x;
     double step = 0.0;
     bool bad = false;
-    if (i < n) {
+    const double speed = st->speed;
+    for (uint32_t i = blockIdx.x * FRC_THREADS + threadIdx.x; i < n; i += gridDim.x * FRC_THREADS) {
         float4 p = pos[i];
-        step = node_update<D>(p, U + (size_t)i * D, st->speed, bad);
+        bool b;
+        step += node_update<D>(p, U + (size_t)i * D, speed, b);
+        bad = bad || b;
         pos[i] = p;
     }
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&st->error, (uint32_t)ERR_NONFINITE);

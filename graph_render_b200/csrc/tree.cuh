@@ -682,7 +682,7 @@ k_leaf_tiles(DevState *st, uint32_t n, const float4 *__restrict__ pos, const uin
     }
 }
 
-constexpr int CARRY_T = 1024;
+constexpr int CARRY_T = 1024;  // a multiple of 32, at most 1024
 
 // (2 of 3) One block: the exclusive double-double prefix of the tile sums and
 // the exclusive prefix of the tile leaf counts, in a fixed order (thread t
@@ -725,10 +725,10 @@ k_leaf_carry(DevState *st, uint32_t n, const Body *__restrict__ tile_sum, const 
     }
     __syncthreads();
     if (w == 0) {
-        BodyDD t = s_w[lane];
-        uint32_t tc = s_c[lane];
+        BodyDD t = lane < W ? s_w[lane] : BodyDD{};
+        uint32_t tc = lane < W ? s_c[lane] : 0u;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
+        for (int o = 1; o < W; o <<= 1) {
             const BodyDD u = bdd_shfl_up<D>(t, o);
             const uint32_t cu = __shfl_up_sync(GR_FULL, tc, o);
             if (lane >= o) {
@@ -736,8 +736,10 @@ k_leaf_carry(DevState *st, uint32_t n, const Body *__restrict__ tile_sum, const 
                 tc += cu;
             }
         }
-        s_w[lane] = t;  // inclusive over warps 0 .. lane
-        s_c[lane] = tc;
+        if (lane < W) {
+            s_w[lane] = t;  // inclusive over warps 0 .. lane
+            s_c[lane] = tc;
+        }
     }
     __syncthreads();
     BodyDD lanes_before = bdd_shfl_up<D>(inc, 1);
