@@ -497,27 +497,38 @@ static int check_device(gr_fa2 *h, const DevState &s) {
 }
 
 // Heavy rows (degree > LIGHT_MAX) split into SEG-entry segments for the
-// warp-per-segment attraction pass.
+// warp-per-segment attraction pass, counted, scanned and listed on the device.
 static int build_segments(gr_fa2 *h) {
     const uint32_t n = h->n;
     if (n == 0 || h->m == 0) return GR_OK;
-    std::vector<uint32_t> rp((size_t)n + 1);
-    CU(cudaMemcpy(rp.data(), h->rp, rp.size() * 4, cudaMemcpyDeviceToHost));
-    std::vector<uint32_t> first(n, 0), srow;
-    for (uint32_t i = 0; i < n; i++) {
-        uint32_t d = rp[i + 1] - rp[i];
-        if (d <= LIGHT_MAX) continue;
-        first[i] = (uint32_t)srow.size();
-        for (uint32_t k = 0; k < (d + SEG - 1) / SEG; k++) srow.push_back(i);
-    }
-    h->nseg = (uint32_t)srow.size();
-    if (!h->nseg) return GR_OK;
+    cudaStream_t s = h->stream;
     cudaError_t e;
-    if ((e = h->alloc(&h->seg_row, h->nseg)) || (e = h->alloc(&h->seg_first, n)) ||
-        (e = h->alloc(&h->seg_out, (size_t)h->nseg * h->dim)))
+    uint32_t *cnt = nullptr, *total = nullptr;
+    if ((e = h->alloc(&h->seg_first, n)) || (e = cudaMallocAsync((void **)&cnt, (size_t)n * 4, s)) ||
+        (e = cudaMallocAsync((void **)&total, 4, s))) {
+        if (cnt) cudaFreeAsync(cnt, s);
         return set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
-    CU(cudaMemcpy(h->seg_row, srow.data(), srow.size() * 4, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(h->seg_first, first.data(), (size_t)n * 4, cudaMemcpyHostToDevice));
+    }
+    Scanner sc;
+    if ((e = sc.init(n, s, true))) {
+        cudaFreeAsync(cnt, s);
+        cudaFreeAsync(total, s);
+        return set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+    }
+    k_seg_count<<<div_up(n, 256), 256, 0, s>>>(n, h->rp, LIGHT_MAX, SEG, cnt);
+    sc.scan(cnt, h->seg_first, n, nullptr, 0, total, nullptr, s);
+    uint32_t nseg = 0;
+    cudaMemcpyAsync(&nseg, total, 4, cudaMemcpyDeviceToHost, s);
+    sc.release();
+    cudaFreeAsync(cnt, s);
+    cudaFreeAsync(total, s);
+    CU(cudaStreamSynchronize(s));
+    h->nseg = nseg;
+    if (!nseg) return GR_OK;
+    if ((e = h->alloc(&h->seg_row, nseg)) || (e = h->alloc(&h->seg_out, (size_t)nseg * h->dim)))
+        return set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+    k_seg_fill<<<div_up(n, 256), 256, 0, s>>>(n, h->rp, LIGHT_MAX, SEG, h->seg_first, h->seg_row);
+    CU(cudaGetLastError());
     return GR_OK;
 }
 
@@ -549,13 +560,9 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
     if (m && (!src || !dst)) return set_err(GR_INVALID_ARGUMENT, "edge arrays are null");
     if (m > 0x7fffffffull) return set_err(GR_INVALID_ARGUMENT, "more than 2^31 edges");
     const int D = (int)prm[P_DIM];
-    std::vector<float> xyz((size_t)n * D);
-    if (pos0) {
-        for (size_t i = 0; i < xyz.size(); i++) {
-            if (!std::isfinite(pos0[i])) return set_err(GR_INVALID_ARGUMENT, "non-finite start position");
-            xyz[i] = pos0[i];
-        }
-    } else {
+    std::vector<float> xyz;  // the seeded start when none is given (a given one is checked on the device)
+    if (!pos0) {
+        xyz.resize((size_t)n * D);
         // state.rs:272-283 / synthetic.rs:37-50: Mulberry32(seed), dim draws per node.
         uint32_t s = (uint32_t)prm[P_SEED];
         for (size_t i = 0; i < xyz.size(); i++) {
@@ -599,6 +606,7 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
             escan.release();
         };
         const uint64_t cap = std::max<uint64_t>(2 * m, 1);
+        const EdgeKey ekf = edge_key_for(n);
         if ((e = tmp(&d_err, 2 * sizeof(uint32_t))) || (e = tmp(&ms_d, 2 * sizeof(uint32_t))) ||
             (e = tmp(&ek, cap * sizeof(uint64_t))) || (e = tmp(&ev, cap * sizeof(uint32_t))) ||
             (e = tmp(&dk, cap * sizeof(uint64_t))) || (e = tmp(&dv, cap * sizeof(uint32_t))) ||
@@ -619,9 +627,9 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
             cudaMemcpyAsync(d_src, src, m * 4, cudaMemcpyHostToDevice, s);
             cudaMemcpyAsync(d_dst, dst, m * 4, cudaMemcpyHostToDevice, s);
             if (weight) cudaMemcpyAsync(d_w, weight, m * 8, cudaMemcpyHostToDevice, s);
-            k_edge_keys<<<div_up(m, 256), 256, 0, s>>>(m, d_src, d_dst, n, ek, ev, d_err);
-            esort.sort(ek, ev, (uint32_t)m, 64, s);
-            k_edge_flags<<<div_up(m, 256), 256, 0, s>>>((uint32_t)m, ek, eflag);
+            k_edge_keys<<<div_up(m, 256), 256, 0, s>>>(m, d_src, d_dst, n, ekf, ek, ev, d_err);
+            esort.sort_bits(ek, ev, (uint32_t)m, 2 * ekf.bits, s, d_err + 1);
+            k_edge_flags<<<div_up(m, 256), 256, 0, s>>>((uint32_t)m, ekf, ek, eflag);
             escan.scan(eflag, eexcl, (uint32_t)m, nullptr, 0, ms_d, nullptr, s);
         }
         uint32_t hdr[2] = {0, 0};
@@ -635,6 +643,11 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
         if (hdr[0]) {
             cleanup();
             rc = set_err(GR_INVALID_ARGUMENT, "an edge names a node >= n");
+            break;
+        }
+        if (hdr[1]) {
+            cleanup();
+            rc = set_err(GR_DEVICE_FAULT, "the edge sort gave up a bounded wait");
             break;
         }
         h->m = ms;
@@ -653,25 +666,27 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
         }
         cudaMemsetAsync(h->rp, 0, ((size_t)n + 1) * 4, s);
         if (ms) {
-            k_edge_emit<<<div_up(m, 256), 256, 0, s>>>((uint32_t)m, ek, ev, eflag, eexcl, d_w, prm[P_INFLUENCE],
-                                                          weff, slo, shi, dk, dv, d_err, h->simple_raw,
-                                                          h->simple_dcdw);
-            esort.sort(dk, dv, 2 * ms, 64, s);
-            k_csr<<<div_up(2 * (uint64_t)ms, 256), 256, 0, s>>>(n, 2 * ms, dk, dv, weff, h->rp, h->col, h->wt);
+            k_edge_emit<<<div_up(m, 256), 256, 0, s>>>((uint32_t)m, ekf, ek, ev, eflag, eexcl, d_w,
+                                                          prm[P_INFLUENCE], weff, slo, shi, dk, dv, d_err,
+                                                          h->simple_raw, h->simple_dcdw);
+            esort.sort_bits(dk, dv, 2 * ms, 2 * ekf.bits, s, d_err + 1);
+            k_csr<<<div_up(2 * (uint64_t)ms, 256), 256, 0, s>>>(n, 2 * ms, ekf, dk, dv, weff, h->rp, h->col,
+                                                                 h->wt);
             cudaMemcpyAsync(h->csr_simple, dv, 2 * (size_t)ms * 4, cudaMemcpyDeviceToDevice, s);
         }
         float *d_xyz = nullptr;
-        if ((e = tmp(&d_xyz, std::max<size_t>(xyz.size(), 1) * 4))) {
+        const size_t nxyz = (size_t)n * D;
+        if ((e = tmp(&d_xyz, std::max<size_t>(nxyz, 1) * 4))) {
             cleanup();
             rc = set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
             break;
         }
         if (n) {
-            cudaMemcpyAsync(d_xyz, xyz.data(), xyz.size() * 4, cudaMemcpyHostToDevice, s);
+            cudaMemcpyAsync(d_xyz, pos0 ? pos0 : xyz.data(), nxyz * 4, cudaMemcpyHostToDevice, s);
             if (D == 3)
-                k_init_nodes<3><<<div_up(n, 256), 256, 0, s>>>(n, d_xyz, h->rp, h->pos);
+                k_init_nodes<3><<<div_up(n, 256), 256, 0, s>>>(n, d_xyz, h->rp, h->pos, d_err);
             else
-                k_init_nodes<2><<<div_up(n, 256), 256, 0, s>>>(n, d_xyz, h->rp, h->pos);
+                k_init_nodes<2><<<div_up(n, 256), 256, 0, s>>>(n, d_xyz, h->rp, h->pos, d_err);
         }
         DevState init;
         memset(&init, 0, sizeof init);
@@ -686,8 +701,16 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
             rc = set_err(GR_CUDA_ERROR, cudaGetErrorString(e));
             break;
         }
+        if (hdr[0] & 4u) {
+            rc = set_err(GR_INVALID_ARGUMENT, "non-finite start position");
+            break;
+        }
         if (hdr[0] & 2u) {
             rc = set_err(GR_INVALID_ARGUMENT, "edge weights must be finite and > 0 when edge_weight_influence != 0");
+            break;
+        }
+        if (hdr[1]) {
+            rc = set_err(GR_DEVICE_FAULT, "the edge sort gave up a bounded wait");
             break;
         }
         if (int c = build_segments(h)) {
@@ -834,17 +857,23 @@ int gr_fa2_positions(gr_fa2 *h, float *out) {
     if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
     if (!out) return set_err(GR_INVALID_ARGUMENT, "out is null");
     if (h->n == 0) return ok();
+    // the copy flags a non-finite coordinate on the device (one word back, not a
+    // host pass over every coordinate)
+    const size_t count = (size_t)h->n * h->dim;
     float *d = nullptr;
-    CU(cudaMallocAsync((void **)&d, (size_t)h->n * h->dim * 4, h->stream));
+    CU(cudaMallocAsync((void **)&d, count * 4 + 4, h->stream));
+    uint32_t *flag = (uint32_t *)(d + count);
+    cudaMemsetAsync(flag, 0, 4, h->stream);
     if (h->dim == 3)
-        k_export<3><<<div_up(h->n, 256), 256, 0, h->stream>>>(h->n, h->pos, d);
+        k_export<3><<<div_up(h->n, 256), 256, 0, h->stream>>>(h->n, h->pos, d, flag);
     else
-        k_export<2><<<div_up(h->n, 256), 256, 0, h->stream>>>(h->n, h->pos, d);
-    cudaMemcpyAsync(out, d, (size_t)h->n * h->dim * 4, cudaMemcpyDeviceToHost, h->stream);
+        k_export<2><<<div_up(h->n, 256), 256, 0, h->stream>>>(h->n, h->pos, d, flag);
+    uint32_t bad = 0;
+    cudaMemcpyAsync(out, d, count * 4, cudaMemcpyDeviceToHost, h->stream);
+    cudaMemcpyAsync(&bad, flag, 4, cudaMemcpyDeviceToHost, h->stream);
     cudaFreeAsync(d, h->stream);
     CU(cudaStreamSynchronize(h->stream));
-    for (size_t i = 0; i < (size_t)h->n * h->dim; i++)
-        if (!std::isfinite(out[i])) return set_err(GR_LAYOUT_FAILED, "non-finite position (StageError::NonFinite)");
+    if (bad) return set_err(GR_LAYOUT_FAILED, "non-finite position (StageError::NonFinite)");
     return ok();
 }
 

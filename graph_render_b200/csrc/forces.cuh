@@ -279,15 +279,18 @@ k_update(uint32_t n, DevState *st, float4 *__restrict__ pos, const float *__rest
     }
 }
 
-// Row-major n x D copy of the float4 positions (the per-tick buffer).
+// Row-major n x D copy of the float4 positions (the per-tick buffer); with
+// nonfinite, a non-finite coordinate sets it to 1.
 template <int D>
-__global__ void k_export(uint32_t n, const float4 *__restrict__ pos, float *__restrict__ out) {
+__global__ void k_export(uint32_t n, const float4 *__restrict__ pos, float *__restrict__ out,
+                         uint32_t *nonfinite = nullptr) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4 p = pos[i];
     out[(size_t)i * D] = p.x;
     out[(size_t)i * D + 1] = p.y;
     if (D == 3) out[(size_t)i * D + 2] = p.z;
+    if (nonfinite && !(isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z)))) *nonfinite = 1u;
 }
 
 template <int D>

@@ -207,7 +207,7 @@ __global__ void rs_fix_runs(uint64_t *__restrict__ keys, uint32_t *__restrict__ 
 // consecutive threads on consecutive addresses of each digit's run.
 
 constexpr int OS_HIST_THREADS = 256;
-constexpr int OS_MAX_PASSES = 4;
+constexpr int OS_MAX_PASSES = 8;
 constexpr uint32_t OS_FLAG_A = 1u << 30, OS_FLAG_P = 2u << 30, OS_COUNT = (1u << 30) - 1u;
 constexpr uint32_t OS_SPIN_LIMIT = 1u << 22;  // x 32 ns sleeps: ~0.1 s
 
@@ -490,6 +490,19 @@ struct RadixSorter {
             std::swap(ka, kb);
             std::swap(va, vb);
         }
+    }
+
+    // Sorts keys[0..n) (low `bits` bits significant) with their values, in
+    // place: one-sweep passes when they fit (n < 2^30, at most OS_MAX_PASSES
+    // digits), else the upsweep / scan / downsweep passes. A one-sweep wait that
+    // gives up sets ERR_WAIT in *err.
+    void sort_bits(uint64_t *keys, uint32_t *vals, uint32_t n, int bits, cudaStream_t s, uint32_t *err) {
+        int passes = (bits + 7) / 8;
+        passes += passes & 1;
+        if (n < (1u << 30) && passes <= OS_MAX_PASSES)
+            sort_onesweep(keys, vals, n, 0, passes, s, err);
+        else
+            sort(keys, vals, n, bits, s);
     }
 
     // Sorts keys[0..n) (low `bits` bits significant, a multiple of 16) with
