@@ -84,6 +84,7 @@ __host__ __device__ inline size_t slot_carve(unsigned char *base, uint32_t nmax,
     v.bt.rec = nullptr;
     v.bt.levels = nullptr;
     v.bt.cell_flag = nullptr;
+    v.bt.marks = nullptr;
     v.leaf_body = slot_take<Body>(base, off, n);
     v.int_body = slot_take<Body>(base, off, n);
     v.leaf_coinc = slot_take<uint8_t>(base, off, n);

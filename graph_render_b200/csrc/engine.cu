@@ -152,7 +152,7 @@ struct gr_fa2 {
     double *pre_local = nullptr;         // (n + 1) x (D + 1): the in-tile part of every leaf's prefix
     Body *tile_sum = nullptr;            // per tile of AG_TILE sorted points: FP64 term sums
     BodyDD *tile_carry = nullptr;        // and their exclusive double-double prefix
-    uint32_t *tile_cnt = nullptr;        // leaf counts per tile, then their exclusive prefix
+    uint32_t *tile_cnt = nullptr;        // leaves starting in each tile, then (large graphs) their exclusive prefix
     uint8_t *leaf_coinc = nullptr;
     Cells cells{};
     float *rep = nullptr, *U = nullptr;
@@ -176,6 +176,9 @@ struct gr_fa2 {
     cudaStream_t aux = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     bool branch = false;  // set while a whole tick is captured
+    // every edge weight is 1 (no weights given, or edge-weight influence 0): the
+    // tick's attraction reads no weights (wt still holds them for the adjoint)
+    bool unit_w = false;
     void *flush = nullptr;
     size_t flush_bytes = 0;
 
@@ -286,21 +289,77 @@ __global__ void __launch_bounds__(256) k_fix_long_runs(uint64_t *__restrict__ ke
     }
 }
 
-// Sort on the high 32 key bits (4 passes, stable), then put every run of equal
-// high words in full-key order: runs of up to 64 in place by one thread, longer
-// ones by one CTA each. The order is exactly the full stable 64-bit sort's.
-static void sort_fast(gr_fa2 *h, cudaStream_t s) {
+// Morton keys of every node (k_keys' work) fused with the one-sweep digit
+// histograms of the keys' high 32 bits (os_hist's work for 4 digits from digit
+// 4) and the zeroing of those passes' look-back words. ghist (digit counts and
+// tile counters) was zeroed by the bounds pass. Grid-stride over the nodes in
+// order, 4 positions in flight per thread; counts are integers, so the
+// histogram does not depend on the order the atomics land in.
+template <int D>
+__global__ void __launch_bounds__(OS_HIST_THREADS)
+k_keys_hist(const float4 *__restrict__ pos, uint32_t n, const DevState *st, uint64_t *__restrict__ keys,
+            uint32_t *__restrict__ vals, uint32_t *__restrict__ ghist, uint32_t *__restrict__ status,
+            uint64_t status_words) {
+    static_assert(OS_HIST_THREADS == RS_BINS, "one thread per digit");
+    constexpr int PASSES = 4, FIRST = 4, U = 4;
+    if (st->converged) return;
+    __shared__ uint32_t s_h[PASSES][RS_BINS];
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int p = 0; p < PASSES; p++) s_h[p][t] = 0;
+    __syncthreads();
+    const double r0[3] = {st->root0[0], st->root0[1], D == 3 ? st->root0[2] : 0.0};
+    const double rw = st->root_w;
+    const uint64_t stride = (uint64_t)gridDim.x * OS_HIST_THREADS;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * OS_HIST_THREADS + t; i0 < n; i0 += U * stride) {
+        float4 pv[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t i = i0 + u * stride;
+            pv[u] = i < n ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t i = i0 + u * stride;
+            if (i < n) {
+                const uint64_t key = morton_key<D>(pv[u], r0, rw);
+                keys[i] = key;
+                vals[i] = (uint32_t)i;
+#pragma unroll
+                for (int p = 0; p < PASSES; p++) atomicAdd(&s_h[p][(uint32_t)(key >> (8 * (FIRST + p))) & 0xffu], 1u);
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < PASSES; p++)
+        if (s_h[p][t]) atomicAdd(&ghist[p * RS_BINS + t], s_h[p][t]);
+    for (uint64_t i = (uint64_t)blockIdx.x * OS_HIST_THREADS + t; i < status_words; i += stride) status[i] = 0u;
+}
+
+// Keys, then a sort on the high 32 key bits (4 passes, stable), then every run
+// of equal high words put in full-key order: runs of up to 64 in place by one
+// thread, longer ones by one CTA each. The order is exactly the full stable
+// 64-bit sort's. The bounds pass zeroed os_ghist and too_long.
+template <int D>
+static void keys_sort_fast(gr_fa2 *h, cudaStream_t s) {
     const uint32_t n = h->n;
     const uint32_t *conv = &h->st->converged;
-    cudaMemsetAsync(h->too_long, 0, 4, s);
-    if (n < (1u << 30))
-        h->sorter.sort_onesweep(h->keys, h->vals, n, 4, 4, s, &h->st->error, conv);
-    else
+    if (n < (1u << 30)) {
+        const uint32_t nt = div_up(n, OS_T * OS_I);
+        k_keys_hist<D><<<std::min<uint32_t>(div_up(n, OS_HIST_THREADS * 4), 4 * 148), OS_HIST_THREADS, 0, s>>>(
+            h->pos, n, h->st, h->keys, h->vals, h->sorter.os_ghist, h->sorter.os_status, (uint64_t)4 * nt * RS_BINS);
+        h->sorter.onesweep_passes(h->keys, h->vals, n, 4, 4, s, &h->st->error, conv);
+    } else {
+        k_keys<D><<<div_up(n, 256), 256, 0, s>>>(h->pos, n, h->st, h->keys, h->vals);
         h->sorter.sort_digits(h->keys, h->vals, n, 4, 4, s, conv);
+    }
     rs_fix_runs<<<div_up(n, 256), 256, 0, s>>>(h->keys, h->vals, n, 64, h->too_long, h->long_runs, conv);
     k_fix_long_runs<<<148, 256, 0, s>>>(h->keys, h->vals, h->sorter.k_alt, h->sorter.v_alt, h->too_long,
                                         h->long_runs, conv);
 }
+
+static_assert(SC_TILE == (int)SC_TILE_LEAVES, "k_karras counts level bits per cell-level scan block");
 
 template <int D>
 static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
@@ -315,12 +374,13 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
     auto attraction_seg = [&](cudaStream_t q) {
         if (h->nseg)
             k_attract_seg<D><<<div_up((uint64_t)h->nseg * GR_WARP, FRC_THREADS), FRC_THREADS, 0, q>>>(
-                h->nseg, lin_log, st, h->pos, h->rp, h->col, h->wt, h->seg_row, h->seg_first, h->seg_out);
+                h->nseg, lin_log, st, h->pos, h->rp, h->col, h->unit_w ? nullptr : h->wt, h->seg_row,
+                h->seg_first, h->seg_out);
     };
     auto attraction_rows = [&](cudaStream_t q) {
-        k_attract<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, q>>>(n, lin_log, st, h->pos, h->rp, h->col, h->wt,
-                                                                     h->nseg ? h->seg_first : nullptr, h->seg_out,
-                                                                     h->U);
+        k_attract<D><<<div_up(n, FRC_THREADS), FRC_THREADS, 0, q>>>(
+            n, lin_log, st, h->pos, h->rp, h->col, h->unit_w ? nullptr : h->wt, h->nseg ? h->seg_first : nullptr,
+            h->seg_out, h->U);
     };
     // In a captured whole tick the attraction runs on its own branch beside the
     // walk (which is bound by instruction issue, the attraction by memory
@@ -329,19 +389,33 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
     const bool branch = h->branch && phases == PH_ALL;
     if (h->timing_events) cudaEventRecordWithFlags(h->ev[0], s, cudaEventRecordExternal);
     if (phases & PH_TREE) {
-        k_bounds<D><<<h->bnd_blocks(), BND_THREADS, 0, s>>>(h->pos, n, st, h->part);
+        // counters later kernels of the tree build accumulate into: the fast
+        // sort's digit counts and long-run count, the cell-level scan's marks
+        ZeroWords zw;
+        if (h->long_runs) {
+            zw.add(h->sorter.os_ghist, RadixSorter::ghist_words());
+            zw.add(h->too_long, 1);
+        }
+        const bool fold_scan = h->scanner.folds(n);
+        if (fold_scan) zw.add(h->scanner.bsum, div_up(n, SC_TILE));
+        k_bounds<D><<<h->bnd_blocks(), BND_THREADS, 0, s>>>(h->pos, n, st, h->part, zw);
         const uint32_t ab = div_up(n, AG_TILE);
-        k_keys<D><<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals);
-        if (h->long_runs)
-            sort_fast(h, s);
-        else
+        if (h->long_runs) {
+            keys_sort_fast<D>(h, s);
+        } else {
+            k_keys<D><<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals);
             h->sorter.sort(h->keys, h->vals, n, 64, s, conv);
+        }
         k_leaf_tiles<D><<<ab, AG_T, 0, s>>>(st, n, h->pos, h->keys, h->vals, h->sp, h->sorig, h->tile_sum,
                                              h->tile_cnt);
-        k_leaf_carry<D><<<1, CARRY_T, 0, s>>>(st, n, h->tile_sum, h->tile_cnt, h->tile_carry, h->tile_cnt + ab,
-                                              h->leaf_start, h->pre_local);
-        k_leaf_prefix<D><<<ab, AG_T, 0, s>>>(st, n, h->sp, h->keys, h->tile_cnt + ab, h->uid, h->leaf_start,
-                                              h->ukey, h->levels, h->pre_local);
+        const uint32_t *ccarry = nullptr;  // the carries come from one block above LEAF_FOLD_MAX_TILES tiles
+        if (ab > LEAF_FOLD_MAX_TILES) {
+            k_leaf_carry<D><<<1, CARRY_T, 0, s>>>(st, n, h->tile_sum, h->tile_cnt, h->tile_carry, h->tile_cnt + ab,
+                                                  h->leaf_start, h->pre_local);
+            ccarry = h->tile_cnt + ab;
+        }
+        k_leaf_prefix<D><<<ab, AG_T, 0, s>>>(st, n, h->sp, h->keys, h->tile_sum, h->tile_cnt, h->tile_carry,
+                                              ccarry, h->uid, h->leaf_start, h->ukey, h->levels, h->pre_local);
         const Prefix pre{h->pre_local, h->tile_carry, h->leaf_start, 0u, ab};  // nu: read on the device
         const bool adjoint = h->bt.cell_of != nullptr;  // the adjoint reads leaf and node bodies as arrays
         BinTree bt = h->bt;  // the tick itself reads only the packed records and leaf_parent
@@ -351,10 +425,14 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
             bt.first = bt.last = bt.left = bt.right = bt.visit = nullptr;
             bt.delta = bt.int_parent = nullptr;
         }
+        bt.marks = fold_scan ? h->scanner.bsum : nullptr;
         k_karras<D><<<gn, 256, 0, s>>>(st, h->ukey, bt);
         if (adjoint) k_leaf_body<D><<<gn, 256, 0, s>>>(st, h->sp, h->leaf_start, h->leaf_body, h->leaf_coinc);
         if (adjoint) k_node_body<D><<<gn, 256, 0, s>>>(st, h->bt, pre, h->int_body);
-        h->scanner.scan_levels(h->levels, h->P, n, &st->n_unique, &st->n_cells, s, conv);
+        if (fold_scan)
+            h->scanner.scan_levels_marked(h->levels, h->P, n, &st->n_unique, &st->n_cells, s, conv);
+        else
+            h->scanner.scan_levels(h->levels, h->P, n, &st->n_unique, &st->n_cells, s, conv);
         k_assign_cells<D><<<2 * gn, 256, 0, s>>>(st, bt, gn * 256, h->sp, h->P, h->levels, h->leaf_start,
                                                  pre, h->cells, h->leaf_pre, st);
     }
@@ -651,6 +729,7 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
             break;
         }
         h->m = ms;
+        h->unit_w = weight == nullptr || prm[P_INFLUENCE] == 0.0;
         uint32_t *slo = nullptr, *shi = nullptr;
         float *weff = nullptr;
         h->m_raw = m;

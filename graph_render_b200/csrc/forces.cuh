@@ -49,6 +49,7 @@ __device__ __forceinline__ void attr_term(const float4 &p, const float4 &q, floa
 
 // Heavy rows: warp s sums entries [seg_begin(s), seg_begin(s) + SEG) of row
 // seg_row[s] (lanes stride by 32, then a fixed butterfly), writing D floats.
+// A null wt means every weight is 1.
 template <int D>
 __global__ void __launch_bounds__(FRC_THREADS)
 k_attract_seg(uint32_t nseg, int lin_log, const DevState *st, const float4 *__restrict__ pos,
@@ -64,7 +65,8 @@ k_attract_seg(uint32_t nseg, int lin_log, const DevState *st, const float4 *__re
     const uint32_t e1 = min(e0 + SEG, rp[row + 1]);
     const float4 p = pos[row];
     float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-    for (uint32_t e = e0 + lane; e < e1; e += GR_WARP) attr_term<D>(p, pos[col[e]], wt[e], lin_log, a0, a1, a2);
+    for (uint32_t e = e0 + lane; e < e1; e += GR_WARP)
+        attr_term<D>(p, pos[col[e]], wt ? wt[e] : 1.f, lin_log, a0, a1, a2);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         a0 += __shfl_xor_sync(GR_FULL, a0, o);
@@ -168,6 +170,7 @@ __device__ __forceinline__ double node_update(float4 &p, const float *__restrict
 
 // Attraction of node i over its own CSR row (rows of <= LIGHT_MAX entries), or
 // its segment sums in segment order (longer rows, when seg_first is given).
+// A null wt means every weight is 1 (the same terms, without the weight reads).
 template <int D>
 __device__ __forceinline__ void node_attraction(uint32_t i, const float4 &p, int lin_log,
                                                 const float4 *__restrict__ pos, const uint32_t *__restrict__ rp,
@@ -177,7 +180,7 @@ __device__ __forceinline__ void node_attraction(uint32_t i, const float4 &p, int
     a0 = a1 = a2 = 0.f;
     const uint32_t e0 = rp[i], e1 = rp[i + 1];
     if (seg_first == nullptr || e1 - e0 <= LIGHT_MAX) {
-        for (uint32_t e = e0; e < e1; e++) attr_term<D>(p, pos[col[e]], wt[e], lin_log, a0, a1, a2);
+        for (uint32_t e = e0; e < e1; e++) attr_term<D>(p, pos[col[e]], wt ? wt[e] : 1.f, lin_log, a0, a1, a2);
     } else {  // the row's segment sums, in segment order
         const uint32_t s0 = seg_first[i], ns = (e1 - e0 + SEG - 1) / SEG;
         for (uint32_t s = s0; s < s0 + ns; s++) {

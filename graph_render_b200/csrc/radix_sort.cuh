@@ -473,14 +473,28 @@ struct RadixSorter {
                        uint32_t *err, const uint32_t *skip = nullptr) {
         if (n == 0) return;
         const uint32_t nt = div_up(n, OS_T * OS_I);
+        cudaMemsetAsync(os_ghist, 0, ghist_words() * sizeof(uint32_t), s);
+        const uint64_t words = (uint64_t)passes * nt * RS_BINS;
+        os_hist<<<std::min<uint32_t>(div_up(n, OS_HIST_THREADS * 4), 4 * 148), OS_HIST_THREADS, 0, s>>>(
+            keys, n, first_digit, passes, os_ghist, os_status, words, skip);
+        onesweep_passes(keys, vals, n, first_digit, passes, s, err, skip);
+    }
+
+    // Words of os_ghist (digit counts, then the passes' tile counters) that
+    // must be zero before a histogram pass.
+    static constexpr uint32_t ghist_words() { return (uint32_t)OS_MAX_PASSES * (RS_BINS + 1); }
+
+    // The one-sweep passes alone, for a caller whose own kernel already filled
+    // os_ghist (zeroed first) with the digit counts and zeroed the look-back
+    // words (os_hist's work).
+    void onesweep_passes(uint64_t *keys, uint32_t *vals, uint32_t n, int first_digit, int passes, cudaStream_t s,
+                         uint32_t *err, const uint32_t *skip = nullptr) {
+        if (n == 0) return;
+        const uint32_t nt = div_up(n, OS_T * OS_I);
         constexpr size_t smem = os_smem<uint32_t, OS_T, OS_I>();
         if (smem > 48 * 1024)
             cudaFuncSetAttribute(os_pass<uint32_t, OS_T, OS_I, OS_L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
-        cudaMemsetAsync(os_ghist, 0, (size_t)OS_MAX_PASSES * (RS_BINS + 1) * sizeof(uint32_t), s);
-        const uint64_t words = (uint64_t)passes * nt * RS_BINS;
-        os_hist<<<std::min<uint32_t>(div_up(n, OS_HIST_THREADS * 4), 4 * 148), OS_HIST_THREADS, 0, s>>>(
-            keys, n, first_digit, passes, os_ghist, os_status, words, skip);
         uint64_t *ka = keys, *kb = k_alt;
         uint32_t *va = vals, *vb = v_alt;
         for (int p = 0; p < passes; p++) {

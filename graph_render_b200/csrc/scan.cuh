@@ -123,6 +123,66 @@ sc_down(const uint32_t *__restrict__ in, uint32_t *__restrict__ out, uint32_t n_
     }
 }
 
+// Up to this many blocks the cell-level scan runs as one pass (sc_levels_fold).
+constexpr uint32_t SC_FOLD_MAX_BLOCKS = 2048;
+
+// Exclusive scan of 1 + popc(levels[s]) over s < *n_dev in one pass, for at
+// most SC_FOLD_MAX_BLOCKS blocks: marks[b], counted by the kernel that set the
+// level bits, is the number of bits set in block b's leaves, so the sum of
+// block b is its leaf count plus marks[b], and every block folds the sums of the
+// blocks before its own (integers: the same value in any order). The block
+// holding the last leaf writes the grand total.
+__global__ void __launch_bounds__(SC_THREADS)
+sc_levels_fold(const uint32_t *__restrict__ levels, uint32_t *__restrict__ out, const uint32_t *n_dev,
+               const uint32_t *__restrict__ marks, uint32_t *total, const uint32_t *skip) {
+    if (skip && *skip) return;
+    const uint32_t n = *n_dev;
+    const uint32_t b = blockIdx.x;
+    const uint64_t base = (uint64_t)b * SC_TILE;
+    if (base >= n) return;
+    __shared__ uint32_t s_w[SC_THREADS / GR_WARP];
+    __shared__ uint32_t s_pre;
+    const int t = threadIdx.x, lane = t % GR_WARP, w = t / GR_WARP;
+    uint32_t pm = 0;  // level bits set in the blocks before this one
+    for (uint32_t j = t; j < b; j += SC_THREADS) pm += marks[j];
+    pm = __reduce_add_sync(GR_FULL, pm);
+    if (lane == 0) s_w[w] = pm;
+    __syncthreads();
+    if (t == 0) {
+        uint32_t a = (uint32_t)base;  // one cell per leaf before this block
+        for (int k = 0; k < SC_THREADS / GR_WARP; k++) a += s_w[k];
+        s_pre = a;
+    }
+    __syncthreads();
+    // blocked arrangement: thread t owns items [t*ITEMS, t*ITEMS+ITEMS)
+    uint32_t x[SC_ITEMS];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int r = 0; r < SC_ITEMS; r++) {
+        const uint64_t i = base + (uint64_t)t * SC_ITEMS + r;
+        x[r] = i < n ? scan_item<true>(levels[i]) : 0u;
+        sum += x[r];
+    }
+    uint32_t sc = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(GR_FULL, sc, o);
+        if (lane >= o) sc += y;
+    }
+    if (lane == 31) s_w[w] = sc;
+    __syncthreads();
+    uint32_t wb = 0;
+    for (int k = 0; k < w; k++) wb += s_w[k];
+    uint32_t run = s_pre + wb + sc - sum;
+#pragma unroll
+    for (int r = 0; r < SC_ITEMS; r++) {
+        const uint64_t i = base + (uint64_t)t * SC_ITEMS + r;
+        if (i < n) out[i] = run;
+        run += x[r];
+    }
+    if (t == SC_THREADS - 1 && (uint64_t)n <= base + SC_TILE) *total = run;
+}
+
 // Exclusive scan of in[0..n) into out[0..n) (in == out allowed); out[n] is not
 // written, the total goes to *total. n = n_host, or *n_dev + n_add when n_dev
 // is given (n_host is then the launch bound).
@@ -165,6 +225,15 @@ struct Scanner {
     void scan_levels(const uint32_t *levels, uint32_t *out, uint32_t n_host, const uint32_t *n_dev,
                      uint32_t *total, cudaStream_t s, const uint32_t *skip = nullptr) {
         run<true>(levels, out, n_host, n_dev, 0, total, nullptr, s, skip);
+    }
+    // The same scan in one pass when the block sums were counted beforehand
+    // into bsum (marks; zeroed before they were counted): up to
+    // SC_FOLD_MAX_BLOCKS blocks, n_dev given.
+    bool folds(uint32_t n_host) const { return div_up(n_host, SC_TILE) <= SC_FOLD_MAX_BLOCKS; }
+    void scan_levels_marked(const uint32_t *levels, uint32_t *out, uint32_t n_host, const uint32_t *n_dev,
+                            uint32_t *total, cudaStream_t s, const uint32_t *skip = nullptr) {
+        if (n_host == 0) return;
+        sc_levels_fold<<<div_up(n_host, SC_TILE), SC_THREADS, 0, s>>>(levels, out, n_dev, bsum, total, skip);
     }
 };
 

@@ -26,6 +26,10 @@
 
 namespace gr {
 
+// Leaves per block of the cell-level scan (scan.cuh's SC_TILE); k_karras
+// counts the level bits it sets per block of this many leaves.
+constexpr uint32_t SC_TILE_LEAVES = 2048;
+
 template <int D> struct Levels;
 template <> struct Levels<2> { static constexpr int L = 32; };  // 64-bit keys
 template <> struct Levels<3> { static constexpr int L = 21; };  // 63-bit keys
@@ -94,13 +98,34 @@ __device__ __forceinline__ uint64_t morton_key(const float4 &p, const double *ro
 
 constexpr int BND_THREADS = 256;
 
+// Counters a later kernel of the tick accumulates into (nullable), zeroed by
+// block 0 of the bounds pass so that no memset node precedes them.
+struct ZeroWords {
+    uint32_t *p[3] = {nullptr, nullptr, nullptr};
+    uint32_t len[3] = {0, 0, 0};
+    void add(uint32_t *q, uint32_t words) {
+        for (int j = 0; j < 3; j++)
+            if (!p[j]) {
+                p[j] = q;
+                len[j] = words;
+                return;
+            }
+    }
+    __device__ __forceinline__ void clear() const {
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            for (uint32_t i = threadIdx.x; i < len[j]; i += blockDim.x) p[j][i] = 0u;
+    }
+};
+
 // Extent and FP64 coordinate sums of the positions; the last block turns them
 // into the root square (quadtree.rs:157-195 cover, both corners) and the mean
 // gravity pulls toward (state.rs:208-218).
 template <int D>
 __global__ void __launch_bounds__(BND_THREADS)
-k_bounds(const float4 *__restrict__ pos, uint32_t n, DevState *st, double *__restrict__ part) {
+k_bounds(const float4 *__restrict__ pos, uint32_t n, DevState *st, double *__restrict__ part, ZeroWords zw) {
     if (st->converged) return;
+    if (blockIdx.x == 0) zw.clear();
     __shared__ double s_red[32];
     __shared__ float s_f[2 * D][32];
     __shared__ bool s_last;
@@ -251,6 +276,7 @@ struct BinTree {
     int4 *rec;            // internal node -> {first, last, parent, delta} in one load (nullable)
     uint32_t *levels;     // unique leaf s -> bit l set when a cell of level l begins at s (nullable)
     uint8_t *cell_flag;   // internal node -> 1 when it is a cell (written with levels)
+    uint32_t *marks;      // nullable: per SC_TILE-leaf block, the count of level bits set in it (zeroed before)
 };
 
 // What karras_node found for internal node i: its leaf range, split and
@@ -332,24 +358,53 @@ __device__ __forceinline__ KarrasNode karras_node(int32_t i, int32_t nu, const u
 // 1 + popc(levels[s]) cells and the level-l one is the popc(levels[s] & (2^l -
 // 1))-th of them in preorder. A level is at most 31 (2D, 64-bit keys) or 20
 // (3D, 63-bit keys).
+// Adds 1 at marks[tgt] for every lane with `has`, with one atomic per warp when
+// all those lanes name the same counter (the common case: a warp's nodes are
+// 32 consecutive split positions). The whole warp calls it.
+__device__ __forceinline__ void count_marks(bool has, uint32_t tgt, uint32_t *__restrict__ marks) {
+    const uint32_t act = __ballot_sync(GR_FULL, has);
+    if (act == 0u) return;
+    const int leader = __ffs(act) - 1;
+    const uint32_t t0 = __shfl_sync(GR_FULL, tgt, leader);
+    if (__all_sync(GR_FULL, !has || tgt == t0)) {
+        if ((int)(threadIdx.x % GR_WARP) == leader) atomicAdd(&marks[t0], (uint32_t)__popc(act));
+    } else if (has) {
+        atomicAdd(&marks[tgt], 1u);
+    }
+}
+
+// With marks, each bit set also counts once in marks[leaf / mark_tile] (the
+// block sums of the cell-level scan, so that scan needs no reduce pass). The
+// whole warp calls it; lanes without a node (valid false) only vote.
 template <int D>
-__device__ __forceinline__ void mark_cells(int32_t i, int32_t nu, const uint64_t *__restrict__ k,
+__device__ __forceinline__ void mark_cells(bool valid, int32_t i, int32_t nu, const uint64_t *__restrict__ k,
                                            const KarrasNode &q, uint32_t *__restrict__ levels,
-                                           uint8_t *__restrict__ cell_flag) {
-    const int lv = q.delta / D;
-    if (i == 0) {
-        atomicOr(&levels[0], 1u << lv);
-        cell_flag[0] = 1;
+                                           uint8_t *__restrict__ cell_flag, uint32_t *__restrict__ marks,
+                                           uint32_t mark_tile) {
+    bool ml = false, mr = false;
+    if (valid) {
+        const int lv = q.delta / D;
+        if (i == 0) {
+            atomicOr(&levels[0], 1u << lv);
+            if (marks) atomicAdd(&marks[0], 1u);
+            cell_flag[0] = 1;
+        }
+        if (q.first != q.gamma) {  // left child [first, gamma], internal node gamma
+            const int c = kdelta(k, q.first, q.gamma, nu) / D;
+            ml = c != lv;
+            if (ml) atomicOr(&levels[q.first], 1u << c);
+            cell_flag[q.gamma] = ml ? 1 : 0;
+        }
+        if (q.last != q.gamma + 1) {  // right child [gamma + 1, last], internal node gamma + 1
+            const int c = kdelta(k, q.gamma + 1, q.last, nu) / D;
+            mr = c != lv;
+            if (mr) atomicOr(&levels[q.gamma + 1], 1u << c);
+            cell_flag[q.gamma + 1] = mr ? 1 : 0;
+        }
     }
-    if (q.first != q.gamma) {  // left child [first, gamma], internal node gamma
-        const int c = kdelta(k, q.first, q.gamma, nu) / D;
-        if (c != lv) atomicOr(&levels[q.first], 1u << c);
-        cell_flag[q.gamma] = c != lv ? 1 : 0;
-    }
-    if (q.last != q.gamma + 1) {  // right child [gamma + 1, last], internal node gamma + 1
-        const int c = kdelta(k, q.gamma + 1, q.last, nu) / D;
-        if (c != lv) atomicOr(&levels[q.gamma + 1], 1u << c);
-        cell_flag[q.gamma + 1] = c != lv ? 1 : 0;
+    if (marks) {
+        count_marks(ml, valid ? (uint32_t)q.first / mark_tile : 0u, marks);
+        count_marks(mr, valid ? (uint32_t)(q.gamma + 1) / mark_tile : 0u, marks);
     }
 }
 
@@ -359,9 +414,11 @@ __global__ void k_karras(const DevState *st, const uint64_t *__restrict__ k, Bin
     const int32_t nu = (int32_t)st->n_unique;
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0 && nu == 1) t.leaf_parent[0] = -1;
-    if (i >= nu - 1) return;
-    const KarrasNode q = karras_node(i, nu, k, t);
-    if (t.levels) mark_cells<D>(i, nu, k, q, t.levels, t.cell_flag);
+    const bool valid = i < nu - 1;
+    if (__all_sync(GR_FULL, !valid)) return;  // whole warps only: mark_cells votes across the warp
+    KarrasNode q{0, 0, 0, 0};
+    if (valid) q = karras_node(i, nu, k, t);
+    if (t.levels) mark_cells<D>(valid, i, nu, k, q, t.levels, t.cell_flag, t.marks, SC_TILE_LEAVES);
 }
 
 // Leaf s's FP64 sums, then the bottom-up pass: the second thread to reach a
@@ -639,7 +696,7 @@ __device__ __forceinline__ Body point_chunk(uint32_t n, uint32_t p0, const float
     return acc;
 }
 
-// (1 of 3) Tile b of AG_TILE sorted points: the sorted point records sp[p] =
+// (1 of 2) Tile b of AG_TILE sorted points: the sorted point records sp[p] =
 // pos[perm[p]], sorig[p] = perm[p]; the tile's FP64 term sums and its count of
 // leaves (points that start a key), as block_scan_body totals them.
 template <int D>
@@ -682,9 +739,84 @@ k_leaf_tiles(DevState *st, uint32_t n, const float4 *__restrict__ pos, const uin
     }
 }
 
+__device__ __forceinline__ DD dd_shfl_down(DD v, int o) {
+    return DD{__shfl_down_sync(GR_FULL, v.hi, o), __shfl_down_sync(GR_FULL, v.lo, o)};
+}
+
+template <int D>
+__device__ __forceinline__ BodyDD bdd_shfl_down(const BodyDD &v, int o) {
+    return BodyDD{dd_shfl_down(v.m, o), dd_shfl_down(v.c0, o), dd_shfl_down(v.c1, o),
+                  D == 3 ? dd_shfl_down(v.c2, o) : DD{0.0, 0.0}};
+}
+
+// Up to this many tiles each leaf-prefix block folds the tile sums before its
+// own (at most 2,047 x 36 B of L2 reads a block); above it one block computes
+// every carry (k_leaf_carry).
+constexpr uint32_t LEAF_FOLD_MAX_TILES = 2048;
+
+// The double-double sum of the tile sums before tile b and the count of the
+// leaves they start, folded by the calling block (AG_T threads) in a fixed
+// shape: thread t adds tiles t, t + AG_T, ... < b in turn, the lanes of a warp
+// combine by a shuffle-down tree into lane 0, and one thread adds the warp
+// totals in warp order. s_bw / s_bc hold AG_W + 1 entries.
+template <int D>
+__device__ __forceinline__ void tiles_before(uint32_t b, const Body *__restrict__ tile_sum,
+                                             const uint32_t *__restrict__ tile_cnt, BodyDD &carry, uint32_t &count,
+                                             BodyDD *s_bw, uint32_t *s_bc) {
+    constexpr int U = 2;  // tile sums in flight per thread
+    BodyDD acc{};
+    uint32_t c = 0;
+    for (uint32_t j0 = threadIdx.x; j0 < b; j0 += U * AG_T) {
+        Body v[U];
+        uint32_t k[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint32_t j = j0 + u * AG_T;
+            v[u] = j < b ? tile_sum[j] : Body{0.0, 0.0, 0.0, 0.0};
+            k[u] = j < b ? tile_cnt[j] : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (j0 + u * AG_T < b) {
+                acc = bdd_add_body<D>(acc, v[u]);
+                c += k[u];
+            }
+    }
+    const int lane = threadIdx.x % GR_WARP, w = threadIdx.x / GR_WARP;
+#pragma unroll
+    for (int o = GR_WARP / 2; o >= 1; o >>= 1) {
+        const BodyDD u = bdd_shfl_down<D>(acc, o);
+        const uint32_t cu = __shfl_down_sync(GR_FULL, c, o);
+        if (lane < o) {
+            acc = bdd_add<D>(acc, u);
+            c += cu;
+        }
+    }
+    if (lane == 0) {
+        s_bw[w] = acc;
+        s_bc[w] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        BodyDD t = s_bw[0];
+        uint32_t tc = s_bc[0];
+        for (int q = 1; q < AG_W; q++) {
+            t = bdd_add<D>(t, s_bw[q]);
+            tc += s_bc[q];
+        }
+        s_bw[AG_W] = t;
+        s_bc[AG_W] = tc;
+    }
+    __syncthreads();
+    carry = s_bw[AG_W];
+    count = s_bc[AG_W];
+}
+
 constexpr int CARRY_T = 1024;  // a multiple of 32, at most 1024
 
-// (2 of 3) One block: the exclusive double-double prefix of the tile sums and
+// One block, for graphs of more than LEAF_FOLD_MAX_TILES tiles (where each
+// block's own fold of the tiles before it, tiles_before, would cost O(tiles^2)
+// reads in all): the exclusive double-double prefix of the tile sums and
 // the exclusive prefix of the tile leaf counts, in a fixed order (thread t
 // folds tiles [t c, t c + c) in turn, then a fixed-shape scan over the
 // threads). Writes n_unique, leaf_start[n_unique] = n, the grand total as
@@ -765,29 +897,53 @@ k_leaf_carry(DevState *st, uint32_t n, const Body *__restrict__ tile_sum, const 
     }
 }
 
-// (3 of 3) Tile b again: every point's leaf index uid[p]; at a leaf's first
-// point leaf_start, ukey, an empty cell level mask and the in-tile part of its
-// prefix (the FP64 in-tile exclusive prefix of the terms).
+// (2 of 2) Tile b again: the double-double carry of the tiles before it (its
+// own fold of their sums, tiles_before, or with ccarry k_leaf_carry's, for
+// more than LEAF_FOLD_MAX_TILES tiles); every point's leaf index uid[p]; at a
+// leaf's first point leaf_start, ukey, an empty cell level mask and the
+// in-tile part of its prefix (the FP64 in-tile exclusive prefix of the terms).
+// The last tile also writes n_unique, leaf_start[n_unique] = n, the grand total
+// as carry[nt] and a zero in-tile part for leaf n_unique.
 template <int D>
 __global__ void __launch_bounds__(AG_T)
-k_leaf_prefix(const DevState *st, uint32_t n, const float4 *__restrict__ sp, const uint64_t *__restrict__ keys,
+k_leaf_prefix(DevState *st, uint32_t n, const float4 *__restrict__ sp, const uint64_t *__restrict__ keys,
+              const Body *__restrict__ tile_sum, const uint32_t *__restrict__ tile_cnt, BodyDD *__restrict__ carry,
               const uint32_t *__restrict__ ccarry, uint32_t *__restrict__ uid, uint32_t *__restrict__ leaf_start,
               uint64_t *__restrict__ ukey, uint32_t *__restrict__ levels, double *__restrict__ pre) {
     if (st->converged) return;
     __shared__ Body s_w[2 * AG_W];
     __shared__ uint32_t s_c[2 * AG_W];
+    __shared__ BodyDD s_bw[AG_W + 1];
+    __shared__ uint32_t s_bc[AG_W + 1];
     const uint32_t b = blockIdx.x;
     const uint32_t p0 = b * AG_TILE + threadIdx.x * AG_I;
     float4 pt[AG_I];
 #pragma unroll
     for (int r = 0; r < AG_I; r++) pt[r] = p0 + r < n ? sp[p0 + r] : make_float4(0.f, 0.f, 0.f, 0.f);
+    BodyDD cb;
+    uint32_t cbefore;
+    if (ccarry) {  // k_leaf_carry wrote the carries, the totals and n_unique
+        cbefore = ccarry[b];
+    } else {
+        tiles_before<D>(b, tile_sum, tile_cnt, cb, cbefore, s_bw, s_bc);
+    }
+    if (!ccarry && threadIdx.x == 0) {
+        carry[b] = cb;
+        if (b + 1 == gridDim.x) {
+            const uint32_t nu = min(cbefore + tile_cnt[b], n);
+            st->n_unique = nu;
+            leaf_start[nu] = n;
+            carry[b + 1] = bdd_add_body<D>(cb, tile_sum[b]);
+            local_put<D>(pre, nu, Body{0.0, 0.0, 0.0, 0.0});
+        }
+    }
     uint64_t k[AG_I];
     uint32_t fl;
     const Body acc = point_chunk<D>(n, p0, pt, keys, k, fl);
     Body ex, total;
     uint32_t exc, tcnt;
     block_scan_body<D>(acc, (uint32_t)__popc(fl), ex, exc, total, tcnt, s_w, s_c);
-    uint32_t e = ccarry[b] + exc;  // leaves that start before this thread's first point
+    uint32_t e = cbefore + exc;  // leaves that start before this thread's first point
     Body run = ex;
 #pragma unroll
     for (int r = 0; r < AG_I; r++) {

@@ -93,6 +93,14 @@ def test_large_2d_powerlaw_forces():
     assert abs(info["far_count"] - sc["far"]) <= 1e-3 * sc["far"]
 
 
+def test_large_2d_forces_with_one_block_tile_carries():
+    # past 2,048 tiles of 1,024 sorted points the leaf pass's tile carries come
+    # from one block (k_leaf_carry) instead of each tile's own fold
+    wl = synth.powerlaw_1m(n=2_200_000, dim=2)
+    rel, info, sc = _check(wl.n, wl.src, wl.dst, None, wl.pos0, wl.params)
+    assert abs(info["far_count"] - sc["far"]) <= 1e-3 * sc["far"]
+
+
 def test_run_is_deterministic():
     wl = synth.sbm_1500()
     outs = []
