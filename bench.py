@@ -360,6 +360,7 @@ def run_3d(args, dist: Dist):
 
     wl = workload("powerlaw-3d", 0)
     with Fa2(wl.n, wl.src, wl.dst, wl.weight, params=wl.params, pos0=wl.pos0) as eng:
+        eng.set_interaction_counting(False)
         eng.tick(1)
         chosen, tuned = eng.tune(2)
         eng.tick(3)
@@ -436,11 +437,12 @@ def run_gpu(args, dist: Dist):
     wl = workload(args.workload, args.n)
     dim = int(wl.params.get("dim", 2))
     eng = Fa2(wl.n, wl.src, wl.dst, wl.weight, params=wl.params, pos0=wl.pos0)
+    eng.set_interaction_counting(False)  # the walk without its diagnostic counters
     eng.tick(1)
     schedule, schedule_ms = eng.tune(3)  # walk schedule autotuner (state restored)
     eng.tick(max(args.warmup, 3))
     torch.cuda.synchronize()
-    info0 = eng.info()
+    start_pos, start_ctl = eng.positions(), eng.controller()
     uuid = str(torch.cuda.get_device_properties(dev).uuid)
     sampler = ClockSampler(uuid if uuid.startswith("GPU-") else f"GPU-{uuid}")
     sampler.start()
@@ -451,7 +453,7 @@ def run_gpu(args, dist: Dist):
     torch.cuda.synchronize()
     dist.barrier()
     clocks = sampler.stop()
-    info1 = eng.info()
+    end_pos = eng.positions()
     done = len(ms)
     total_ms = float(ms[:, 3].sum())
     max_ms = dist.max(total_ms)
@@ -459,13 +461,23 @@ def run_gpu(args, dist: Dist):
     walk_ms = float(ms[:, 1].mean())
     tree_ms = float(ms[:, 0].mean())
     fin_ms = float(ms[:, 2].mean())
+    eng.close()
+    # The timed ticks' interactions (the FLOP count): the same ticks from the same
+    # state (positions and controller) on a second handle whose walk counts them.
+    # Ticks are bit-reproducible, so its end positions equal the timed run's.
+    with Fa2(wl.n, wl.src, wl.dst, wl.weight, params=wl.params, pos0=wl.pos0) as cnt:
+        cnt.set_positions(start_pos)
+        cnt.set_controller(**start_ctl)
+        info0 = cnt.info()
+        cnt.tick(done)
+        info1 = cnt.info()
+        replay_identical = bool(np.array_equal(cnt.positions(), end_pos))
     far = (info1["far_count"] - info0["far_count"]) / max(done, 1)
     pair = (info1["pair_count"] - info0["pair_count"]) / max(done, 1)
     flops = (far + pair) * FLOPS_PER_INTERACTION[dim]
     sm_max = clocks.get("sm_max_mhz") or 1965.0
     fp32_peak = 148 * 128 * 2 * sm_max * 1e6
     achieved = flops / (walk_ms / 1e3)
-    eng.close()
 
     # e2e: the public one-shot path from pinned host buffers, create -> ticks -> positions
     e2e = None
@@ -482,6 +494,7 @@ def run_gpu(args, dist: Dist):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         with F(wl.n, src, dst, w, params=prm, pos0=pos0) as e:
+            e.set_interaction_counting(False)
             ran = e.run()
             out = e.positions()
         el = time.perf_counter() - t0
@@ -561,6 +574,9 @@ def run_gpu(args, dist: Dist):
                          "peak_source": "nominal FP32 FMA rate, 148 SM x 128 lanes x 2 x sm_max_mhz "
                                         "(MEASURED_PEAKS.json has no non-tensor FP32 figure)",
                          "interactions_per_tick": {"far": far, "pair": pair},
+                         "interactions_from": "the timed ticks replayed from their start state on a second handle "
+                                              "whose walk counts them (the timed walk keeps no counters)",
+                         "replay_identical": replay_identical,
                          "flops_per_interaction": FLOPS_PER_INTERACTION[dim]},
             "cpu_baseline": cpu,
             "batched": batched,

@@ -165,6 +165,7 @@ struct gr_fa2 {
     cudaGraphExec_t exec = nullptr;
     uint32_t graph_kernels = 0;
     int walk_schedule = 1;  // 0: warp-cooperative union walk, 1: per-lane walk, 2: two nodes per lane
+    bool count_interactions = true;  // the walk adds its far / pair interaction counts to the state
     // the same tick with event records at its phase boundaries (tick start,
     // tree built, walk done, tick end), for per-phase timing
     cudaGraph_t tgraph = nullptr;
@@ -361,6 +362,22 @@ static void keys_sort_fast(gr_fa2 *h, cudaStream_t s) {
 
 static_assert(SC_TILE == (int)SC_TILE_LEAVES, "k_karras counts level bits per cell-level scan block");
 
+// The repulsion walk in the handle's schedule, with or without its interaction counts.
+template <int D, bool COUNT>
+static void launch_walk(gr_fa2 *h, const WalkParams &wp, cudaStream_t s) {
+    const uint32_t n = h->n;
+    DevState *st = h->st;
+    if (h->walk_schedule == 2)
+        k_walk_s<D, 2, COUNT><<<div_up(div_up(n, 2), WALK_THREADS), WALK_THREADS, 0, s>>>(
+            wp, st, h->cells, h->sp, h->sorig, h->uid, h->leaf_pre, h->rep, st);
+    else if (h->walk_schedule == 1)
+        k_walk_s<D, 1, COUNT><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig,
+                                                                              h->uid, h->leaf_pre, h->rep, st);
+    else
+        k_walk_s<D, 0, COUNT><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig,
+                                                                              h->uid, h->leaf_pre, h->rep, st);
+}
+
 template <int D>
 static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
     const uint32_t n = h->n;
@@ -450,15 +467,10 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
         wp.kr = (float)h->prm[P_SCALING];
         wp.theta2 = (float)(h->prm[P_THETA] * h->prm[P_THETA]);
         wp.seed = (uint32_t)h->prm[P_SEED];
-        if (h->walk_schedule == 2)
-            k_walk_s<D, 2><<<div_up(div_up(n, 2), WALK_THREADS), WALK_THREADS, 0, s>>>(
-                wp, st, h->cells, h->sp, h->sorig, h->uid, h->leaf_pre, h->rep, st);
-        else if (h->walk_schedule == 1)
-            k_walk_s<D, 1><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig, h->uid,
-                                                                           h->leaf_pre, h->rep, st);
+        if (h->count_interactions)
+            launch_walk<D, true>(h, wp, s);
         else
-            k_walk_s<D, 0><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig, h->uid,
-                                                                           h->leaf_pre, h->rep, st);
+            launch_walk<D, false>(h, wp, s);
     }
     if (h->timing_events) cudaEventRecordWithFlags(h->ev[2], s, cudaEventRecordExternal);
     if (phases & PH_FINISH) {
@@ -1038,6 +1050,16 @@ int gr_fa2_set_walk_schedule(gr_fa2 *h, int schedule) {
         return set_err(GR_INVALID_ARGUMENT, "walk schedule must be 0, 1 or 2");
     if (schedule != h->walk_schedule) {
         h->walk_schedule = schedule;
+        h->drop_graphs();
+    }
+    return ok();
+}
+
+int gr_fa2_set_interaction_counting(gr_fa2 *h, int on) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    if (on != 0 && on != 1) return set_err(GR_INVALID_ARGUMENT, "on must be 0 or 1");
+    if ((on == 1) != h->count_interactions) {
+        h->count_interactions = on == 1;
         h->drop_graphs();
     }
     return ok();

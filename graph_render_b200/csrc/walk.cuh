@@ -43,7 +43,7 @@ struct WalkView {
 // The whole warp calls this for the sorted nodes p = base + lane (lanes with
 // p >= n take part in the votes only). Returns each lane's repulsion and its
 // far / pair interaction counts.
-template <int D>
+template <int D, bool COUNT = true>
 __device__ __forceinline__ void walk_group(const WalkView &V, uint32_t p, float &f0, float &f1, float &f2,
                                            uint32_t &nfar, uint32_t &npair) {
     const Cells cells = V.cells;
@@ -97,7 +97,7 @@ __device__ __forceinline__ void walk_group(const WalkView &V, uint32_t p, float 
             f1 += dy * f;
             if (D == 3) f2 += dz * f;
             resume = skip;
-            nfar++;
+            if (COUNT) nfar++;
         }
         const bool open = active && !far;
         if (sk == -1) {
@@ -118,7 +118,7 @@ __device__ __forceinline__ void walk_group(const WalkView &V, uint32_t p, float 
                 f0 += ex * f;
                 f1 += ey * f;
                 if (D == 3) f2 += ez * f;
-                npair++;
+                if (COUNT) npair++;
             }
             k = k + 1;
         } else if (leaf) {
@@ -146,7 +146,7 @@ __device__ __forceinline__ void walk_group(const WalkView &V, uint32_t p, float 
                         f0 += ex * f;
                         f1 += ey * f;
                         if (D == 3) f2 += ez * f;
-                        npair++;
+                        if (COUNT) npair++;
                     }
                 }
             }
@@ -184,8 +184,8 @@ __device__ __forceinline__ void lane_init(const WalkView &V, uint32_t p, LaneNod
 }
 
 // The visit of cell X.k (X.k < ncells): a body term, a leaf's pairs, or a
-// descent; X.k moves on.
-template <int D>
+// descent; X.k moves on. COUNT: keep the far / pair interaction counts.
+template <int D, bool COUNT = true>
 __device__ __forceinline__ void lane_step(const WalkView &V, LaneNode &X) {
     const Cells cells = V.cells;
     const float4 *__restrict__ sp = V.sp;
@@ -210,8 +210,9 @@ __device__ __forceinline__ void lane_step(const WalkView &V, LaneNode &X) {
         start = (uint32_t)Cc.y;
     }
     const bool leaf = sk < 0;
-    uint32_t skip = leaf ? k + 1 : (uint32_t)sk;
-    skip = max(skip, k + 1);  // every step moves forward, whatever a cell holds
+    // a leaf (sk < 0) moves on to k + 1, a cell to its skip; every step moves
+    // forward, whatever a cell holds (k < ncells <= 2^31)
+    const uint32_t skip = (uint32_t)max(sk, (int32_t)k + 1);
     const bool holds = (k <= X.mylp) && (X.mylp < skip);
     const float dx = (me.x - cx) - lx;
     const float dy = (me.y - cy) - ly;
@@ -227,8 +228,10 @@ __device__ __forceinline__ void lane_step(const WalkView &V, LaneNode &X) {
     X.f0 += dx * f;
     X.f1 += dy * f;
     if (D == 3) X.f2 += dz * f;
-    X.nfar += far ? 1u : 0u;
-    X.npair += (body && !far) ? 1u : 0u;
+    if (COUNT) {
+        X.nfar += far ? 1u : 0u;
+        X.npair += (body && !far) ? 1u : 0u;
+    }
     if (!leaf || body) {
         X.k = body ? skip : k + 1;
     } else if (!holds && sk == -1) {  // coincident one-point leaf: the jiggle
@@ -242,7 +245,7 @@ __device__ __forceinline__ void lane_step(const WalkView &V, LaneNode &X) {
         X.f0 += ex * g;
         X.f1 += ey * g;
         if (D == 3) X.f2 += ez * g;
-        X.npair++;
+        if (COUNT) X.npair++;
         X.k = k + 1;
     } else {  // several points (or this node's own leaf): exact pairs
         int32_t cnt = -sk;
@@ -267,18 +270,18 @@ __device__ __forceinline__ void lane_step(const WalkView &V, LaneNode &X) {
             X.f0 += ex * g;
             X.f1 += ey * g;
             if (D == 3) X.f2 += ez * g;
-            X.npair++;
+            if (COUNT) X.npair++;
         }
         X.k = k + 1;
     }
 }
 
-template <int D>
+template <int D, bool COUNT = true>
 __device__ __forceinline__ void walk_lane(const WalkView &V, uint32_t p, float &f0, float &f1, float &f2,
                                           uint32_t &nfar, uint32_t &npair) {
     LaneNode X;
     lane_init<D>(V, p, X);
-    while (X.k < V.ncells) lane_step<D>(V, X);
+    while (X.k < V.ncells) lane_step<D, COUNT>(V, X);
     f0 = X.f0;
     f1 = X.f1;
     f2 = X.f2;
@@ -308,7 +311,7 @@ __device__ __forceinline__ void pair_init(const WalkView &V, uint32_t p, PairNod
     X.nfar = X.npair = 0;
 }
 
-template <int D>
+template <int D, bool COUNT = true>
 __device__ __forceinline__ void pair_visit(const WalkView &V, PairNode &X, uint32_t k, float cx, float cy, float cz,
                                            float lx, float ly, float lz, float cm, float w2, int32_t sk,
                                            uint32_t start, uint32_t skip, bool leaf) {
@@ -325,8 +328,10 @@ __device__ __forceinline__ void pair_visit(const WalkView &V, PairNode &X, uint3
     X.f0 += dx * f;
     X.f1 += dy * f;
     if (D == 3) X.f2 += dz * f;
-    X.nfar += far ? 1u : 0u;
-    X.npair += (body && !far) ? 1u : 0u;
+    if (COUNT) {
+        X.nfar += far ? 1u : 0u;
+        X.npair += (body && !far) ? 1u : 0u;
+    }
     X.resume = body ? skip : k + 1;
     if (!leaf || body) return;
     const float4 *__restrict__ sp = V.sp;
@@ -342,7 +347,7 @@ __device__ __forceinline__ void pair_visit(const WalkView &V, PairNode &X, uint3
         X.f0 += ex * g;
         X.f1 += ey * g;
         if (D == 3) X.f2 += ez * g;
-        X.npair++;
+        if (COUNT) X.npair++;
         return;
     }
     int32_t cnt = -sk;  // several points (or this node's own leaf): exact pairs
@@ -367,7 +372,7 @@ __device__ __forceinline__ void pair_visit(const WalkView &V, PairNode &X, uint3
         X.f0 += ex * g;
         X.f1 += ey * g;
         if (D == 3) X.f2 += ez * g;
-        X.npair++;
+        if (COUNT) X.npair++;
     }
 }
 
@@ -376,7 +381,7 @@ __device__ __forceinline__ void pair_visit(const WalkView &V, PairNode &X, uint3
 // cells of its own walk (k >= its resume), in the same order, so its forces are
 // walk_lane's bit for bit. Adjacent nodes' walks nearly coincide, so the union
 // is little longer than either.
-template <int D>
+template <int D, bool COUNT = true>
 __device__ __forceinline__ void walk_pair(const WalkView &V, PairNode &a, PairNode &b) {
     const Cells cells = V.cells;
     const uint32_t ncells = V.ncells;
@@ -400,17 +405,19 @@ __device__ __forceinline__ void walk_pair(const WalkView &V, PairNode &a, PairNo
             start = (uint32_t)Cc.y;
         }
         const bool leaf = sk < 0;
-        uint32_t skip = leaf ? k + 1 : (uint32_t)sk;
-        skip = max(skip, k + 1);  // every step moves forward, whatever a cell holds
-        pair_visit<D>(V, a, k, cx, cy, cz, lx, ly, lz, cm, w2, sk, start, skip, leaf);
-        pair_visit<D>(V, b, k, cx, cy, cz, lx, ly, lz, cm, w2, sk, start, skip, leaf);
+        // leaves move on to k + 1; every step moves forward, whatever a cell holds
+        const uint32_t skip = (uint32_t)max(sk, (int32_t)k + 1);
+        pair_visit<D, COUNT>(V, a, k, cx, cy, cz, lx, ly, lz, cm, w2, sk, start, skip, leaf);
+        pair_visit<D, COUNT>(V, b, k, cx, cy, cz, lx, ly, lz, cm, w2, sk, start, skip, leaf);
         k = min(a.resume, b.resume);
     }
 }
 
 // Walk schedules: 0 = walk_group (a warp over the union of its 32 nodes),
 // 1 = walk_lane (one node per lane), 2 = walk_pair (two adjacent nodes per lane).
-template <int D, int SCHED>
+// COUNT: add the far / pair interaction counts to the state (a diagnostic; the
+// forces are the same either way).
+template <int D, int SCHED, bool COUNT>
 __global__ void __launch_bounds__(WALK_THREADS)
 k_walk_s(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 *__restrict__ sp,
          const uint32_t *__restrict__ sorig, const uint32_t *__restrict__ uid,
@@ -425,7 +432,7 @@ k_walk_s(WalkParams P, const DevState *__restrict__ st, Cells cells, const float
         PairNode a, b;
         pair_init<D>(V, p, a);
         pair_init<D>(V, p + 1, b);
-        walk_pair<D>(V, a, b);
+        walk_pair<D, COUNT>(V, a, b);
         const PairNode *X[2] = {&a, &b};
 #pragma unroll
         for (int j = 0; j < 2; j++)
@@ -440,9 +447,9 @@ k_walk_s(WalkParams P, const DevState *__restrict__ st, Cells cells, const float
     } else {
         float f0, f1, f2;
         if (SCHED == 1)
-            walk_lane<D>(V, p, f0, f1, f2, nfar, npair);
+            walk_lane<D, COUNT>(V, p, f0, f1, f2, nfar, npair);
         else
-            walk_group<D>(V, p, f0, f1, f2, nfar, npair);
+            walk_group<D, COUNT>(V, p, f0, f1, f2, nfar, npair);
         if (p < P.n) {
             const uint32_t oi = sorig[p];
             rep[(size_t)oi * D + 0] = f0;
@@ -450,6 +457,7 @@ k_walk_s(WalkParams P, const DevState *__restrict__ st, Cells cells, const float
             if (D == 3) rep[(size_t)oi * D + 2] = f2;
         }
     }
+    if (!COUNT) return;
     nfar = __reduce_add_sync(GR_FULL, nfar);
     npair = __reduce_add_sync(GR_FULL, npair);
     if ((threadIdx.x % GR_WARP) == 0) {

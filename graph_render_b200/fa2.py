@@ -156,6 +156,11 @@ class Fa2:
     def set_walk_schedule(self, schedule: int) -> None:
         N.check(self._L.gr_fa2_set_walk_schedule(self.h, int(schedule)))
 
+    def set_interaction_counting(self, on: bool) -> None:
+        """On (the default): the walk counts far / pair interactions into info();
+        off: it keeps no counts (same forces, fewer instructions per cell)."""
+        N.check(self._L.gr_fa2_set_interaction_counting(self.h, 1 if on else 0))
+
     def tune(self, sample_ticks: int = 3):
         """Autotunes the walk schedule; returns (chosen, {schedule: mean walk ms})."""
         chosen = C.c_int()

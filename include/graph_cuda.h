@@ -133,6 +133,12 @@ int gr_fa2_tick_timed(gr_fa2 *h, uint32_t ticks, size_t l2_flush_bytes, float *m
  * floats) gets the mean walk time of each. */
 #define GR_WALK_SCHEDULES 3
 int gr_fa2_set_walk_schedule(gr_fa2 *h, int schedule);
+/* Interaction counting (on = 1, the default): the walk adds every tick's far-cell
+ * and exact-pair interaction counts to gr_fa2_info.far_count / pair_count. With
+ * on = 0 the walk keeps no counts (fewer instructions per visited cell; the
+ * forces are the same bit for bit) and the counters keep their values.
+ * No counterpart in the reference (it counts nothing). */
+int gr_fa2_set_interaction_counting(gr_fa2 *h, int on);
 int gr_fa2_tune(gr_fa2 *h, uint32_t sample_ticks, int *chosen, float *walk_ms_each);
 
 /* Current positions to a host buffer (n x dim), refusing non-finite ones as

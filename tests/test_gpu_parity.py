@@ -161,6 +161,29 @@ def test_walk_schedules_give_bit_identical_forces_and_tuning_keeps_the_state(dim
         assert np.array_equal(outs[0][0], outs[sch][0])
 
 
+@pytest.mark.parametrize("dim", [2, 3])
+def test_walk_without_interaction_counts_gives_the_same_forces_and_run(dim):
+    wl = synth.powerlaw_1m(n=100_000, dim=dim)
+    with Fa2(wl.n, wl.src, wl.dst, params=wl.params, pos0=wl.pos0) as eng:
+        eng.tick(2)
+        ref = eng.forces()
+        far = eng.info()["far_count"]
+        assert far > 0
+        eng.set_interaction_counting(False)
+        for sch in (0, 1, 2):
+            eng.set_walk_schedule(sch)
+            assert np.array_equal(eng.forces(), ref)
+        eng.tick(2)
+        assert eng.info()["far_count"] == far  # no counts while off
+    ends = []
+    for on in (True, False):
+        with Fa2(wl.n, wl.src, wl.dst, params=wl.params, pos0=wl.pos0) as eng:
+            eng.set_interaction_counting(on)
+            eng.tick(5)
+            ends.append(eng.positions())
+    assert np.array_equal(ends[0], ends[1])
+
+
 def _full_sort_forces(n, src, dst, pos, prm):
     """Forces through gr_fa2_forces_static, which sorts the whole 64-bit key
     (8 passes) where a handle sorts the high word and fixes the runs."""
