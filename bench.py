@@ -443,6 +443,7 @@ def run_gpu(args, dist: Dist):
     eng.tick(max(args.warmup, 3))
     torch.cuda.synchronize()
     start_pos, start_ctl = eng.positions(), eng.controller()
+    programmatic = eng.programmatic_launches()
     uuid = str(torch.cuda.get_device_properties(dev).uuid)
     sampler = ClockSampler(uuid if uuid.startswith("GPU-") else f"GPU-{uuid}")
     sampler.start()
@@ -558,6 +559,7 @@ def run_gpu(args, dist: Dist):
                        "l2": f"{FLUSH_BYTES >> 20} MiB buffer overwritten before every timed tick "
                              "(outside the events)",
                        "parallelism": f"{dist.world} independent replicas" if dist.world > 1 else "1 GPU",
+                       "programmatic_launches": programmatic,
                        "phase_ms": {"tree": tree_ms, "walk": walk_ms, "finish": fin_ms},
                        "walk_schedule": {"chosen": WALK_SCHEDULE_NAMES[schedule],
                                          "tuned_walk_ms": {WALK_SCHEDULE_NAMES[i]: schedule_ms[i]

@@ -111,6 +111,7 @@ SIGNATURES = {
     "gr_fa2_batch_stats": ([P, P, P, P], C.c_int),
     "gr_fa2_set_walk_schedule": ([P, C.c_int], C.c_int),
     "gr_fa2_set_interaction_counting": ([P, C.c_int], C.c_int),
+    "gr_fa2_launch_mode": ([P, C.POINTER(C.c_int)], C.c_int),
     "gr_fa2_tune": ([P, C.c_uint32, C.POINTER(C.c_int), P], C.c_int),
     "gr_fa2_get_controller": ([P, P], C.c_int),
     "gr_fa2_set_controller": ([P, P], C.c_int),

@@ -161,6 +161,39 @@ __device__ __forceinline__ bool last_block_done(uint32_t *ticket, bool *smem_fla
     return *smem_flag;
 }
 
+// Programmatic dependent launch (sm_90 and later). A kernel launched with
+// programmatic stream serialization (gr_launch with pdl) may be scheduled while
+// the kernel before it in the stream drains. gr_pdl_enter first lets the next
+// such kernel be scheduled once every block of this grid has started, then
+// waits until the kernel before this one has completed and its writes are
+// visible. Every kernel that calls it does so before any access to global
+// memory, so it sees exactly what plain stream order would give it; in a kernel
+// launched without the attribute both instructions return at once.
+__device__ __forceinline__ void gr_pdl_enter() {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+
+// Launches kernel k on stream s; with pdl, as a programmatic dependent of the
+// kernel before it in the stream (k must call gr_pdl_enter first).
+template <typename... KArgs, typename... Args>
+inline cudaError_t gr_launch(bool pdl, void (*k)(KArgs...), uint32_t grid, uint32_t block, size_t smem,
+                             cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 __host__ __device__ __forceinline__ uint32_t div_up(uint64_t a, uint32_t b) {
     return (uint32_t)((a + b - 1) / b);
 }

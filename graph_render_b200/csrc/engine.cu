@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -166,6 +167,11 @@ struct gr_fa2 {
     uint32_t graph_kernels = 0;
     int walk_schedule = 1;  // 0: warp-cooperative union walk, 1: per-lane walk, 2: two nodes per lane
     bool count_interactions = true;  // the walk adds its far / pair interaction counts to the state
+    // tick kernels launched as programmatic dependents of the kernel before them
+    // (each waits in gr_pdl_enter); off when the environment sets GR_PDL=0, or
+    // after a capture with them failed
+    bool pdl = true;
+    bool pdl_fell_back = false;  // a capture with programmatic launches failed
     // the same tick with event records at its phase boundaries (tick start,
     // tree built, walk done, tick end), for per-phase timing
     cudaGraph_t tgraph = nullptr;
@@ -280,6 +286,7 @@ __global__ void __launch_bounds__(256) k_fix_long_runs(uint64_t *__restrict__ ke
                                                        uint64_t *__restrict__ kalt, uint32_t *__restrict__ valt,
                                                        const uint32_t *long_count, const uint2 *__restrict__ runs,
                                                        const uint32_t *skip) {
+    gr_pdl_enter();
     if (skip && *skip) return;
     __shared__ uint32_t s_cnt[8][256];
     __shared__ uint32_t s_tot[256];
@@ -301,6 +308,7 @@ __global__ void __launch_bounds__(OS_HIST_THREADS)
 k_keys_hist(const float4 *__restrict__ pos, uint32_t n, const DevState *st, uint64_t *__restrict__ keys,
             uint32_t *__restrict__ vals, uint32_t *__restrict__ ghist, uint32_t *__restrict__ status,
             uint64_t status_words) {
+    gr_pdl_enter();
     static_assert(OS_HIST_THREADS == RS_BINS, "one thread per digit");
     constexpr int PASSES = 4, FIRST = 4, U = 4;
     if (st->converged) return;
@@ -348,34 +356,36 @@ static void keys_sort_fast(gr_fa2 *h, cudaStream_t s) {
     const uint32_t *conv = &h->st->converged;
     if (n < (1u << 30)) {
         const uint32_t nt = div_up(n, OS_T * OS_I);
-        k_keys_hist<D><<<std::min<uint32_t>(div_up(n, OS_HIST_THREADS * 4), 4 * 148), OS_HIST_THREADS, 0, s>>>(
-            h->pos, n, h->st, h->keys, h->vals, h->sorter.os_ghist, h->sorter.os_status, (uint64_t)4 * nt * RS_BINS);
-        h->sorter.onesweep_passes(h->keys, h->vals, n, 4, 4, s, &h->st->error, conv);
+        gr_launch(h->pdl, k_keys_hist<D>, std::min<uint32_t>(div_up(n, OS_HIST_THREADS * 4), 4 * 148),
+                  OS_HIST_THREADS, 0, s, h->pos, n, h->st, h->keys, h->vals, h->sorter.os_ghist, h->sorter.os_status,
+                  (uint64_t)4 * nt * RS_BINS);
+        h->sorter.onesweep_passes(h->keys, h->vals, n, 4, 4, s, &h->st->error, conv, h->pdl);
     } else {
         k_keys<D><<<div_up(n, 256), 256, 0, s>>>(h->pos, n, h->st, h->keys, h->vals);
         h->sorter.sort_digits(h->keys, h->vals, n, 4, 4, s, conv);
     }
-    rs_fix_runs<<<div_up(n, 256), 256, 0, s>>>(h->keys, h->vals, n, 64, h->too_long, h->long_runs, conv);
-    k_fix_long_runs<<<148, 256, 0, s>>>(h->keys, h->vals, h->sorter.k_alt, h->sorter.v_alt, h->too_long,
-                                        h->long_runs, conv);
+    gr_launch(h->pdl, rs_fix_runs, div_up(n, 256), 256, 0, s, h->keys, h->vals, n, 64u, h->too_long, h->long_runs,
+              conv);
+    gr_launch(h->pdl, k_fix_long_runs, 148, 256, 0, s, h->keys, h->vals, h->sorter.k_alt, h->sorter.v_alt,
+              h->too_long, h->long_runs, conv);
 }
 
 static_assert(SC_TILE == (int)SC_TILE_LEAVES, "k_karras counts level bits per cell-level scan block");
 
 // The repulsion walk in the handle's schedule, with or without its interaction counts.
 template <int D, bool COUNT>
-static void launch_walk(gr_fa2 *h, const WalkParams &wp, cudaStream_t s) {
+static void launch_walk(gr_fa2 *h, const WalkParams &wp, cudaStream_t s, bool pdl) {
     const uint32_t n = h->n;
     DevState *st = h->st;
     if (h->walk_schedule == 2)
-        k_walk_s<D, 2, COUNT><<<div_up(div_up(n, 2), WALK_THREADS), WALK_THREADS, 0, s>>>(
-            wp, st, h->cells, h->sp, h->sorig, h->uid, h->leaf_pre, h->rep, st);
+        gr_launch(pdl, k_walk_s<D, 2, COUNT>, div_up(div_up(n, 2), WALK_THREADS), WALK_THREADS, 0, s, wp, st,
+                  h->cells, h->sp, h->sorig, h->uid, h->leaf_pre, h->rep, st);
     else if (h->walk_schedule == 1)
-        k_walk_s<D, 1, COUNT><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig,
-                                                                              h->uid, h->leaf_pre, h->rep, st);
+        gr_launch(pdl, k_walk_s<D, 1, COUNT>, div_up(n, WALK_THREADS), WALK_THREADS, 0, s, wp, st, h->cells, h->sp,
+                  h->sorig, h->uid, h->leaf_pre, h->rep, st);
     else
-        k_walk_s<D, 0, COUNT><<<div_up(n, WALK_THREADS), WALK_THREADS, 0, s>>>(wp, st, h->cells, h->sp, h->sorig,
-                                                                              h->uid, h->leaf_pre, h->rep, st);
+        gr_launch(pdl, k_walk_s<D, 0, COUNT>, div_up(n, WALK_THREADS), WALK_THREADS, 0, s, wp, st, h->cells, h->sp,
+                  h->sorig, h->uid, h->leaf_pre, h->rep, st);
 }
 
 template <int D>
@@ -423,16 +433,16 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
             k_keys<D><<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals);
             h->sorter.sort(h->keys, h->vals, n, 64, s, conv);
         }
-        k_leaf_tiles<D><<<ab, AG_T, 0, s>>>(st, n, h->pos, h->keys, h->vals, h->sp, h->sorig, h->tile_sum,
-                                             h->tile_cnt);
+        gr_launch(h->pdl, k_leaf_tiles<D>, ab, AG_T, 0, s, st, n, h->pos, h->keys, h->vals, h->sp, h->sorig,
+                  h->tile_sum, h->tile_cnt);
         const uint32_t *ccarry = nullptr;  // the carries come from one block above LEAF_FOLD_MAX_TILES tiles
         if (ab > LEAF_FOLD_MAX_TILES) {
             k_leaf_carry<D><<<1, CARRY_T, 0, s>>>(st, n, h->tile_sum, h->tile_cnt, h->tile_carry, h->tile_cnt + ab,
                                                   h->leaf_start, h->pre_local);
             ccarry = h->tile_cnt + ab;
         }
-        k_leaf_prefix<D><<<ab, AG_T, 0, s>>>(st, n, h->sp, h->keys, h->tile_sum, h->tile_cnt, h->tile_carry,
-                                              ccarry, h->uid, h->leaf_start, h->ukey, h->levels, h->pre_local);
+        gr_launch(h->pdl, k_leaf_prefix<D>, ab, AG_T, 0, s, st, n, h->sp, h->keys, h->tile_sum, h->tile_cnt,
+                  h->tile_carry, ccarry, h->uid, h->leaf_start, h->ukey, h->levels, h->pre_local);
         const Prefix pre{h->pre_local, h->tile_carry, h->leaf_start, 0u, ab};  // nu: read on the device
         const bool adjoint = h->bt.cell_of != nullptr;  // the adjoint reads leaf and node bodies as arrays
         BinTree bt = h->bt;  // the tick itself reads only the packed records and leaf_parent
@@ -443,15 +453,15 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
             bt.delta = bt.int_parent = nullptr;
         }
         bt.marks = fold_scan ? h->scanner.bsum : nullptr;
-        k_karras<D><<<gn, 256, 0, s>>>(st, h->ukey, bt);
+        gr_launch(h->pdl, k_karras<D>, gn, 256, 0, s, st, h->ukey, bt);
         if (adjoint) k_leaf_body<D><<<gn, 256, 0, s>>>(st, h->sp, h->leaf_start, h->leaf_body, h->leaf_coinc);
         if (adjoint) k_node_body<D><<<gn, 256, 0, s>>>(st, h->bt, pre, h->int_body);
         if (fold_scan)
-            h->scanner.scan_levels_marked(h->levels, h->P, n, &st->n_unique, &st->n_cells, s, conv);
+            h->scanner.scan_levels_marked(h->levels, h->P, n, &st->n_unique, &st->n_cells, s, conv, h->pdl);
         else
             h->scanner.scan_levels(h->levels, h->P, n, &st->n_unique, &st->n_cells, s, conv);
-        k_assign_cells<D><<<2 * gn, 256, 0, s>>>(st, bt, gn * 256, h->sp, h->P, h->levels, h->leaf_start,
-                                                 pre, h->cells, h->leaf_pre, st);
+        gr_launch(h->pdl, k_assign_cells<D>, 2 * gn, 256, 0, s, st, bt, gn * 256, h->sp, h->P, h->levels,
+                  h->leaf_start, pre, h->cells, h->leaf_pre, st);
     }
     if (h->timing_events) cudaEventRecordWithFlags(h->ev[1], s, cudaEventRecordExternal);
     if (branch) {
@@ -467,10 +477,13 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
         wp.kr = (float)h->prm[P_SCALING];
         wp.theta2 = (float)(h->prm[P_THETA] * h->prm[P_THETA]);
         wp.seed = (uint32_t)h->prm[P_SEED];
+        // in the timed graph an event record node stands before the walk: no
+        // programmatic edge there
+        const bool pdl = h->pdl && (phases & PH_TREE) && !h->timing_events;
         if (h->count_interactions)
-            launch_walk<D, true>(h, wp, s);
+            launch_walk<D, true>(h, wp, s, pdl);
         else
-            launch_walk<D, false>(h, wp, s);
+            launch_walk<D, false>(h, wp, s, pdl);
     }
     if (h->timing_events) cudaEventRecordWithFlags(h->ev[2], s, cudaEventRecordExternal);
     if (phases & PH_FINISH) {
@@ -490,7 +503,7 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
         k_forces<D><<<frc_blocks(n), FRC_THREADS, 0, s>>>(fp, st, h->pos, h->rep, h->U, h->part,
                                                                     forces_only ? 0 : 1);
         if (!forces_only)
-            k_update<D><<<frc_blocks(n), FRC_THREADS, 0, s>>>(n, st, h->pos, h->U, h->part);
+            gr_launch(h->pdl, k_update<D>, frc_blocks(n), FRC_THREADS, 0, s, n, st, h->pos, h->U, h->part);
     }
     if (h->timing_events) cudaEventRecordWithFlags(h->ev[3], s, cudaEventRecordExternal);
 }
@@ -502,8 +515,55 @@ static void enqueue(gr_fa2 *h, bool forces_only, int phases = PH_ALL) {
         enqueue_tick<2>(h, forces_only, phases);
 }
 
+// One capture of a whole tick into *g, its node priorities set and the graph
+// instantiated into *x (the error of the first step that failed).
+static cudaError_t capture_once(gr_fa2 *h, bool timing, cudaGraph_t *g, cudaGraphExec_t *x) {
+    cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    h->branch = true;
+    h->timing_events = timing;
+    enqueue(h, false, PH_ALL);
+    h->branch = false;
+    h->timing_events = false;
+    if ((e = cudaStreamEndCapture(h->stream, g)) != cudaSuccess) return e;
+    // The attraction branch fills what the tree build leaves idle: its kernels
+    // run at the lowest priority, the tick's own path at the highest, so a free
+    // SM slot goes to the tree's next block first.
+    int least = 0, greatest = 0;
+    if ((e = cudaDeviceGetStreamPriorityRange(&least, &greatest)) != cudaSuccess) return e;
+    size_t nn = 0;
+    if ((e = cudaGraphGetNodes(*g, nullptr, &nn)) != cudaSuccess) return e;
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if ((e = cudaGraphGetNodes(*g, nodes.data(), &nn)) != cudaSuccess) return e;
+    const void *side[4] = {(const void *)k_attract<2>, (const void *)k_attract<3>, (const void *)k_attract_seg<2>,
+                           (const void *)k_attract_seg<3>};
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        if ((e = cudaGraphNodeGetType(nd, &t)) != cudaSuccess) return e;
+        if (t != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp;
+        if ((e = cudaGraphKernelNodeGetParams(nd, &kp)) != cudaSuccess) return e;
+        bool low = false;
+        for (const void *f : side) low = low || kp.func == f;
+        cudaLaunchAttributeValue v;
+        memset(&v, 0, sizeof v);
+        v.priority = low ? least : greatest;
+        if ((e = cudaGraphKernelNodeSetAttribute(nd, cudaLaunchAttributePriority, &v)) != cudaSuccess) return e;
+    }
+    return cudaGraphInstantiate(x, *g, 0);
+}
+
+// Programmatic dependent launches for a new handle's ticks: on unless the
+// environment sets GR_PDL=0.
+static bool pdl_default() {
+    const char *v = getenv("GR_PDL");
+    return !(v && strcmp(v, "0") == 0);
+}
+
 // Captures one whole tick (with the attraction on its own branch), and with
-// timing the event records at its phase boundaries.
+// timing the event records at its phase boundaries. If the capture with
+// programmatic dependent launches fails, the handle drops them and captures
+// again with plain stream order.
 static int capture(gr_fa2 *h, bool timing, cudaGraph_t *g, cudaGraphExec_t *x) {
     if (!h->aux) {
         CU(cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking));
@@ -513,40 +573,20 @@ static int capture(gr_fa2 *h, bool timing, cudaGraph_t *g, cudaGraphExec_t *x) {
     if (timing)
         for (int i = 0; i < 4; i++)
             if (!h->ev[i]) CU(cudaEventCreate(&h->ev[i]));
-    CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    h->branch = true;
-    h->timing_events = timing;
-    enqueue(h, false, PH_ALL);
-    h->branch = false;
-    h->timing_events = false;
-    cudaError_t e = cudaStreamEndCapture(h->stream, g);
-    if (e != cudaSuccess) return set_err(GR_CUDA_ERROR, cudaGetErrorString(e));
-    // The attraction branch fills what the tree build leaves idle: its kernels
-    // run at the lowest priority, the tick's own path at the highest, so a free
-    // SM slot goes to the tree's next block first.
-    int least = 0, greatest = 0;
-    CU(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    size_t nn = 0;
-    CU(cudaGraphGetNodes(*g, nullptr, &nn));
-    std::vector<cudaGraphNode_t> nodes(nn);
-    CU(cudaGraphGetNodes(*g, nodes.data(), &nn));
-    const void *side[4] = {(const void *)k_attract<2>, (const void *)k_attract<3>, (const void *)k_attract_seg<2>,
-                           (const void *)k_attract_seg<3>};
-    for (auto nd : nodes) {
-        cudaGraphNodeType t;
-        CU(cudaGraphNodeGetType(nd, &t));
-        if (t != cudaGraphNodeTypeKernel) continue;
-        cudaKernelNodeParams kp;
-        CU(cudaGraphKernelNodeGetParams(nd, &kp));
-        bool low = false;
-        for (const void *f : side) low = low || kp.func == f;
-        cudaLaunchAttributeValue v;
-        memset(&v, 0, sizeof v);
-        v.priority = low ? least : greatest;
-        CU(cudaGraphKernelNodeSetAttribute(nd, cudaLaunchAttributePriority, &v));
+    for (;;) {
+        *g = nullptr;
+        *x = nullptr;
+        cudaError_t e = capture_once(h, timing, g, x);
+        if (e == cudaSuccess) return GR_OK;
+        cudaGetLastError();  // a capture error is not sticky: clear it
+        if (*x) cudaGraphExecDestroy(*x);
+        if (*g) cudaGraphDestroy(*g);
+        *g = nullptr;
+        *x = nullptr;
+        if (!h->pdl) return set_err(GR_CUDA_ERROR, cudaGetErrorString(e));
+        h->pdl = false;
+        h->pdl_fell_back = true;
     }
-    CU(cudaGraphInstantiate(x, *g, 0));
-    return GR_OK;
 }
 
 static int build_graph(gr_fa2 *h) {
@@ -675,6 +715,7 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
             break;
         }
         h->own_stream = true;
+        h->pdl = pdl_default();
         keep_pool();
         cudaStream_t s = h->stream;
         cudaError_t e = cudaSuccess;
@@ -1052,6 +1093,13 @@ int gr_fa2_set_walk_schedule(gr_fa2 *h, int schedule) {
         h->walk_schedule = schedule;
         h->drop_graphs();
     }
+    return ok();
+}
+
+int gr_fa2_launch_mode(gr_fa2 *h, int *programmatic) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    if (!programmatic) return set_err(GR_INVALID_ARGUMENT, "programmatic is null");
+    *programmatic = h->pdl ? 1 : 0;
     return ok();
 }
 

@@ -216,6 +216,7 @@ template <int D>
 __global__ void __launch_bounds__(FRC_THREADS)
 k_forces(ForceParams P, DevState *st, const float4 *__restrict__ pos, const float *__restrict__ rep, float *U,
          double *__restrict__ part, int speed_update) {
+    gr_pdl_enter();
     if (st->converged) return;
     __shared__ double s_red[32];
     __shared__ bool s_last;
@@ -256,6 +257,7 @@ template <int D>
 __global__ void __launch_bounds__(FRC_THREADS)
 k_update(uint32_t n, DevState *st, float4 *__restrict__ pos, const float *__restrict__ U,
          double *__restrict__ part) {
+    gr_pdl_enter();
     if (st->converged) return;
     __shared__ double s_red[32];
     __shared__ bool s_last;

@@ -167,6 +167,7 @@ __global__ void rs_zero(uint32_t *__restrict__ totals) { totals[blockIdx.x * RS_
 // max_run is left alone and raises *too_long instead.
 __global__ void rs_fix_runs(uint64_t *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t n, uint32_t max_run,
                             uint32_t *long_count, uint2 *__restrict__ long_runs, const uint32_t *skip) {
+    gr_pdl_enter();
     if (skip && *skip) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i + 1 >= n) return;
@@ -280,6 +281,7 @@ __global__ void __launch_bounds__(T)
 os_pass(const uint64_t *__restrict__ kin, const V *__restrict__ vin, uint64_t *__restrict__ kout, V *__restrict__ vout,
         uint32_t n, int shift, const uint32_t *__restrict__ ghist, uint32_t *status, uint32_t *counter, uint32_t *err,
         const uint32_t *skip) {
+    gr_pdl_enter();
     static_assert(T % RS_BINS == 0, "one thread per digit at least");
     constexpr int W = T / GR_WARP, TILE = T * I, CHUNK = I * GR_WARP;
     if (skip && *skip) return;
@@ -488,7 +490,7 @@ struct RadixSorter {
     // os_ghist (zeroed first) with the digit counts and zeroed the look-back
     // words (os_hist's work).
     void onesweep_passes(uint64_t *keys, uint32_t *vals, uint32_t n, int first_digit, int passes, cudaStream_t s,
-                         uint32_t *err, const uint32_t *skip = nullptr) {
+                         uint32_t *err, const uint32_t *skip = nullptr, bool pdl = false) {
         if (n == 0) return;
         const uint32_t nt = div_up(n, OS_T * OS_I);
         constexpr size_t smem = os_smem<uint32_t, OS_T, OS_I>();
@@ -498,9 +500,9 @@ struct RadixSorter {
         uint64_t *ka = keys, *kb = k_alt;
         uint32_t *va = vals, *vb = v_alt;
         for (int p = 0; p < passes; p++) {
-            os_pass<uint32_t, OS_T, OS_I, OS_L><<<nt, OS_T, smem, s>>>(
-                ka, va, kb, vb, n, 8 * (first_digit + p), os_ghist + p * RS_BINS, os_status + (size_t)p * nt * RS_BINS,
-                os_ghist + OS_MAX_PASSES * RS_BINS + p, err, skip);
+            gr_launch(pdl, os_pass<uint32_t, OS_T, OS_I, OS_L>, nt, OS_T, smem, s, ka, (const uint32_t *)va, kb, vb,
+                      n, 8 * (first_digit + p), (const uint32_t *)(os_ghist + p * RS_BINS),
+                      os_status + (size_t)p * nt * RS_BINS, os_ghist + OS_MAX_PASSES * RS_BINS + p, err, skip);
             std::swap(ka, kb);
             std::swap(va, vb);
         }

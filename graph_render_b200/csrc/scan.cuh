@@ -135,6 +135,7 @@ constexpr uint32_t SC_FOLD_MAX_BLOCKS = 2048;
 __global__ void __launch_bounds__(SC_THREADS)
 sc_levels_fold(const uint32_t *__restrict__ levels, uint32_t *__restrict__ out, const uint32_t *n_dev,
                const uint32_t *__restrict__ marks, uint32_t *total, const uint32_t *skip) {
+    gr_pdl_enter();
     if (skip && *skip) return;
     const uint32_t n = *n_dev;
     const uint32_t b = blockIdx.x;
@@ -231,9 +232,10 @@ struct Scanner {
     // SC_FOLD_MAX_BLOCKS blocks, n_dev given.
     bool folds(uint32_t n_host) const { return div_up(n_host, SC_TILE) <= SC_FOLD_MAX_BLOCKS; }
     void scan_levels_marked(const uint32_t *levels, uint32_t *out, uint32_t n_host, const uint32_t *n_dev,
-                            uint32_t *total, cudaStream_t s, const uint32_t *skip = nullptr) {
+                            uint32_t *total, cudaStream_t s, const uint32_t *skip = nullptr, bool pdl = false) {
         if (n_host == 0) return;
-        sc_levels_fold<<<div_up(n_host, SC_TILE), SC_THREADS, 0, s>>>(levels, out, n_dev, bsum, total, skip);
+        gr_launch(pdl, sc_levels_fold, div_up(n_host, SC_TILE), SC_THREADS, 0, s, levels, out, n_dev,
+                  (const uint32_t *)bsum, total, skip);
     }
 };
 

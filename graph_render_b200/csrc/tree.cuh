@@ -124,6 +124,7 @@ struct ZeroWords {
 template <int D>
 __global__ void __launch_bounds__(BND_THREADS)
 k_bounds(const float4 *__restrict__ pos, uint32_t n, DevState *st, double *__restrict__ part, ZeroWords zw) {
+    gr_pdl_enter();
     if (st->converged) return;
     if (blockIdx.x == 0) zw.clear();
     __shared__ double s_red[32];
@@ -254,6 +255,7 @@ k_bounds(const float4 *__restrict__ pos, uint32_t n, DevState *st, double *__res
 template <int D>
 __global__ void k_keys(const float4 *__restrict__ pos, uint32_t n, const DevState *st,
                        uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+    gr_pdl_enter();
     if (st->converged) return;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -410,6 +412,7 @@ __device__ __forceinline__ void mark_cells(bool valid, int32_t i, int32_t nu, co
 
 template <int D>
 __global__ void k_karras(const DevState *st, const uint64_t *__restrict__ k, BinTree t) {
+    gr_pdl_enter();
     if (st->converged) return;
     const int32_t nu = (int32_t)st->n_unique;
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -704,6 +707,7 @@ __global__ void __launch_bounds__(AG_T)
 k_leaf_tiles(DevState *st, uint32_t n, const float4 *__restrict__ pos, const uint64_t *__restrict__ keys,
              const uint32_t *__restrict__ perm, float4 *__restrict__ sp, uint32_t *__restrict__ sorig,
              Body *__restrict__ tile_sum, uint32_t *__restrict__ tile_cnt) {
+    gr_pdl_enter();
     if (st->converged) return;
     __shared__ Body s_w[2 * AG_W];
     __shared__ uint32_t s_c[2 * AG_W];
@@ -826,6 +830,7 @@ __global__ void __launch_bounds__(CARRY_T)
 k_leaf_carry(DevState *st, uint32_t n, const Body *__restrict__ tile_sum, const uint32_t *__restrict__ tile_cnt,
              BodyDD *__restrict__ carry, uint32_t *__restrict__ ccarry, uint32_t *__restrict__ leaf_start,
              double *__restrict__ pre) {
+    gr_pdl_enter();
     if (st->converged) return;
     constexpr int W = CARRY_T / GR_WARP;
     __shared__ BodyDD s_w[W];
@@ -910,6 +915,7 @@ k_leaf_prefix(DevState *st, uint32_t n, const float4 *__restrict__ sp, const uin
               const Body *__restrict__ tile_sum, const uint32_t *__restrict__ tile_cnt, BodyDD *__restrict__ carry,
               const uint32_t *__restrict__ ccarry, uint32_t *__restrict__ uid, uint32_t *__restrict__ leaf_start,
               uint64_t *__restrict__ ukey, uint32_t *__restrict__ levels, double *__restrict__ pre) {
+    gr_pdl_enter();
     if (st->converged) return;
     __shared__ Body s_w[2 * AG_W];
     __shared__ uint32_t s_c[2 * AG_W];
@@ -1096,6 +1102,7 @@ __global__ void k_assign_cells(const DevState *st, BinTree t, uint32_t n_slots, 
                                const uint32_t *__restrict__ leaf_start, Prefix pre,
                                Cells cells, uint32_t *__restrict__ leaf_pre,
                                DevState *stw) {
+    gr_pdl_enter();
     if (st->converged) return;
     constexpr int L = Levels<D>::L;
     const uint32_t nu = st->n_unique;

@@ -422,6 +422,7 @@ __global__ void __launch_bounds__(WALK_THREADS)
 k_walk_s(WalkParams P, const DevState *__restrict__ st, Cells cells, const float4 *__restrict__ sp,
          const uint32_t *__restrict__ sorig, const uint32_t *__restrict__ uid,
          const uint32_t *__restrict__ leaf_pre, float *__restrict__ rep, DevState *stw) {
+    gr_pdl_enter();
     if (st->converged) return;
     const uint32_t g = blockIdx.x * WALK_THREADS + threadIdx.x;
     const uint32_t p = SCHED == 2 ? 2 * g : g;

@@ -156,6 +156,12 @@ class Fa2:
     def set_walk_schedule(self, schedule: int) -> None:
         N.check(self._L.gr_fa2_set_walk_schedule(self.h, int(schedule)))
 
+    def programmatic_launches(self) -> bool:
+        """True when the tick's kernels are programmatic dependent launches."""
+        v = C.c_int()
+        N.check(self._L.gr_fa2_launch_mode(self.h, C.byref(v)))
+        return bool(v.value)
+
     def set_interaction_counting(self, on: bool) -> None:
         """On (the default): the walk counts far / pair interactions into info();
         off: it keeps no counts (same forces, fewer instructions per cell)."""

@@ -139,6 +139,12 @@ int gr_fa2_set_walk_schedule(gr_fa2 *h, int schedule);
  * forces are the same bit for bit) and the counters keep their values.
  * No counterpart in the reference (it counts nothing). */
 int gr_fa2_set_interaction_counting(gr_fa2 *h, int on);
+/* Launch mode of the tick's kernels: *programmatic = 1 when each is a programmatic
+ * dependent launch (scheduled while the kernel before it drains, then waiting for
+ * it before it reads anything; the default), 0 when they follow plain stream order
+ * (GR_PDL=0 in the environment at create, or a capture with them failed).
+ * No counterpart in the reference. */
+int gr_fa2_launch_mode(gr_fa2 *h, int *programmatic);
 int gr_fa2_tune(gr_fa2 *h, uint32_t sample_ticks, int *chosen, float *walk_ms_each);
 
 /* Current positions to a host buffer (n x dim), refusing non-finite ones as
