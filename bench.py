@@ -489,23 +489,26 @@ def run_gpu(args, dist: Dist):
         dst = torch.from_numpy(wl.dst).pin_memory().numpy()
         pos0 = torch.from_numpy(np.ascontiguousarray(wl.pos0)).pin_memory().numpy()
         w = None if wl.weight is None else torch.from_numpy(wl.weight).pin_memory().numpy()
+        out = torch.empty((wl.n, dim), dtype=torch.float32).pin_memory().numpy()
         T = args.e2e_ticks
         prm = dict(wl.params, max_iter=T)
-        dist.barrier()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        with F(wl.n, src, dst, w, params=prm, pos0=pos0) as e:
-            e.set_interaction_counting(False)
-            ran = e.run()
-            out = e.positions()
-        el = time.perf_counter() - t0
-        el = dist.max(el)
+        calls = []
+        for _ in range(3):  # one call is ~50 ms of wall clock: the median of three
+            dist.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            with F(wl.n, src, dst, w, params=prm, pos0=pos0) as e:
+                e.set_interaction_counting(False)
+                ran = e.run()
+                e.positions(out=out)
+            calls.append(dist.max(time.perf_counter() - t0))
+        el = float(np.median(calls))
         h2d = wl.m * 8 + wl.n * dim * 4 + (0 if w is None else wl.m * 8)
         d2h = wl.n * dim * 4
         e2e = {"value": dist.world * wl.n * ran / el, "unit": "node-ticks/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "step": f"one layout call: create from host edges + {ran} ticks + positions back",
-               "seconds": el}
+               "seconds": el, "calls_s": calls, "of": "median of 3 calls"}
 
     # the reference's quality measure of that layout (graph-cli bench.rs stress), on the device
     quality = None

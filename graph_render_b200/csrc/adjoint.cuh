@@ -226,8 +226,8 @@ k_adj_walk(WalkParams P, const DevState *__restrict__ st, Cells cells, const flo
     const uint32_t lane = threadIdx.x % GR_WARP;
     uint32_t k = 0;
     while (k < ncells) {
-        const float4 A = __ldg(&cells.A[k]);
-        const float4 B = __ldg(&cells.B[k]);
+        const float4 A = cell_a<D>(cells, k);
+        const float4 B = cell_b<D>(cells, k);
         int32_t sk;
         uint32_t start;
         float cx, cy, cz, cm, w2, ox, oy, oz;
@@ -237,7 +237,7 @@ k_adj_walk(WalkParams P, const DevState *__restrict__ st, Cells cells, const flo
             sk = __float_as_int(B.z);
             start = __float_as_uint(B.w);
         } else {
-            const int2 Cc = __ldg(&cells.C[k]);
+            const int2 Cc = cell_c3(cells, k);
             cx = A.x; cy = A.y; cz = A.z; cm = A.w;
             ox = B.x; oy = B.y; oz = B.z; w2 = B.w;
             sk = Cc.x;

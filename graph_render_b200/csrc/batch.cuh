@@ -88,10 +88,7 @@ __host__ __device__ inline size_t slot_carve(unsigned char *base, uint32_t nmax,
     v.leaf_body = slot_take<Body>(base, off, n);
     v.int_body = slot_take<Body>(base, off, n);
     v.leaf_coinc = slot_take<uint8_t>(base, off, n);
-    v.cells.A = slot_take<float4>(base, off, 2 * n);
-    v.cells.B = slot_take<float4>(base, off, 2 * n);
-    v.cells.C = D == 3 ? slot_take<int2>(base, off, 2 * n) : nullptr;
-    v.cells.bounds = nullptr;
+    v.cells = cells_view(slot_take<float4>(base, off, cells_float4s(2 * nmax, D)), 2 * nmax, D);
     v.rep = slot_take<float>(base, off, n * D);
     v.U = slot_take<float>(base, off, n * D);
     v.att = slot_take<float>(base, off, n * D);

@@ -172,8 +172,8 @@ k_d3_charge(D3Params P, const D3State *st, const DevState *ts, Cells cells, cons
     float ax = 0.f, ay = 0.f;
     uint32_t k = 0;
     while (k < ncells) {
-        const float4 A = __ldg(&cells.A[k]);
-        const float4 B = __ldg(&cells.B[k]);
+        const float4 A = cell_a<2>(cells, k);
+        const float4 B = cell_b<2>(cells, k);
         const int32_t sk = __float_as_int(B.z);
         const bool leaf = sk < 0;
         float dx = (A.x - me.x) + B.x, dy = (A.y - me.y) + B.y;
@@ -237,7 +237,7 @@ k_d3_collide(D3Params P, const D3State *st, const DevState *ts, Cells cells, con
     float ax = 0.f, ay = 0.f;
     uint32_t k = 0;
     while (k < ncells) {
-        const float4 B = __ldg(&cells.B[k]);
+        const float4 B = cell_b<2>(cells, k);
         const int32_t sk = __float_as_int(B.z);
         if (sk < 0) {
             const uint32_t start = __float_as_uint(B.w), cnt = (uint32_t)(-sk);

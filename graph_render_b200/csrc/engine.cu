@@ -264,9 +264,11 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
     A(h->tile_sum, div_up(n, AG_TILE) + 1);
     A(h->tile_carry, div_up(n, AG_TILE) + 1);
     A(h->tile_cnt, 2 * ((size_t)div_up(n, AG_TILE) + 1));
-    A(h->cells.A, 2 * (size_t)n);
-    A(h->cells.B, 2 * (size_t)n);
-    if (D == 3) A(h->cells.C, 2 * (size_t)n);
+    {
+        float4 *cb = nullptr;  // cells: 2n at most
+        A(cb, cells_float4s(2 * n, D));
+        h->cells = cells_view(cb, 2 * n, D);
+    }
     A(h->rep, (size_t)n * D);
     A(h->U, (size_t)n * D);
     size_t np = std::max<size_t>((size_t)h->bnd_blocks() * 3 * D, 2 * (size_t)div_up(n, FRC_THREADS)) + 8;
@@ -1325,9 +1327,7 @@ static int forces_static(uint32_t n, const float4 *nodes, const uint32_t *rp, co
     h.tile_sum = cv.take<Body>(div_up(n, AG_TILE) + 1);
     h.tile_carry = cv.take<BodyDD>(div_up(n, AG_TILE) + 1);
     h.tile_cnt = cv.take<uint32_t>(2 * ((size_t)div_up(n, AG_TILE) + 1));
-    h.cells.A = cv.take<float4>(2 * (size_t)n);
-    h.cells.B = cv.take<float4>(2 * (size_t)n);
-    h.cells.C = D == 3 ? cv.take<int2>(2 * (size_t)n) : nullptr;
+    h.cells = cells_view(cv.take<float4>(cells_float4s(2 * n, D)), 2 * n, D);
     h.rep = cv.take<float>((size_t)n * D);
     h.part = cv.take<double>(std::max<size_t>((size_t)h.bnd_blocks() * 3 * D, 2 * (size_t)div_up(n, FRC_THREADS)) + 8);
     h.sorter.cap = n;

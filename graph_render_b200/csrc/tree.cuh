@@ -1005,14 +1005,45 @@ __device__ __forceinline__ uint32_t count_leaf(uint32_t s, const BinTree &t) {
 }
 
 // Cell record, 2D: A = {cx, cy, mass, w^2}, B = {cx_lo, cy_lo, skip | -count, start}.
-// 3D: A = {cx, cy, cz, mass}, B = {cx_lo, cy_lo, cz_lo, w^2}, C = {skip | -count, start}.
+// 3D: A = {cx, cy, cz, mass}, B = {cx_lo, cy_lo, cz_lo, w^2}, C = {skip | -count, start, -, -}.
 // The centre is an FP32 hi/lo pair of the FP64 centre of mass, so a node at
 // 1e4 still resolves a nearby centre to ~1e-3 ulp instead of a whole FP32 ulp.
+// In 2D the A and B records are two arrays (rec[k], rec_b[k]): the 32 lanes of a
+// walk warp visit different but nearby cells, and one 32-byte sector of the A
+// array holds two cells' A (measured: a per-cell 32-byte record made the 2D
+// per-lane walk 13% slower). In 3D a cell's records lie together (rec[3k + 0] =
+// A, + 1 = B, + 2 = C): one line per visit instead of three (the 3D walk 6%
+// faster than with three arrays).
+template <int D> struct CellF { static constexpr uint32_t F = D == 3 ? 3 : 1; };  // float4s per cell in rec
+
 struct Cells {
-    float4 *A, *B;
-    int2 *C;
+    float4 *rec;     // 2D: A of cell k at rec[k]; 3D: cell k's A, B, C at rec[3k ..]
+    float4 *rec_b;   // 2D: B of cell k at rec_b[k]; 3D: unused
     float4 *bounds;  // nullable: each cell's square {x0, y0, x1, y1} (2D), for range pruning
 };
+
+template <int D>
+__device__ __forceinline__ float4 cell_a(const Cells &c, uint32_t k) {
+    return __ldg(&c.rec[(size_t)k * CellF<D>::F]);
+}
+template <int D>
+__device__ __forceinline__ float4 cell_b(const Cells &c, uint32_t k) {
+    return D == 3 ? __ldg(&c.rec[(size_t)k * 3 + 1]) : __ldg(&c.rec_b[k]);
+}
+__device__ __forceinline__ int2 cell_c3(const Cells &c, uint32_t k) {  // 3D: {skip | -count, start}
+    const float4 v = __ldg(&c.rec[(size_t)k * 3 + 2]);
+    return make_int2(__float_as_int(v.x), __float_as_int(v.y));
+}
+
+// Float4 records a cells buffer holds for `cap` cells, and its two views.
+__host__ __device__ inline size_t cells_float4s(uint32_t cap, int dim) { return (size_t)cap * (dim == 3 ? 3 : 2); }
+__host__ __device__ inline Cells cells_view(float4 *buf, uint32_t cap, int dim) {
+    Cells c;
+    c.rec = buf;
+    c.rec_b = dim == 3 ? nullptr : buf + cap;
+    c.bounds = nullptr;
+    return c;
+}
 
 // The square of the level-`level` cell holding point p: the root corner plus
 // floor((p - corner) / w) sides, exact in FP64 (w is a power of two times the
@@ -1042,13 +1073,14 @@ __device__ __forceinline__ void write_cell(Cells c, uint32_t idx, const Body &b,
     }
     double w = ldexp(root_w, -level);
     float w2 = (float)(w * w);
+    float4 *r = c.rec + (size_t)idx * CellF<D>::F;
     if (D == 2) {
-        c.A[idx] = make_float4(hi[0], hi[1], (float)b.m, w2);
-        c.B[idx] = make_float4(lo[0], lo[1], __int_as_float(skip_or_count), __uint_as_float(start));
+        r[0] = make_float4(hi[0], hi[1], (float)b.m, w2);
+        c.rec_b[idx] = make_float4(lo[0], lo[1], __int_as_float(skip_or_count), __uint_as_float(start));
     } else {
-        c.A[idx] = make_float4(hi[0], hi[1], hi[2], (float)b.m);
-        c.B[idx] = make_float4(lo[0], lo[1], lo[2], w2);
-        c.C[idx] = make_int2(skip_or_count, (int32_t)start);
+        r[0] = make_float4(hi[0], hi[1], hi[2], (float)b.m);
+        r[1] = make_float4(lo[0], lo[1], lo[2], w2);
+        r[2] = make_float4(__int_as_float(skip_or_count), __uint_as_float(start), 0.f, 0.f);
     }
 }
 

@@ -61,8 +61,8 @@ __device__ __forceinline__ void walk_group(const WalkView &V, uint32_t p, float 
 
     uint32_t k = 0;
     while (k < ncells) {
-        const float4 A = __ldg(&cells.A[k]);
-        const float4 B = __ldg(&cells.B[k]);
+        const float4 A = cell_a<D>(cells, k);
+        const float4 B = cell_b<D>(cells, k);
         int32_t sk;
         uint32_t start;
         float cx, cy, cz, cm, w2, lx, ly, lz;
@@ -72,7 +72,7 @@ __device__ __forceinline__ void walk_group(const WalkView &V, uint32_t p, float 
             sk = __float_as_int(B.z);
             start = __float_as_uint(B.w);
         } else {
-            const int2 Cc = __ldg(&cells.C[k]);
+            const int2 Cc = cell_c3(cells, k);
             cx = A.x; cy = A.y; cz = A.z; cm = A.w;
             lx = B.x; ly = B.y; lz = B.z; w2 = B.w;
             sk = Cc.x;
@@ -192,8 +192,8 @@ __device__ __forceinline__ void lane_step(const WalkView &V, LaneNode &X) {
     const uint32_t n = V.n, iter = V.iter, k = X.k, oi = X.oi;
     const float4 me = X.me;
     const float th2 = V.th2, mk = X.mk;
-    const float4 A = __ldg(&cells.A[k]);
-    const float4 B = __ldg(&cells.B[k]);
+    const float4 A = cell_a<D>(cells, k);
+    const float4 B = cell_b<D>(cells, k);
     int32_t sk;
     uint32_t start;
     float cx, cy, cz, cm, w2, lx, ly, lz;
@@ -203,7 +203,7 @@ __device__ __forceinline__ void lane_step(const WalkView &V, LaneNode &X) {
         sk = __float_as_int(B.z);
         start = __float_as_uint(B.w);
     } else {
-        const int2 Cc = __ldg(&cells.C[k]);
+        const int2 Cc = cell_c3(cells, k);
         cx = A.x; cy = A.y; cz = A.z; cm = A.w;
         lx = B.x; ly = B.y; lz = B.z; w2 = B.w;
         sk = Cc.x;
@@ -387,8 +387,8 @@ __device__ __forceinline__ void walk_pair(const WalkView &V, PairNode &a, PairNo
     const uint32_t ncells = V.ncells;
     uint32_t k = min(a.resume, b.resume);
     while (k < ncells) {
-        const float4 A = __ldg(&cells.A[k]);
-        const float4 B = __ldg(&cells.B[k]);
+        const float4 A = cell_a<D>(cells, k);
+        const float4 B = cell_b<D>(cells, k);
         int32_t sk;
         uint32_t start;
         float cx, cy, cz, cm, w2, lx, ly, lz;
@@ -398,7 +398,7 @@ __device__ __forceinline__ void walk_pair(const WalkView &V, PairNode &a, PairNo
             sk = __float_as_int(B.z);
             start = __float_as_uint(B.w);
         } else {
-            const int2 Cc = __ldg(&cells.C[k]);
+            const int2 Cc = cell_c3(cells, k);
             cx = A.x; cy = A.y; cz = A.z; cm = A.w;
             lx = B.x; ly = B.y; lz = B.z; w2 = B.w;
             sk = Cc.x;

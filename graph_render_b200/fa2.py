@@ -129,8 +129,14 @@ class Fa2:
         N.check(self._L.gr_fa2_adjoint_backward(self.h, _ptr(g), _ptr(dp0), _ptr(dw)))
         return dp0, dw[:self.m_raw]
 
-    def positions(self) -> np.ndarray:
-        out = np.zeros((self.n, self.dim), np.float32)
+    def positions(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """The positions, row-major n x dim FP32. `out` (optional) is written in
+        place: a C-contiguous float32 array of that shape, e.g. in pinned memory,
+        which the device copies into directly."""
+        if out is None:
+            out = np.empty((self.n, self.dim), np.float32)
+        elif out.dtype != np.float32 or out.shape != (self.n, self.dim) or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous float32 array of shape ({self.n}, {self.dim})")
         N.check(self._L.gr_fa2_positions(self.h, _ptr(out)))
         return out
 
