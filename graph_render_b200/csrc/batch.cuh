@@ -2,8 +2,8 @@
 //
 // Each CTA takes graphs from a queue ordered largest first and runs every tick
 // of its graph by itself: the same per-item functions as the one-graph engine
-// (Morton key, Karras node, bottom-up sums, cell assignment, warp-cooperative
-// walk, node force, node update) over block-level sort / scan / reductions, with
+// (Morton key, Karras node with its cell marks, point-term prefix, cell writer,
+// per-lane walk, node force, node update) over block-level sort / scan / reductions, with
 // __syncthreads between phases instead of kernel boundaries. A graph's state
 // (positions, CSR rows, FP64 speed controller) lives in global memory; the
 // tree scratch lives in the CTA's slot, sized for the largest graph. No
@@ -35,11 +35,11 @@ struct BatchState {  // per graph; FP64 controller as in DevState
 // Per-slot scratch, carved from one allocation in a fixed order.
 struct SlotView {
     uint64_t *keys, *kalt, *ukey;
-    uint32_t *vals, *valt, *sorig, *flag, *excl, *uid, *leaf_start, *cells_at, *P, *leaf_pre;
+    uint32_t *vals, *valt, *sorig, *flag, *excl, *uid, *leaf_start, *levels, *P, *leaf_pre;
     float4 *sp;
     BinTree bt;
-    Body *leaf_body, *int_body;
-    uint8_t *leaf_coinc;
+    BodyDD *pre;        // double-double prefix of the point terms at every leaf start (nu + 1)
+    uint8_t *cell_flag;  // internal node -> 1 when it is a cell
     Cells cells;
     float *rep, *U, *att;
 };
@@ -68,7 +68,7 @@ __host__ __device__ inline size_t slot_carve(unsigned char *base, uint32_t nmax,
     v.excl = slot_take<uint32_t>(base, off, n);
     v.uid = slot_take<uint32_t>(base, off, n);
     v.leaf_start = slot_take<uint32_t>(base, off, n + 1);
-    v.cells_at = slot_take<uint32_t>(base, off, n);
+    v.levels = slot_take<uint32_t>(base, off, n);
     v.P = slot_take<uint32_t>(base, off, n + 1);
     v.leaf_pre = slot_take<uint32_t>(base, off, n);
     v.sp = slot_take<float4>(base, off, n);
@@ -85,9 +85,8 @@ __host__ __device__ inline size_t slot_carve(unsigned char *base, uint32_t nmax,
     v.bt.levels = nullptr;
     v.bt.cell_flag = nullptr;
     v.bt.marks = nullptr;
-    v.leaf_body = slot_take<Body>(base, off, n);
-    v.int_body = slot_take<Body>(base, off, n);
-    v.leaf_coinc = slot_take<uint8_t>(base, off, n);
+    v.pre = slot_take<BodyDD>(base, off, n + 1);
+    v.cell_flag = slot_take<uint8_t>(base, off, n);
     v.cells = cells_view(slot_take<float4>(base, off, cells_float4s(2 * nmax, D)), 2 * nmax, D);
     v.rep = slot_take<float>(base, off, n * D);
     v.U = slot_take<float>(base, off, n * D);
@@ -126,6 +125,48 @@ __device__ uint32_t block_scan_excl(const uint32_t *in, uint32_t *out, uint32_t 
         __syncthreads();
     }
     return carry;
+}
+
+// The double-double prefix of the sorted points' FP64 terms (m, m x per axis) at
+// every leaf start: pre[e] for leaf e (flag[p] marks the first point of leaf
+// excl[p]) and pre[nu] the total. Chunks of BT points, each an FP64 block scan
+// in a fixed shape (warp scans, then the warp totals in warp order), carried
+// across chunks in double-double: a cell's sums as the difference of two
+// prefixes are as exact as a direct FP64 sum over its points.
+template <int D, int BT>
+__device__ void block_leaf_prefix(const float4 *sp, const uint32_t *flag, const uint32_t *excl, uint32_t n,
+                                  uint32_t nu, BodyDD *pre, Body *s_bw, BodyDD *s_carry) {
+    constexpr int W = BT / GR_WARP;
+    const int t = threadIdx.x, lane = t % GR_WARP, w = t / GR_WARP;
+    if (t == 0) *s_carry = BodyDD{};
+    __syncthreads();
+    for (uint32_t base = 0; base < n; base += BT) {
+        const uint32_t p = base + t;
+        const Body x = p < n ? point_body<D>(sp[p]) : Body{0.0, 0.0, 0.0, 0.0};
+        Body inc = x;
+#pragma unroll
+        for (int o = 1; o < GR_WARP; o <<= 1) {
+            const Body u{shfl_up_d(inc.m, o), shfl_up_d(inc.c0, o), shfl_up_d(inc.c1, o),
+                         D == 3 ? shfl_up_d(inc.c2, o) : 0.0};
+            if (lane >= o) inc = body_sum<D>(u, inc);
+        }
+        Body lanes_before{shfl_up_d(inc.m, 1), shfl_up_d(inc.c0, 1), shfl_up_d(inc.c1, 1),
+                          D == 3 ? shfl_up_d(inc.c2, 1) : 0.0};
+        if (lane == 0) lanes_before = Body{0.0, 0.0, 0.0, 0.0};
+        if (lane == GR_WARP - 1) s_bw[w] = inc;
+        __syncthreads();
+        Body before{0.0, 0.0, 0.0, 0.0}, tot{0.0, 0.0, 0.0, 0.0};
+        for (int k = 0; k < W; k++) {
+            if (k < w) before = body_sum<D>(before, s_bw[k]);
+            tot = body_sum<D>(tot, s_bw[k]);
+        }
+        if (p < n && flag[p]) pre[excl[p]] = bdd_add_body<D>(*s_carry, body_sum<D>(before, lanes_before));
+        __syncthreads();
+        if (t == 0) *s_carry = bdd_add_body<D>(*s_carry, tot);
+        __syncthreads();
+    }
+    if (t == 0) pre[nu] = *s_carry;
+    __syncthreads();
 }
 
 // Stable LSD radix sort of keys[0..n) with vals, 8 x 8-bit passes, in place
@@ -258,6 +299,8 @@ __global__ void __launch_bounds__(BT) k_batch(BatchArgs A) {
     __shared__ uint32_t s_graph;
     __shared__ double s_root0[3], s_root_w, s_mean[3];
     __shared__ BatchState s_st;
+    __shared__ Body s_bw[32];
+    __shared__ BodyDD s_carry;
 
     const int t = threadIdx.x, lane = t % GR_WARP, w = t / GR_WARP;
     SlotView S;
@@ -367,23 +410,59 @@ __global__ void __launch_bounds__(BT) k_batch(BatchArgs A) {
                 if (f) {
                     S.leaf_start[e] = p;
                     S.ukey[e] = S.keys[p];
+                    S.levels[e] = 0;
                 }
                 if (p == n - 1) S.leaf_start[e + f] = n;
             }
             __syncthreads();
-            // ---- tree
+            // ---- tree: the one-graph engine's construction at block level. The
+            //      point-term prefix at every leaf start; Karras nodes, each marking
+            //      the cells among its children (bit `level` at the cell's first
+            //      leaf); leaf s starts 1 + popc(levels[s]) cells, so an exclusive
+            //      scan gives every leaf's first cell; then every cell at once: a
+            //      leaf's body from its points, an internal cell's as the
+            //      difference of two prefixes.
+            block_leaf_prefix<D, BT>(S.sp, S.flag, S.excl, n, nu, S.pre, s_bw, &s_carry);
             if (t == 0 && nu == 1) S.bt.leaf_parent[0] = -1;
-            for (uint32_t i = t; i + 1 < nu; i += BT) karras_node((int32_t)i, (int32_t)nu, S.ukey, S.bt);
+            for (uint32_t i = t; i + 1 < nu; i += BT) {
+                const KarrasNode q = karras_node((int32_t)i, (int32_t)nu, S.ukey, S.bt);
+                mark_cells<D>(true, (int32_t)i, (int32_t)nu, S.ukey, q, S.levels, S.cell_flag, nullptr, 1u);
+            }
             __syncthreads();
-            for (uint32_t s = t; s < nu; s += BT)
-                aggregate_leaf<D>(s, S.sp, S.leaf_start, S.bt, S.leaf_body, S.int_body, S.leaf_coinc, &s_st.error);
+            for (uint32_t s = t; s < nu; s += BT) S.excl[s] = 1u + (uint32_t)__popc(S.levels[s]);
             __syncthreads();
-            for (uint32_t s = t; s < nu; s += BT) S.cells_at[s] = count_leaf<D>(s, S.bt);
-            __syncthreads();
-            const uint32_t ncells = block_scan_excl<BT>(S.cells_at, S.P, nu, s_warp);
-            for (uint32_t s = t; s < nu; s += BT)
-                assign_leaf<D>(s, nu, ncells, s_root_w, S.bt, S.sp, S.P, S.cells_at, S.leaf_start, S.leaf_body,
-                               S.int_body, S.leaf_coinc, S.cells, S.leaf_pre, &s_st.error);
+            const uint32_t ncells = block_scan_excl<BT>(S.excl, S.P, nu, s_warp);
+            {
+                constexpr int L = Levels<D>::L;
+                for (uint32_t s = t; s < nu; s += BT) {  // leaf cells
+                    const uint32_t idx = S.P[s] + (uint32_t)__popc(S.levels[s]);
+                    const uint32_t a0 = S.leaf_start[s], a1 = S.leaf_start[s + 1];
+                    if (idx >= ncells || a1 <= a0) {
+                        atomicOr(&s_st.error, (uint32_t)ERR_TREE);
+                        continue;
+                    }
+                    const float4 one = S.sp[a0];
+                    bool coinc;
+                    const Body body = leaf_sum<D>(S.sp, a0, a1, coinc);
+                    const int level = nu == 1 ? 0 : coinc ? S.bt.delta[S.bt.leaf_parent[s]] / D + 1 : L;
+                    write_cell<D>(S.cells, idx, body, level, s_root_w, -(int32_t)(a1 - a0), a0,
+                                  a1 - a0 == 1 ? &one : nullptr);
+                    S.leaf_pre[s] = idx;
+                }
+                for (uint32_t i = t; i + 1 < nu; i += BT) {  // internal cells
+                    if (!S.cell_flag[i]) continue;
+                    const int lv = S.bt.delta[i] / D;
+                    const uint32_t f = S.bt.first[i], end = S.bt.last[i] + 1;
+                    const uint32_t idx = S.P[f] + (uint32_t)__popc(S.levels[f] & ((1u << lv) - 1u));
+                    const uint32_t skip = end == nu ? ncells : S.P[end];
+                    if (idx >= ncells || skip <= idx || skip > ncells) {
+                        atomicOr(&s_st.error, (uint32_t)ERR_TREE);
+                        continue;
+                    }
+                    write_cell<D>(S.cells, idx, range_body(S.pre[f], S.pre[end]), lv, s_root_w, (int32_t)skip,
+                                  S.leaf_start[f]);
+                }
+            }
             __syncthreads();
             // ---- repulsion walk: warp w takes groups of 32 sorted nodes, one per lane
             //      (walk_lane: the same forces, bit for bit, as the warp-union walk)

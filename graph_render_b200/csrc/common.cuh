@@ -66,12 +66,6 @@ __device__ __forceinline__ Body body_add(const Body &a, const Body &b) {
     return r;
 }
 
-__device__ __forceinline__ Body body_load_cg(const Body *p) {
-    const double2 *q = reinterpret_cast<const double2 *>(p);
-    double2 a = __ldcg(q), b = __ldcg(q + 1);
-    return Body{a.x, a.y, b.x, b.y};
-}
-
 __device__ __forceinline__ void body_store(Body *p, const Body &b) {
     double2 *q = reinterpret_cast<double2 *>(p);
     q[0] = make_double2(b.m, b.c0);

@@ -11,11 +11,13 @@
 // exactly the reference's cells that hold two or more distinct keys.
 //
 // Build, all integer except the FP64 sums:
-//   keys -> LSD radix sort -> unique keys (leaves) -> Karras binary radix tree
-//   over the unique keys -> FP64 mass / mass-moment sums bottom-up ->
-//   quad/oct cells = binary nodes whose level (common prefix / D) differs from
-//   their parent's -> preorder index of every cell from an exclusive scan of
-//   "cells starting at leaf s" -> skip(cell) = P[last leaf + 1].
+//   keys -> LSD radix sort -> unique keys (leaves) and the prefix of the points'
+//   FP64 mass / mass-moment terms at every leaf start -> Karras binary radix
+//   tree over the unique keys, each node marking the quad/oct cells among its
+//   children (binary nodes whose level, common prefix / D, differs from their
+//   parent's) -> preorder index of every cell from an exclusive scan of "cells
+//   starting at leaf s" -> every cell written at once, its sums from its points
+//   (a leaf) or as the difference of two prefixes, skip(cell) = P[last leaf + 1].
 // A chain of single-child cells in the reference collapses to its deepest
 // member here; the walk's far test is monotone in the cell width and the chain
 // shares one mass and centre, so the collapsed cell opens and approximates
@@ -422,59 +424,6 @@ __global__ void k_karras(const DevState *st, const uint64_t *__restrict__ k, Bin
     KarrasNode q{0, 0, 0, 0};
     if (valid) q = karras_node(i, nu, k, t);
     if (t.levels) mark_cells<D>(valid, i, nu, k, q, t.levels, t.cell_flag, t.marks, SC_TILE_LEAVES);
-}
-
-// Leaf s's FP64 sums, then the bottom-up pass: the second thread to reach a
-// node sums its two children, left then right, so every node's value is
-// independent of arrival order.
-template <int D>
-__device__ __forceinline__ void aggregate_leaf(uint32_t s, const float4 *__restrict__ sp,
-                                               const uint32_t *__restrict__ leaf_start, BinTree t,
-                                               Body *__restrict__ leaf_body, Body *__restrict__ int_body,
-                                               uint8_t *__restrict__ leaf_coinc, uint32_t *err) {
-    const uint32_t a0 = leaf_start[s], a1 = leaf_start[s + 1];
-    Body b{0.0, 0.0, 0.0, 0.0};
-    const float4 f0 = sp[a0];
-    bool coinc = true;
-    for (uint32_t q = a0; q < a1; q++) {
-        float4 p = sp[q];
-        double m = (double)p.w;
-        b.m += m;
-        b.c0 += m * (double)p.x;
-        b.c1 += m * (double)p.y;
-        if (D == 3) b.c2 += m * (double)p.z;
-        coinc = coinc && p.x == f0.x && p.y == f0.y && (D == 2 || p.z == f0.z);
-    }
-    body_store(&leaf_body[s], b);
-    leaf_coinc[s] = coinc ? 1 : 0;
-    int32_t node = t.leaf_parent[s];
-    // a binary radix tree over 64-bit keys is at most 64 levels deep
-    for (int depth = 0; node >= 0; depth++) {
-        if (depth > 66) {
-            atomicOr(err, (uint32_t)ERR_TREE);
-            return;
-        }
-        __threadfence();
-        if (atomicAdd(&t.visit[node], 1u) == 0u) return;
-        __threadfence();
-        uint32_t l = t.left[node], r = t.right[node];
-        Body bl = (l & LEAF_BIT) ? body_load_cg(&leaf_body[l & ~LEAF_BIT]) : body_load_cg(&int_body[l]);
-        Body br = (r & LEAF_BIT) ? body_load_cg(&leaf_body[r & ~LEAF_BIT]) : body_load_cg(&int_body[r]);
-        body_store(&int_body[node], body_add(bl, br));
-        node = t.int_parent[node];
-    }
-}
-
-template <int D>
-__global__ void k_aggregate(DevState *st, const float4 *__restrict__ sp,
-                            const uint32_t *__restrict__ leaf_start, BinTree t,
-                            Body *__restrict__ leaf_body, Body *__restrict__ int_body,
-                            uint8_t *__restrict__ leaf_coinc) {
-    if (st->converged) return;
-    const uint32_t nu = st->n_unique;
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nu) return;
-    aggregate_leaf<D>(s, sp, leaf_start, t, leaf_body, int_body, leaf_coinc, &st->error);
 }
 
 // ---- bodies without atomics: a prefix of the point terms (m, m x per axis;
@@ -991,19 +940,6 @@ __device__ __forceinline__ bool is_cell(const BinTree &t, int32_t node) {
     return par < 0 || (t.delta[node] / D) != (t.delta[par] / D);
 }
 
-// How many cells start at unique leaf s (the leaf itself plus the cell
-// ancestors whose range begins there).
-template <int D>
-__device__ __forceinline__ uint32_t count_leaf(uint32_t s, const BinTree &t) {
-    uint32_t c = 1;
-    int32_t par = t.leaf_parent[s];
-    for (int depth = 0; par >= 0 && t.first[par] == s && depth <= 66; depth++) {
-        if (is_cell<D>(t, par)) c++;
-        par = t.int_parent[par];
-    }
-    return c;
-}
-
 // Cell record, 2D: A = {cx, cy, mass, w^2}, B = {cx_lo, cy_lo, skip | -count, start}.
 // 3D: A = {cx, cy, cz, mass}, B = {cx_lo, cy_lo, cz_lo, w^2}, C = {skip | -count, start, -, -}.
 // The centre is an FP32 hi/lo pair of the FP64 centre of mass, so a node at
@@ -1082,41 +1018,6 @@ __device__ __forceinline__ void write_cell(Cells c, uint32_t idx, const Body &b,
         r[1] = make_float4(lo[0], lo[1], lo[2], w2);
         r[2] = make_float4(__int_as_float(skip_or_count), __uint_as_float(start), 0.f, 0.f);
     }
-}
-
-// Writes every cell at its preorder index: leaf s at P[s] + cells_at[s] - 1,
-// its cell ancestors starting at s above it, skip(cell) = P[last leaf + 1].
-// A leaf of coincident points sits one level below its parent cell (where the
-// reference chains them); a leaf of distinct points the key could not separate
-// sits at the key's last level.
-template <int D>
-__device__ __forceinline__ void assign_leaf(uint32_t s, uint32_t nu, uint32_t ncells, double rw, const BinTree &t,
-                                            const float4 *__restrict__ sp, const uint32_t *__restrict__ P,
-                                            const uint32_t *__restrict__ cells_at,
-                                            const uint32_t *__restrict__ leaf_start,
-                                            const Body *__restrict__ leaf_body, const Body *__restrict__ int_body,
-                                            const uint8_t *__restrict__ leaf_coinc, Cells cells,
-                                            uint32_t *__restrict__ leaf_pre, uint32_t *err) {
-    constexpr int L = Levels<D>::L;
-    uint32_t idx = P[s] + cells_at[s] - 1;
-    int32_t par = t.leaf_parent[s];
-    int level = 0;
-    if (par >= 0) level = leaf_coinc[s] ? t.delta[par] / D + 1 : L;
-    uint32_t a0 = leaf_start[s], a1 = leaf_start[s + 1];
-    const float4 one = sp[a0];
-    write_cell<D>(cells, idx, leaf_body[s], level, rw, -(int32_t)(a1 - a0), a0, a1 - a0 == 1 ? &one : nullptr);
-    leaf_pre[s] = idx;
-    for (int depth = 0; par >= 0 && t.first[par] == s && depth <= 66; depth++) {
-        if (is_cell<D>(t, par)) {
-            idx--;
-            uint32_t end = t.last[par] + 1;
-            uint32_t skip = end == nu ? ncells : P[end];
-            write_cell<D>(cells, idx, int_body[par], t.delta[par] / D, rw, (int32_t)skip, a0);
-            if (t.cell_of) t.cell_of[par] = idx;
-        }
-        par = t.int_parent[par];
-    }
-    if (idx != P[s]) atomicOr(err, (uint32_t)ERR_TREE);
 }
 
 // Every cell at its preorder index, without walking chains: threads
