@@ -169,12 +169,13 @@ __device__ void block_leaf_prefix(const float4 *sp, const uint32_t *flag, const 
     __syncthreads();
 }
 
-// Stable LSD radix sort of keys[0..n) with vals, 8 x 8-bit passes, in place
-// (kalt/valt are the ping-pong partners). Warp w owns a contiguous chunk and
-// ranks it in order with match/popc, so equal digits keep their input order.
+// Stable LSD radix sort of keys[0..n) with vals by the 8-bit digits
+// first_digit .. first_digit + passes - 1 (passes even, so the result lands back
+// in place; kalt/valt are the ping-pong partners). Warp w owns a contiguous chunk
+// and ranks it in order with ballots/popc, so equal digits keep their input order.
 template <int BT>
 __device__ void block_sort(uint64_t *keys, uint32_t *vals, uint64_t *kalt, uint32_t *valt, uint32_t n,
-                           uint32_t (*s_cnt)[256], uint32_t *s_tot) {
+                           uint32_t (*s_cnt)[256], uint32_t *s_tot, int first_digit = 0, int passes = 8) {
     const int t = threadIdx.x, lane = t % GR_WARP, w = t / GR_WARP;
     constexpr int W = BT / GR_WARP;
     const uint32_t chunk = ((n + W - 1) / W + 31) & ~31u;
@@ -182,8 +183,8 @@ __device__ void block_sort(uint64_t *keys, uint32_t *vals, uint64_t *kalt, uint3
     const uint32_t lt = (1u << lane) - 1u;
     uint64_t *ka = keys, *kb = kalt;
     uint32_t *va = vals, *vb = valt;
-    for (int pass = 0; pass < 8; pass++) {
-        const int shift = 8 * pass;
+    for (int pass = 0; pass < passes; pass++) {
+        const int shift = 8 * (first_digit + pass);
         for (int d = lane; d < 256; d += GR_WARP) s_cnt[w][d] = 0;
         __syncwarp();
         for (uint32_t b = c0; b < c1; b += GR_WARP) {
@@ -260,6 +261,50 @@ __device__ void block_sort(uint64_t *keys, uint32_t *vals, uint64_t *kalt, uint3
     }
 }
 
+// The same order as an 8-pass block_sort of the full keys, in fewer passes: a
+// stable sort on the high 32 key bits (4 passes), then every run of equal high
+// words in full-key order, by one thread's in-place stable insertion sort (runs
+// of up to 64) or, one after another, by the whole block's 4-pass sort of the
+// run's low words (longer runs; their starts and lengths kept in runs[], at most
+// n / 65 pairs). The one-graph engine's tick sort, at block level.
+template <int BT>
+__device__ void block_sort_keys(uint64_t *keys, uint32_t *vals, uint64_t *kalt, uint32_t *valt, uint32_t n,
+                                uint32_t (*s_cnt)[256], uint32_t *s_tot, uint32_t *runs, uint32_t *s_nlong) {
+    block_sort<BT>(keys, vals, kalt, valt, n, s_cnt, s_tot, 4, 4);
+    if (threadIdx.x == 0) *s_nlong = 0;
+    __syncthreads();
+    for (uint32_t p = threadIdx.x; p < n; p += BT) {
+        const uint32_t hi = (uint32_t)(keys[p] >> 32);
+        if (p > 0 && (uint32_t)(keys[p - 1] >> 32) == hi) continue;        // not the start of a run
+        if (p + 1 >= n || (uint32_t)(keys[p + 1] >> 32) != hi) continue;  // a run of one
+        uint32_t r = 2;
+        while (p + r < n && (uint32_t)(keys[p + r] >> 32) == hi) r++;
+        if (r <= 64) {
+            for (uint32_t a = p + 1; a < p + r; a++) {
+                const uint64_t k = keys[a];
+                const uint32_t v = vals[a];
+                uint32_t b = a;
+                for (; b > p && keys[b - 1] > k; b--) {
+                    keys[b] = keys[b - 1];
+                    vals[b] = vals[b - 1];
+                }
+                keys[b] = k;
+                vals[b] = v;
+            }
+        } else {
+            const uint32_t q = atomicAdd(s_nlong, 1u);
+            runs[2 * q] = p;
+            runs[2 * q + 1] = r;
+        }
+    }
+    __syncthreads();
+    const uint32_t nlong = *s_nlong;
+    for (uint32_t q = 0; q < nlong; q++) {
+        const uint32_t p = runs[2 * q], r = runs[2 * q + 1];
+        block_sort<BT>(keys + p, vals + p, kalt + p, valt + p, r, s_cnt, s_tot, 0, 4);
+    }
+}
+
 template <int BT>
 __device__ __forceinline__ double block_sum_all(double v, double *s_red) {
     double r = block_sum_d<BT>(v, s_red);
@@ -301,6 +346,7 @@ __global__ void __launch_bounds__(BT) k_batch(BatchArgs A) {
     __shared__ BatchState s_st;
     __shared__ Body s_bw[32];
     __shared__ BodyDD s_carry;
+    __shared__ uint32_t s_nlong;
 
     const int t = threadIdx.x, lane = t % GR_WARP, w = t / GR_WARP;
     SlotView S;
@@ -394,7 +440,7 @@ __global__ void __launch_bounds__(BT) k_batch(BatchArgs A) {
                 S.vals[i] = i;
             }
             __syncthreads();
-            block_sort<BT>(S.keys, S.vals, S.kalt, S.valt, n, s_cnt, s_tot);
+            block_sort_keys<BT>(S.keys, S.vals, S.kalt, S.valt, n, s_cnt, s_tot, S.flag, &s_nlong);
             // ---- sorted nodes, unique keys
             for (uint32_t p = t; p < n; p += BT) {
                 const uint32_t i = S.vals[p];

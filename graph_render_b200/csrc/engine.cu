@@ -295,7 +295,8 @@ __global__ void __launch_bounds__(256) k_fix_long_runs(uint64_t *__restrict__ ke
     const uint32_t count = *long_count;
     for (uint32_t q = blockIdx.x; q < count; q += gridDim.x) {
         const uint2 r = runs[q];
-        block_sort<256>(keys + r.x, vals + r.x, kalt + r.x, valt + r.x, r.y, s_cnt, s_tot);
+        // the run's high words are equal: a stable sort of its low words (digits 0-3)
+        block_sort<256>(keys + r.x, vals + r.x, kalt + r.x, valt + r.x, r.y, s_cnt, s_tot, 0, 4);
     }
 }
 

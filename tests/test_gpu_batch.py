@@ -41,6 +41,32 @@ def test_batch_matches_the_one_graph_engine(threads):
         assert rel_extent(pos, want) < 1e-5, (g.kind, g.n)
 
 
+@pytest.mark.parametrize("dim", [2, 3])
+def test_coincident_clusters_take_the_long_run_sort(dim):
+    # clusters of 70-400 coincident points: runs of equal high key words longer
+    # than the in-place fix-up's 64, which the block sorts run by run
+    gs = []
+    rng = np.random.default_rng(7 + dim)
+    for i, (n, cl) in enumerate([(900, 300), (1500, 70), (600, 400), (2000, 130)]):
+        src = rng.integers(0, n, 3 * n).astype(np.uint32)
+        dst = rng.integers(0, n, 3 * n).astype(np.uint32)
+        pos = rng.uniform(0, 100, (n, dim)).astype(np.float32)
+        pos[:cl] = pos[0]
+        gs.append(batch.GraphSpec(n, src, dst, dict(dim=dim, theta=1.0, seed=i), None, pos, "clustered"))
+    with batch.Batch(gs) as b:
+        b.run(1)
+        got = b.positions()
+        st = b.stats()
+    assert (st["errors"] == 0).all()
+    for i, (g, pos) in enumerate(zip(gs, got)):
+        with Fa2(g.n, g.src, g.dst, params=g.params, pos0=g.pos0) as eng:
+            eng.tick(1)
+            want = eng.positions()
+            inf = eng.info()
+        assert rel_extent(pos, want) < 1e-5, g.n
+        assert (int(st["far"][i]), int(st["pair"][i])) == (inf["far_count"], inf["pair_count"]), g.n
+
+
 def test_first_tick_interactions_equal_the_one_graph_engine():
     gs = small_mix(16, seed=3)
     with batch.Batch(gs) as b:
