@@ -1774,6 +1774,7 @@ struct Adjoint {
     float *lam1 = nullptr, *lam = nullptr, *ub = nullptr, *v = nullptr, *lam_rep = nullptr, *lam_com = nullptr;
     double *lam_pair = nullptr, *xbar = nullptr, *gce = nullptr, *gs = nullptr, *graw = nullptr, *part = nullptr;
     AdjScalars *A = nullptr;
+    DevState *before = nullptr;  // the state before the tick the captured adjoint tick differentiates
     std::vector<void *> allocs;
     template <typename T>
     cudaError_t alloc(T **p, size_t count) {
@@ -1834,6 +1835,44 @@ static void adjoint_tick(gr_fa2 *h, Adjoint *a, const DevState *before) {
                                                a->lam, a->ub, a->v, a->lam_rep, a->lam_com, a->gce, a->lam1);
 }
 
+// The adjoint tick captured once into a graph (its per-tick input, the state
+// before the tick, read from a->before); retried in plain stream order if the
+// capture with programmatic launches fails.
+static int capture_adjoint(gr_fa2 *h, Adjoint *a, cudaGraph_t *g, cudaGraphExec_t *x) {
+    for (;;) {
+        *g = nullptr;
+        *x = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            if (h->dim == 3)
+                adjoint_tick<3>(h, a, a->before);
+            else
+                adjoint_tick<2>(h, a, a->before);
+            e = cudaStreamEndCapture(h->stream, g);
+            if (e == cudaSuccess) e = cudaGraphInstantiate(x, *g, 0);
+        }
+        if (e == cudaSuccess) return GR_OK;
+        cudaGetLastError();
+        if (*x) cudaGraphExecDestroy(*x);
+        if (*g) cudaGraphDestroy(*g);
+        *g = nullptr;
+        *x = nullptr;
+        if (!h->pdl) return set_err(GR_CUDA_ERROR, cudaGetErrorString(e));
+        h->pdl = false;
+        h->pdl_fell_back = true;
+    }
+}
+
+// Destroys a captured graph when the scope ends.
+struct GraphGuard {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t x = nullptr;
+    ~GraphGuard() {
+        if (x) cudaGraphExecDestroy(x);
+        if (g) cudaGraphDestroy(g);
+    }
+};
+
 extern "C" {
 
 int gr_fa2_adjoint_forward(gr_fa2 *h, uint32_t ticks, uint32_t every) {
@@ -1860,7 +1899,8 @@ int gr_fa2_adjoint_forward(gr_fa2 *h, uint32_t ticks, uint32_t every) {
         (e = a->alloc(&a->lam_rep, (size_t)n * D)) || (e = a->alloc(&a->lam_com, (size_t)n * D)) ||
         (e = a->alloc(&a->lam_pair, (size_t)n * D)) || (e = a->alloc(&a->xbar, 2 * (size_t)n * D)) ||
         (e = a->alloc(&a->gce, ne)) || (e = a->alloc(&a->gs, h->m)) || (e = a->alloc(&a->graw, h->m_raw)) ||
-        (e = a->alloc(&a->part, 3 * (size_t)div_up(n, FRC_THREADS) + 8)) || (e = a->alloc(&a->A, 1))) {
+        (e = a->alloc(&a->part, 3 * (size_t)div_up(n, FRC_THREADS) + 8)) || (e = a->alloc(&a->A, 1)) ||
+        (e = a->alloc(&a->before, 1))) {
         adjoint_release(a);
         return set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
     }
@@ -1906,7 +1946,10 @@ int gr_fa2_adjoint_backward(gr_fa2 *h, const float *dL_dpT, double *dL_dp0, doub
     CU(cudaMemcpyAsync(a->lam1, dL_dpT, (size_t)n * D * 4, cudaMemcpyHostToDevice, s));
     CU(cudaMemsetAsync(a->A, 0, sizeof(AdjScalars), s));
     CU(cudaMemsetAsync(a->gce, 0, std::max<uint64_t>(2 * h->m, 1) * sizeof(double), s));
+    GraphGuard adj;  // the adjoint tick, captured once per call
     if (n && a->done) {
+        if (int c = build_graph(h)) return c;  // the replay runs the recorded run's own tick graph
+        if (int c = capture_adjoint(h, a, &adj.g, &adj.x)) return c;
         const uint32_t nseg = (a->done + a->every - 1) / a->every;
         for (uint32_t g = nseg; g-- > 0;) {
             const uint32_t t0 = g * a->every, t1 = std::min(t0 + a->every, a->done);
@@ -1916,16 +1959,14 @@ int gr_fa2_adjoint_backward(gr_fa2 *h, const float *dL_dpT, double *dL_dp0, doub
                 CU(cudaMemcpyAsync(a->segp + (size_t)(t - t0) * n, h->pos, (size_t)n * sizeof(float4),
                                    cudaMemcpyDeviceToDevice, s));
                 CU(cudaMemcpyAsync(a->segst + (t - t0), h->st, sizeof(DevState), cudaMemcpyDeviceToDevice, s));
-                enqueue(h, false);
+                CU(cudaGraphLaunch(h->exec, s));
             }
             for (uint32_t t = t1; t-- > t0;) {
                 CU(cudaMemcpyAsync(h->pos, a->segp + (size_t)(t - t0) * n, (size_t)n * sizeof(float4),
                                    cudaMemcpyDeviceToDevice, s));
                 CU(cudaMemcpyAsync(h->st, a->segst + (t - t0), sizeof(DevState), cudaMemcpyDeviceToDevice, s));
-                if (D == 3)
-                    adjoint_tick<3>(h, a, a->segst + (t - t0));
-                else
-                    adjoint_tick<2>(h, a, a->segst + (t - t0));
+                CU(cudaMemcpyAsync(a->before, a->segst + (t - t0), sizeof(DevState), cudaMemcpyDeviceToDevice, s));
+                CU(cudaGraphLaunch(adj.x, s));
             }
         }
     }
