@@ -69,6 +69,24 @@ def walk_traffic_per_node():
         return None
 
 
+def walk_hbm_view(n: int, n_cells: int, dim: int, walk_ms: float) -> dict:
+    """The walk against the measured HBM copy bandwidth: its algorithmic bytes per
+    launch (every cell record and sorted node read once, the per-node indices read,
+    the repulsion written) over the walk phase's time."""
+    cell_bytes = 32 if dim == 2 else 48
+    algo = n_cells * cell_bytes + n * (16 + 12) + n * dim * 4
+    peak = None
+    try:
+        peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        pass
+    ach = algo / (walk_ms / 1e3) / 1e9
+    return {"bytes_per_launch": algo, "achieved": ach, "peak": peak, "unit": "GB/s",
+            "frac": (ach / peak) if peak else None,
+            "note": "cells x record size + nodes x (16 B point + 12 B indices) + nodes x dim x 4 B written; "
+                    "the walk is bound by instruction issue and load latency, not by this"}
+
+
 def workload(name: str, n: int = 0):
     from graph_render_b200 import synth
 
@@ -582,7 +600,8 @@ def run_gpu(args, dist: Dist):
                          "interactions_from": "the timed ticks replayed from their start state on a second handle "
                                               "whose walk counts them (the timed walk keeps no counters)",
                          "replay_identical": replay_identical,
-                         "flops_per_interaction": FLOPS_PER_INTERACTION[dim]},
+                         "flops_per_interaction": FLOPS_PER_INTERACTION[dim],
+                         "hbm_view": walk_hbm_view(wl.n, int(info1["n_cells"]), dim, walk_ms)},
             "cpu_baseline": cpu,
             "batched": batched,
             "adjoint": adjoint,
