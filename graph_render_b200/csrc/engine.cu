@@ -463,7 +463,9 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
             h->scanner.scan_levels_marked(h->levels, h->P, n, &st->n_unique, &st->n_cells, s, conv, h->pdl);
         else
             h->scanner.scan_levels(h->levels, h->P, n, &st->n_unique, &st->n_cells, s, conv);
-        gr_launch(h->pdl, k_assign_cells<D>, 2 * gn, 256, 0, s, st, bt, gn * 256, h->sp, h->P, h->levels,
+        // 128-thread blocks: measured faster than 256 and 512 (the 1M 3D tree by 3.5 us)
+        const uint32_t cb = div_up(n, 128);
+        gr_launch(h->pdl, k_assign_cells<D>, 2 * cb, 128, 0, s, st, bt, cb * 128, h->sp, h->P, h->levels,
                   h->leaf_start, pre, h->cells, h->leaf_pre, st);
     }
     if (h->timing_events) cudaEventRecordWithFlags(h->ev[1], s, cudaEventRecordExternal);

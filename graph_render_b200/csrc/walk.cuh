@@ -21,7 +21,7 @@
 
 namespace gr {
 
-constexpr int WALK_THREADS = 128;
+constexpr int WALK_THREADS = 256;  // measured at 1M 2D nodes: 64 and 128 threads slower (by 3.5% / 1.6% of the walk)
 
 struct WalkParams {
     uint32_t n;
