@@ -327,7 +327,7 @@ def run_batched(args, dist: Dist):
         "graphs": dist.world * len(graphs), "nodes_per_gpu": nodes, "ticks": args.batched_ticks,
         "ms": ms_max, "cta_threads": chosen, "tune_ms": tune_ms, "create_s": create_s,
         "one_by_one": {"value": one_rate, "unit": "graphs/s", "sample": len(pick),
-                       "how": "the one-graph engine (captured tick graph, 22 kernels a tick) per graph, "
+                       "how": "the one-graph engine (one captured tick graph) per graph, "
                               "inputs resident, timed over the same 200 ticks"},
         "speedup_vs_one_by_one": (rate / dist.world) / one_rate if one_rate else None,
         "converged_graphs": int((st["ticks"] < warm + args.batched_ticks).sum()),
