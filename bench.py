@@ -601,6 +601,9 @@ def run_gpu(args, dist: Dist):
                                               "whose walk counts them (the timed walk keeps no counters)",
                          "replay_identical": replay_identical,
                          "flops_per_interaction": FLOPS_PER_INTERACTION[dim],
+                         "flops_convention": "operations per interaction, an FMA counted once (the peak counts it "
+                                             "twice); with FMAs as 2 flops and the hi/lo centre subtractions, "
+                                             "15 in 2D",
                          "hbm_view": walk_hbm_view(wl.n, int(info1["n_cells"]), dim, walk_ms)},
             "cpu_baseline": cpu,
             "batched": batched,
