@@ -358,7 +358,7 @@ static void keys_sort_fast(gr_fa2 *h, cudaStream_t s) {
     const uint32_t n = h->n;
     const uint32_t *conv = &h->st->converged;
     if (n < (1u << 30)) {
-        const uint32_t nt = div_up(n, OS_T * OS_I);
+        const uint32_t nt = div_up(n, os_tile_keys(n));
         gr_launch(h->pdl, k_keys_hist<D>, std::min<uint32_t>(div_up(n, OS_HIST_THREADS * 4), 4 * 148),
                   OS_HIST_THREADS, 0, s, h->pos, n, h->st, h->keys, h->vals, h->sorter.os_ghist, h->sorter.os_status,
                   (uint64_t)4 * nt * RS_BINS);

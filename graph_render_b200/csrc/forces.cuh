@@ -19,8 +19,8 @@ namespace gr {
 
 constexpr int FRC_THREADS = 256;
 // k_forces and k_update stride over the nodes with at most FRC_MAX_BLOCKS
-// blocks (8 per SM): fewer per-block partials and last-block tickets.
-constexpr uint32_t FRC_MAX_BLOCKS = 8 * 148;
+// blocks (4 per SM): fewer per-block partials and last-block tickets.
+constexpr uint32_t FRC_MAX_BLOCKS = 4 * 148;  // measured: 8 and 16 per SM slower (3 and 8 us at 1M nodes)
 
 __host__ __device__ inline uint32_t frc_blocks(uint32_t n) {
     const uint32_t b = (n + FRC_THREADS - 1) / FRC_THREADS;
