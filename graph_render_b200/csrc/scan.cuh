@@ -8,8 +8,8 @@
 
 namespace gr {
 
-constexpr int SC_THREADS = 256;
-constexpr int SC_ITEMS = 8;
+constexpr int SC_THREADS = 512;  // 512 x 4: the 1M-node tick's cell-level scan 2 us faster than 256 x 8
+constexpr int SC_ITEMS = 4;
 constexpr int SC_TILE = SC_THREADS * SC_ITEMS;
 
 __device__ __forceinline__ uint32_t scan_count(uint32_t n_host, const uint32_t *n_dev, uint32_t add) {
