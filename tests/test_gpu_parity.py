@@ -184,6 +184,23 @@ def test_walk_without_interaction_counts_gives_the_same_forces_and_run(dim):
     assert np.array_equal(ends[0], ends[1])
 
 
+@pytest.mark.parametrize("dim", [2, 3])
+def test_programmatic_launches_give_the_same_run(dim, monkeypatch):
+    # each tick kernel waits for the one before it in gr_pdl_enter: the ticks are
+    # those of plain stream order bit for bit (GR_PDL=0 is read at create)
+    wl = synth.powerlaw_1m(n=200_000, dim=dim)
+    ends = []
+    for pdl in ("1", "0"):
+        monkeypatch.setenv("GR_PDL", pdl)
+        with Fa2(wl.n, wl.src, wl.dst, params=wl.params, pos0=wl.pos0) as eng:
+            assert eng.programmatic_launches() == (pdl == "1")
+            eng.tick(4)
+            ends.append((eng.positions(), eng.forces(), eng.info()["far_count"]))
+    assert np.array_equal(ends[0][0], ends[1][0])
+    assert np.array_equal(ends[0][1], ends[1][1])
+    assert ends[0][2] == ends[1][2]
+
+
 def _full_sort_forces(n, src, dst, pos, prm):
     """Forces through gr_fa2_forces_static, which sorts the whole 64-bit key
     (8 passes) where a handle sorts the high word and fixes the runs."""
