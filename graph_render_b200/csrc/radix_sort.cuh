@@ -213,18 +213,20 @@ constexpr uint32_t OS_FLAG_A = 1u << 30, OS_FLAG_P = 2u << 30, OS_COUNT = (1u <<
 constexpr uint32_t OS_SPIN_LIMIT = 1u << 22;  // x 32 ns sleeps: ~0.1 s
 
 // The tile shape the engine uses: T threads x I keys, look-back window L
-// (on B200 at 1M keys: 512 x 8 sorts 4 digits in 78 us, 256 x 8 in 105 us; in the
-// 1M-node tick, 1024 x 8 takes 7.5 us less than 512 x 8, 512 x 16 2 us less, 256 x 16 4 us more).
+// (on B200 at 1M keys: 512 x 8 sorts 4 digits in 78 us, 256 x 8 in 105 us).
 constexpr int OS_T = 512, OS_I = 8, OS_L = 8;
-// From this many keys up the passes take tiles of OS_BIG_T x OS_I keys: fewer
-// tiles to look back over (in the 1M-node tick 7.5 us less than 512 x 8 over the
-// 4 passes); below it the smaller tiles keep more blocks busy.
-constexpr int OS_BIG_T = 1024;
+// From this many keys up the passes take tiles of OS_BIG_T x OS_BIG_I keys: fewer
+// tiles to look back over, and at 1M keys 145 tiles of one block per SM, one wave
+// on 148 SMs. In the 1M-node tick's 4 passes, against 512 x 8: 768 x 9 15 us less,
+// 1024 x 8 and 768 x 10 7.5 us less, 1024 x 7 11 us less; 768 x 8, 1024 x 6 and
+// 512 x 12 (163 tiles) 10-15 us more. Below it the smaller tiles keep more blocks
+// busy (larger ones made small graphs' one-tile sorts slower).
+constexpr int OS_BIG_T = 768, OS_BIG_I = 9;
 constexpr uint32_t OS_BIG_MIN = 1u << 19;
 
 // Keys per one-sweep tile for a sort of n keys.
 __host__ __device__ inline uint32_t os_tile_keys(uint32_t n) {
-    return (n >= OS_BIG_MIN ? OS_BIG_T : OS_T) * OS_I;
+    return n >= OS_BIG_MIN ? OS_BIG_T * OS_BIG_I : OS_T * OS_I;
 }
 
 
@@ -504,23 +506,24 @@ struct RadixSorter {
                          uint32_t *err, const uint32_t *skip = nullptr, bool pdl = false) {
         if (n == 0) return;
         if (n >= OS_BIG_MIN)
-            passes_shaped<OS_BIG_T>(keys, vals, n, first_digit, passes, s, err, skip, pdl);
+            passes_shaped<OS_BIG_T, OS_BIG_I>(keys, vals, n, first_digit, passes, s, err, skip, pdl);
         else
-            passes_shaped<OS_T>(keys, vals, n, first_digit, passes, s, err, skip, pdl);
+            passes_shaped<OS_T, OS_I>(keys, vals, n, first_digit, passes, s, err, skip, pdl);
     }
 
-    template <int T>
+    template <int T, int I>
     void passes_shaped(uint64_t *keys, uint32_t *vals, uint32_t n, int first_digit, int passes, cudaStream_t s,
                        uint32_t *err, const uint32_t *skip, bool pdl) {
-        const uint32_t nt = div_up(n, T * OS_I);
-        constexpr size_t smem = os_smem<uint32_t, T, OS_I>();
+        static_assert(T * I >= OS_T * OS_I, "os_tiles counts tiles of the smallest shape");
+        const uint32_t nt = div_up(n, T * I);
+        constexpr size_t smem = os_smem<uint32_t, T, I>();
         if (smem > 48 * 1024)
-            cudaFuncSetAttribute(os_pass<uint32_t, T, OS_I, OS_L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(os_pass<uint32_t, T, I, OS_L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
         uint64_t *ka = keys, *kb = k_alt;
         uint32_t *va = vals, *vb = v_alt;
         for (int p = 0; p < passes; p++) {
-            gr_launch(pdl, os_pass<uint32_t, T, OS_I, OS_L>, nt, T, smem, s, ka, (const uint32_t *)va, kb, vb, n,
+            gr_launch(pdl, os_pass<uint32_t, T, I, OS_L>, nt, T, smem, s, ka, (const uint32_t *)va, kb, vb, n,
                       8 * (first_digit + p), (const uint32_t *)(os_ghist + p * RS_BINS),
                       os_status + (size_t)p * nt * RS_BINS, os_ghist + OS_MAX_PASSES * RS_BINS + p, err, skip);
             std::swap(ka, kb);
