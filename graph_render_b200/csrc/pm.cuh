@@ -81,16 +81,40 @@ k_pm_bounds(uint32_t n, const float4 *__restrict__ p, uint32_t side, double dmax
         q[5] = sy;
     }
     if (!last_block_done(&S->ticket, &s_last)) return;
-    if (threadIdx.x != 0) return;
-    double L0 = INFINITY, L1 = INFINITY, H0 = -INFINITY, H1 = -INFINITY, X = 0.0, Y = 0.0;
-    for (uint32_t b = 0; b < gridDim.x; b++) {
+    // the last block folds the partials: thread t takes blocks t, t + PM_T, ... in
+    // order, then the block combines the threads (min / max exact in any order, the
+    // sums in block_sum_d's fixed shape)
+    double L0 = INFINITY, L1 = INFINITY, H0 = -INFINITY, H1 = -INFINITY;
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += PM_T) {
         const double *q = part + (size_t)b * 6;
-        L0 = fmin(L0, q[0]);
-        L1 = fmin(L1, q[1]);
-        H0 = fmax(H0, q[2]);
-        H1 = fmax(H1, q[3]);
-        X += q[4];
-        Y += q[5];
+        L0 = fmin(L0, __ldcg(q + 0));
+        L1 = fmin(L1, __ldcg(q + 1));
+        H0 = fmax(H0, __ldcg(q + 2));
+        H1 = fmax(H1, __ldcg(q + 3));
+    }
+    double X = strided_sum_cg<PM_T>(part, gridDim.x, 6, 4);
+    double Y = strided_sum_cg<PM_T>(part, gridDim.x, 6, 5);
+    for (int o = 16; o > 0; o >>= 1) {
+        L0 = fmin(L0, __shfl_xor_sync(GR_FULL, L0, o));
+        L1 = fmin(L1, __shfl_xor_sync(GR_FULL, L1, o));
+        H0 = fmax(H0, __shfl_xor_sync(GR_FULL, H0, o));
+        H1 = fmax(H1, __shfl_xor_sync(GR_FULL, H1, o));
+    }
+    __syncthreads();  // s_m is reused
+    if (l == 0) {
+        s_m[0][w] = L0;
+        s_m[1][w] = L1;
+        s_m[2][w] = H0;
+        s_m[3][w] = H1;
+    }
+    X = block_sum_d<PM_T>(X, s_red);
+    Y = block_sum_d<PM_T>(Y, s_red);
+    if (threadIdx.x != 0) return;
+    for (int k = 1; k < PM_T / GR_WARP; k++) {
+        L0 = fmin(L0, s_m[0][k]);
+        L1 = fmin(L1, s_m[1][k]);
+        H0 = fmax(H0, s_m[2][k]);
+        H1 = fmax(H1, s_m[3][k]);
     }
     S->lo[0] = L0;
     S->lo[1] = L1;
