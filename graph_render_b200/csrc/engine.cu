@@ -2233,7 +2233,9 @@ void pm_enqueue(gr_force_session *S) {
     const double dmax2 = S->prm.distance_max * S->prm.distance_max;
     k_pm_bounds<<<S->pm_blocks, PM_T, 0, s>>>(n, S->p4, side, S->prm.distance_max, dmax2, S->pm_part, S->pm);
     k_pm_stencil<<<g, PM_T, 0, s>>>(n, S->p4, S->pm, side, S->pm_key, S->pm_val, S->pm_frac);
-    S->pm_sorter.sort(S->pm_key, S->pm_val, n, 32, s);
+    // cell keys are row-major indices below side^2: 2 x bits significant bits, one-sweep
+    // passes (a wait that gives up is reported through the tree handle's state)
+    S->pm_sorter.sort_bits(S->pm_key, S->pm_val, n, 2 * (int)S->bits, s, &S->t->st->error);
     cudaMemsetAsync(S->pm_cs, 0, (size_t)side * side * 4, s);
     cudaMemsetAsync(S->pm_ce, 0, (size_t)side * side * 4, s);
     k_pm_mark<<<g, PM_T, 0, s>>>(n, S->pm, S->pm_key, S->pm_cs, S->pm_ce);
