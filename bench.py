@@ -3,14 +3,18 @@
 
 A step is one FA2 tick over the whole graph (tree build, repulsion walk,
 attraction, gravity, FP64 swing/traction, speed, update). The default workload
-is the 1M-node power-law configuration-model graph laid out in 2D (theta 1.2),
-the north-star size; every rank runs its own replica (weak scaling: the single
-graph has no exchange step to shard).
+is the 1M-node power-law configuration-model graph laid out in 2D (theta 1.2);
+every rank runs its own replica (weak scaling: the single graph has no exchange
+step to shard).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-One JSON line on rank 0. See DESIGN.md for the definitions of the roofline
-numbers and the CPU baseline.
+One JSON line on rank 0. The roofline block is the repulsion walk's: its
+algorithmic FLOPs (10 operations per far-cell or exact-pair interaction, the
+interactions counted on a replay of the timed ticks) over its CUDA-event time,
+against the nominal FP32 FMA rate, and its algorithmic bytes against the
+measured HBM copy bandwidth. The CPU baseline is the FP64 restatement of the
+reference's tick (the oracle) on this host's cores, over a bounded sample of ticks.
 """
 
 from __future__ import annotations
