@@ -43,6 +43,8 @@ struct DevState {
     uint32_t n_unique;                                // distinct Morton keys this tick
     uint32_t n_cells;                                 // tree cells this tick
     uint32_t error;                                   // device error bits
+    uint32_t bounds_stamp;                            // iter_no + 1 when root0 / root_w / mean are the
+                                                      // current positions' (the update wrote them); else 0
     uint32_t counters[7];                             // last-block-done tickets
 };
 

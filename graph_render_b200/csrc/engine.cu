@@ -158,6 +158,7 @@ struct gr_fa2 {
     Cells cells{};
     float *rep = nullptr, *U = nullptr;
     double *part = nullptr;
+    double *bpart = nullptr;  // the update's per-block bounds records (the next tick's bounds)
     DevState *st = nullptr;
     RadixSorter sorter;
     Scanner scanner;
@@ -227,7 +228,8 @@ struct gr_fa2 {
             cudaStreamDestroy(stream);
         }
     }
-    uint32_t bnd_blocks() const { return std::max<uint32_t>(1, std::min<uint32_t>(div_up(n, BND_THREADS), 592)); }
+    // k_bounds runs k_update's grid, so that the update can compute the same bounds
+    uint32_t bnd_blocks() const { return frc_blocks(n); }
 };
 
 static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
@@ -273,6 +275,7 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
     A(h->U, (size_t)n * D);
     size_t np = std::max<size_t>((size_t)h->bnd_blocks() * 3 * D, 2 * (size_t)div_up(n, FRC_THREADS)) + 8;
     A(h->part, np);
+    A(h->bpart, (size_t)frc_blocks(n) * 3 * D + 8);
 #undef A
     if ((e = h->sorter.init(n, h->stream, true))) return e;
     if ((e = h->scanner.init(n, h->stream, true))) return e;
@@ -508,7 +511,8 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
         k_forces<D><<<frc_blocks(n), FRC_THREADS, 0, s>>>(fp, st, h->pos, h->rep, h->U, h->part,
                                                                     forces_only ? 0 : 1);
         if (!forces_only)
-            gr_launch(h->pdl, k_update<D>, frc_blocks(n), FRC_THREADS, 0, s, n, st, h->pos, h->U, h->part);
+            gr_launch(h->pdl, k_update<D>, frc_blocks(n), FRC_THREADS, 0, s, n, st, h->pos, h->U, h->part,
+                      h->bpart);
     }
     if (h->timing_events) cudaEventRecordWithFlags(h->ev[3], s, cudaEventRecordExternal);
 }
@@ -1028,6 +1032,8 @@ int gr_fa2_set_positions(gr_fa2 *h, const float *pos) {
     else
         k_import<2><<<div_up(h->n, 256), 256, 0, h->stream>>>(h->n, h->pos, d);
     cudaFreeAsync(d, h->stream);
+    // the bounds the last update computed are not these positions'
+    cudaMemsetAsync(&h->st->bounds_stamp, 0, sizeof(uint32_t), h->stream);
     CU(cudaStreamSynchronize(h->stream));
     return ok();
 }

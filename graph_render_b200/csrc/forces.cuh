@@ -14,6 +14,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "tree.cuh"
 
 namespace gr {
 
@@ -253,26 +254,47 @@ k_forces(ForceParams P, DevState *st, const float4 *__restrict__ pos, const floa
 }
 
 // The update for every node; FP64 sum of |step| decides the 1e-10 early exit
-// (state.rs:122-128).
+// (state.rs:122-128). With bpart, the same pass also takes the new positions'
+// extent and FP64 sums (bounds_block / bounds_finish over k_bounds' grid and
+// per-thread order, so the same bits k_bounds would get) into the root square
+// and mean of the next tick, and stamps them valid for it.
+static_assert(FRC_THREADS == BND_THREADS, "k_update and k_bounds share one grid shape");
 template <int D>
 __global__ void __launch_bounds__(FRC_THREADS)
 k_update(uint32_t n, DevState *st, float4 *__restrict__ pos, const float *__restrict__ U,
-         double *__restrict__ part) {
+         double *__restrict__ part, double *__restrict__ bpart) {
     gr_pdl_enter();
     if (st->converged) return;
     __shared__ double s_red[32];
+    __shared__ float s_f[2 * D][32];
     __shared__ bool s_last;
     double step = 0.0;
     bool bad = false;
     const double speed = st->speed;
+    float lo[D], hi[D];
+    double sum[D];
+#pragma unroll
+    for (int a = 0; a < D; a++) {
+        lo[a] = INFINITY;
+        hi[a] = -INFINITY;
+        sum[a] = 0.0;
+    }
     for (uint32_t i = blockIdx.x * FRC_THREADS + threadIdx.x; i < n; i += gridDim.x * FRC_THREADS) {
         float4 p = pos[i];
         bool b;
         step += node_update<D>(p, U + (size_t)i * D, speed, b);
         bad = bad || b;
         pos[i] = p;
+        const float c[3] = {p.x, p.y, p.z};
+#pragma unroll
+        for (int a = 0; a < D; a++) {
+            lo[a] = fminf(lo[a], c[a]);
+            hi[a] = fmaxf(hi[a], c[a]);
+            sum[a] += (double)c[a];
+        }
     }
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&st->error, (uint32_t)ERR_NONFINITE);
+    if (bpart) bounds_block<D>(lo, hi, sum, bpart, s_red, s_f);
     step = block_sum_d<FRC_THREADS>(step, s_red);
     if (threadIdx.x == 0) part[blockIdx.x] = step;
     if (!last_block_done(&st->counters[2], &s_last)) return;
@@ -282,6 +304,10 @@ k_update(uint32_t n, DevState *st, float4 *__restrict__ pos, const float *__rest
         st->moved = a;
         st->iter_no += 1;
         if (a < 1e-10 || st->error) st->converged = 1;
+    }
+    if (bpart) {
+        bounds_finish<D>(bpart, n, st, s_red);
+        if (threadIdx.x == 0) st->bounds_stamp = st->iter_no + 1u;
     }
 }
 

@@ -120,53 +120,12 @@ struct ZeroWords {
     }
 };
 
-// Extent and FP64 coordinate sums of the positions; the last block turns them
-// into the root square (quadtree.rs:157-195 cover, both corners) and the mean
-// gravity pulls toward (state.rs:208-218).
+// A block's extent and FP64 coordinate sums of this thread's positions (lo, hi,
+// sum, accumulated over its strided nodes in order): warp shuffles for min / max,
+// block_sum_d for the sums, one record of 3 D doubles per block in part.
 template <int D>
-__global__ void __launch_bounds__(BND_THREADS)
-k_bounds(const float4 *__restrict__ pos, uint32_t n, DevState *st, double *__restrict__ part, ZeroWords zw) {
-    gr_pdl_enter();
-    if (st->converged) return;
-    if (blockIdx.x == 0) zw.clear();
-    __shared__ double s_red[32];
-    __shared__ float s_f[2 * D][32];
-    __shared__ bool s_last;
-    float lo[D], hi[D];
-    double sum[D];
-#pragma unroll
-    for (int a = 0; a < D; a++) {
-        lo[a] = INFINITY;
-        hi[a] = -INFINITY;
-        sum[a] = 0.0;
-    }
-    bool bad = false;
-    // this thread's points i0, i0 + stride, ... in order, BND_U loads in flight
-    constexpr int BND_U = 4;
-    const uint64_t stride = (uint64_t)gridDim.x * BND_THREADS;
-    for (uint64_t i0 = blockIdx.x * BND_THREADS + threadIdx.x; i0 < n; i0 += stride * BND_U) {
-        float4 pv[BND_U];
-#pragma unroll
-        for (int u = 0; u < BND_U; u++) {
-            const uint64_t i = i0 + u * stride;
-            pv[u] = i < n ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-#pragma unroll
-        for (int u = 0; u < BND_U; u++) {
-            if (i0 + u * stride >= n) break;
-            const float c[3] = {pv[u].x, pv[u].y, pv[u].z};
-#pragma unroll
-            for (int a = 0; a < D; a++) {
-                if (!isfinite(c[a])) bad = true;
-                lo[a] = fminf(lo[a], c[a]);
-                hi[a] = fmaxf(hi[a], c[a]);
-                sum[a] += (double)c[a];
-            }
-        }
-    }
-    if (__syncthreads_or(bad)) {
-        if (threadIdx.x == 0) atomicOr(&st->error, (uint32_t)ERR_NONFINITE);
-    }
+__device__ __forceinline__ void bounds_block(const float *lo, const float *hi, const double *sum,
+                                             double *__restrict__ part, double *s_red, float (*s_f)[32]) {
     const int lane = threadIdx.x % GR_WARP, w = threadIdx.x / GR_WARP;
 #pragma unroll
     for (int a = 0; a < D; a++) {
@@ -197,8 +156,14 @@ k_bounds(const float4 *__restrict__ pos, uint32_t n, DevState *st, double *__res
             q[2 * D + a] = tot[a];
         }
     }
-    if (!last_block_done(&st->counters[0], &s_last)) return;
-    // last block: fold the partials in block order
+}
+
+// The grid's last block: the block records folded in block order into the
+// reference's root square (quadtree.rs:157-195 cover, both corners) and the
+// mean gravity pulls toward (state.rs:208-218).
+template <int D>
+__device__ __forceinline__ void bounds_finish(const double *part, uint32_t n, DevState *st, double *s_red) {
+    const int lane = threadIdx.x % GR_WARP, w = threadIdx.x / GR_WARP;
     double gl[D], gh[D], gs[D];
 #pragma unroll
     for (int a = 0; a < D; a++) {
@@ -250,6 +215,61 @@ k_bounds(const float4 *__restrict__ pos, uint32_t n, DevState *st, double *__res
         for (int a = 0; a < D; a++) st->mean[a] = S[a] / (double)n;
         if (st->error) st->converged = 1;
     }
+}
+
+// Extent and FP64 coordinate sums of the positions into the root square and the
+// mean. When the previous tick's update already computed them from these
+// positions (bounds_stamp == iter_no + 1, bounds_block / bounds_finish over the
+// same grid and the same per-thread order, so bit for bit the same), only the
+// counters are zeroed. A grid of frc_blocks(n) blocks (the update's grid).
+template <int D>
+__global__ void __launch_bounds__(BND_THREADS)
+k_bounds(const float4 *__restrict__ pos, uint32_t n, DevState *st, double *__restrict__ part, ZeroWords zw) {
+    gr_pdl_enter();
+    if (st->converged) return;
+    if (blockIdx.x == 0) zw.clear();
+    if (st->bounds_stamp == st->iter_no + 1u) return;
+    __shared__ double s_red[32];
+    __shared__ float s_f[2 * D][32];
+    __shared__ bool s_last;
+    float lo[D], hi[D];
+    double sum[D];
+#pragma unroll
+    for (int a = 0; a < D; a++) {
+        lo[a] = INFINITY;
+        hi[a] = -INFINITY;
+        sum[a] = 0.0;
+    }
+    bool bad = false;
+    // this thread's points i0, i0 + stride, ... in order, BND_U loads in flight
+    constexpr int BND_U = 4;
+    const uint64_t stride = (uint64_t)gridDim.x * BND_THREADS;
+    for (uint64_t i0 = blockIdx.x * BND_THREADS + threadIdx.x; i0 < n; i0 += stride * BND_U) {
+        float4 pv[BND_U];
+#pragma unroll
+        for (int u = 0; u < BND_U; u++) {
+            const uint64_t i = i0 + u * stride;
+            pv[u] = i < n ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < BND_U; u++) {
+            if (i0 + u * stride >= n) break;
+            const float c[3] = {pv[u].x, pv[u].y, pv[u].z};
+#pragma unroll
+            for (int a = 0; a < D; a++) {
+                if (!isfinite(c[a])) bad = true;
+                lo[a] = fminf(lo[a], c[a]);
+                hi[a] = fmaxf(hi[a], c[a]);
+                sum[a] += (double)c[a];
+            }
+        }
+    }
+    if (__syncthreads_or(bad)) {
+        if (threadIdx.x == 0) atomicOr(&st->error, (uint32_t)ERR_NONFINITE);
+    }
+    bounds_block<D>(lo, hi, sum, part, s_red, s_f);
+    if (!last_block_done(&st->counters[0], &s_last)) return;
+    bounds_finish<D>(part, n, st, s_red);
 }
 
 // Morton key of every node in the root square: per axis q = floor((x - x0) *

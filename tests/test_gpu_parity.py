@@ -201,6 +201,24 @@ def test_programmatic_launches_give_the_same_run(dim, monkeypatch):
     assert ends[0][2] == ends[1][2]
 
 
+@pytest.mark.parametrize("dim", [2, 3])
+def test_update_bounds_equal_the_bounds_pass(dim):
+    # a tick's update also computes the next tick's root square and mean; setting
+    # the positions again makes the bounds pass recompute them: the runs agree bit
+    # for bit
+    wl = synth.powerlaw_1m(n=150_000, dim=dim)
+    ends = []
+    for reset in (False, True):
+        with Fa2(wl.n, wl.src, wl.dst, params=wl.params, pos0=wl.pos0) as eng:
+            eng.tick(3)
+            if reset:
+                eng.set_positions(eng.positions())
+            eng.tick(3)
+            ends.append((eng.positions(), eng.info()["moved"]))
+    assert np.array_equal(ends[0][0], ends[1][0])
+    assert ends[0][1] == ends[1][1]
+
+
 def _full_sort_forces(n, src, dst, pos, prm):
     """Forces through gr_fa2_forces_static, which sorts the whole 64-bit key
     (8 passes) where a handle sorts the high word and fixes the runs."""
