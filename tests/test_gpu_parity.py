@@ -101,6 +101,16 @@ def test_large_2d_forces_with_one_block_tile_carries():
     assert abs(info["far_count"] - sc["far"]) <= 1e-3 * sc["far"]
 
 
+def test_forces_past_the_one_pass_scan_limit():
+    # past 2,048 scan blocks of 2,048 leaves (~4.2M distinct keys) the cell-level
+    # scan runs as reduce / block-scan / downsweep, and the tile carries come from
+    # one block: both fallbacks against the oracle
+    wl = synth.powerlaw_1m(n=4_500_000, dim=2)
+    rel, info, sc = _check(wl.n, wl.src, wl.dst, None, wl.pos0, wl.params)
+    assert info["n_leaves"] > 2048 * 2048
+    assert abs(info["far_count"] - sc["far"]) <= 1e-3 * sc["far"]
+
+
 def test_run_is_deterministic():
     wl = synth.sbm_1500()
     outs = []
