@@ -440,14 +440,14 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
             h->sorter.sort(h->keys, h->vals, n, 64, s, conv);
         }
         gr_launch(h->pdl, k_leaf_tiles<D>, ab, AG_T, 0, s, st, n, h->pos, h->keys, h->vals, h->sp, h->sorig,
-                  h->tile_sum, h->tile_cnt);
+                  h->tile_sum, h->tile_cnt, h->uid, h->pre_local);
         const uint32_t *ccarry = nullptr;  // the carries come from one block above LEAF_FOLD_MAX_TILES tiles
         if (ab > LEAF_FOLD_MAX_TILES) {
             k_leaf_carry<D><<<1, CARRY_T, 0, s>>>(st, n, h->tile_sum, h->tile_cnt, h->tile_carry, h->tile_cnt + ab,
                                                   h->leaf_start, h->pre_local);
             ccarry = h->tile_cnt + ab;
         }
-        gr_launch(h->pdl, k_leaf_prefix<D>, ab, AG_T, 0, s, st, n, h->sp, h->keys, h->tile_sum, h->tile_cnt,
+        gr_launch(h->pdl, k_leaf_prefix<D>, ab, AG_T, 0, s, st, n, h->keys, h->tile_sum, h->tile_cnt,
                   h->tile_carry, ccarry, h->uid, h->leaf_start, h->ukey, h->levels, h->pre_local);
         const Prefix pre{h->pre_local, h->tile_carry, h->leaf_start, 0u, ab};  // nu: read on the device
         const bool adjoint = h->bt.cell_of != nullptr;  // the adjoint reads leaf and node bodies as arrays

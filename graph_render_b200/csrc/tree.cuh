@@ -620,11 +620,12 @@ __device__ __forceinline__ void block_scan_body(const Body &x, uint32_t c, Body 
 }
 
 // The stored prefix of leaf s: the FP64 in-tile part, D + 1 doubles (the mass,
-// then the D mass moments; 24 B in 2D), beside the double-double carry of the
-// tile that holds the leaf's first point (carry[nt] is the grand total, and
-// leaf nu has in-tile part 0). The prefix is carry + in-tile part.
+// then the D mass moments; 24 B in 2D) stored at the leaf's first point, beside
+// the double-double carry of the tile that holds that point (carry[nt] is the
+// grand total, and point n, leaf nu's start, has in-tile part 0). The prefix is
+// carry + in-tile part.
 struct Prefix {
-    const double *local;  // (nu + 1) x (D + 1)
+    const double *local;  // (n + 1) x (D + 1), at each leaf's first point (and 0 at point n)
     const BodyDD *carry;  // nt + 1
     const uint32_t *leaf_start;
     uint32_t nu, nt;
@@ -641,9 +642,10 @@ __device__ __forceinline__ void local_put(double *__restrict__ pre, uint32_t s, 
 
 template <int D>
 __device__ __forceinline__ BodyDD prefix_at(const Prefix &P, uint32_t s) {
-    const double *q = P.local + (size_t)s * (D + 1);
+    const uint32_t p = P.leaf_start[s];  // leaf_start[nu] = n
+    const double *q = P.local + (size_t)p * (D + 1);
     const Body b{q[0], q[1], q[2], D == 3 ? q[3] : 0.0};
-    const uint32_t tile = s >= P.nu ? P.nt : P.leaf_start[s] / AG_TILE;
+    const uint32_t tile = s >= P.nu ? P.nt : p / AG_TILE;
     return bdd_add_body<D>(P.carry[tile], b);
 }
 
@@ -676,7 +678,8 @@ template <int D>
 __global__ void __launch_bounds__(AG_T)
 k_leaf_tiles(DevState *st, uint32_t n, const float4 *__restrict__ pos, const uint64_t *__restrict__ keys,
              const uint32_t *__restrict__ perm, float4 *__restrict__ sp, uint32_t *__restrict__ sorig,
-             Body *__restrict__ tile_sum, uint32_t *__restrict__ tile_cnt) {
+             Body *__restrict__ tile_sum, uint32_t *__restrict__ tile_cnt, uint32_t *__restrict__ uid,
+             double *__restrict__ pre) {
     gr_pdl_enter();
     if (st->converged) return;
     __shared__ Body s_w[2 * AG_W];
@@ -710,6 +713,24 @@ k_leaf_tiles(DevState *st, uint32_t n, const float4 *__restrict__ pos, const uin
     if (threadIdx.x == 0) {
         tile_sum[b] = total;
         tile_cnt[b] = tcnt;
+    }
+    // at each leaf's first point, the in-tile part of its prefix (indexed by the
+    // point: it needs no carry); every point's in-tile leaf rank + 1 (0: its leaf
+    // began in an earlier tile), bit 31 set at a leaf's first point
+    uint32_t e = exc;
+    Body run = ex;
+#pragma unroll
+    for (int r = 0; r < AG_I; r++) {
+        const uint32_t p = p0 + r;
+        if (p < n) {
+            const bool f = (fl >> r) & 1u;
+            if (f) {
+                local_put<D>(pre, p, run);
+                e++;
+            }
+            uid[p] = e | (f ? 0x80000000u : 0u);
+            run = body_sum<D>(run, point_body<D>(pt[r]));
+        }
     }
 }
 
@@ -868,34 +889,28 @@ k_leaf_carry(DevState *st, uint32_t n, const Body *__restrict__ tile_sum, const 
         st->n_unique = nu;
         leaf_start[nu] = n;
         carry[nt] = run;
-        local_put<D>(pre, nu, Body{0.0, 0.0, 0.0, 0.0});
+        local_put<D>(pre, n, Body{0.0, 0.0, 0.0, 0.0});  // the in-tile part at leaf_start[nu] = n
     }
 }
 
 // (2 of 2) Tile b again: the double-double carry of the tiles before it (its
 // own fold of their sums, tiles_before, or with ccarry k_leaf_carry's, for
-// more than LEAF_FOLD_MAX_TILES tiles); every point's leaf index uid[p]; at a
-// leaf's first point leaf_start, ukey, an empty cell level mask and the
-// in-tile part of its prefix (the FP64 in-tile exclusive prefix of the terms).
-// The last tile also writes n_unique, leaf_start[n_unique] = n, the grand total
-// as carry[nt] and a zero in-tile part for leaf n_unique.
+// more than LEAF_FOLD_MAX_TILES tiles); every point's leaf index uid[p] (its
+// in-tile rank from k_leaf_tiles plus the leaves before the tile); at a leaf's
+// first point leaf_start, ukey and an empty cell level mask. The last tile also
+// writes n_unique, leaf_start[n_unique] = n, the grand total as carry[nt] and a
+// zero in-tile part at point n.
 template <int D>
 __global__ void __launch_bounds__(AG_T)
-k_leaf_prefix(DevState *st, uint32_t n, const float4 *__restrict__ sp, const uint64_t *__restrict__ keys,
-              const Body *__restrict__ tile_sum, const uint32_t *__restrict__ tile_cnt, BodyDD *__restrict__ carry,
-              const uint32_t *__restrict__ ccarry, uint32_t *__restrict__ uid, uint32_t *__restrict__ leaf_start,
-              uint64_t *__restrict__ ukey, uint32_t *__restrict__ levels, double *__restrict__ pre) {
+k_leaf_prefix(DevState *st, uint32_t n, const uint64_t *__restrict__ keys, const Body *__restrict__ tile_sum,
+              const uint32_t *__restrict__ tile_cnt, BodyDD *__restrict__ carry, const uint32_t *__restrict__ ccarry,
+              uint32_t *__restrict__ uid, uint32_t *__restrict__ leaf_start, uint64_t *__restrict__ ukey,
+              uint32_t *__restrict__ levels, double *__restrict__ pre) {
     gr_pdl_enter();
     if (st->converged) return;
-    __shared__ Body s_w[2 * AG_W];
-    __shared__ uint32_t s_c[2 * AG_W];
     __shared__ BodyDD s_bw[AG_W + 1];
     __shared__ uint32_t s_bc[AG_W + 1];
     const uint32_t b = blockIdx.x;
-    const uint32_t p0 = b * AG_TILE + threadIdx.x * AG_I;
-    float4 pt[AG_I];
-#pragma unroll
-    for (int r = 0; r < AG_I; r++) pt[r] = p0 + r < n ? sp[p0 + r] : make_float4(0.f, 0.f, 0.f, 0.f);
     BodyDD cb;
     uint32_t cbefore;
     if (ccarry) {  // k_leaf_carry wrote the carries, the totals and n_unique
@@ -910,30 +925,24 @@ k_leaf_prefix(DevState *st, uint32_t n, const float4 *__restrict__ sp, const uin
             st->n_unique = nu;
             leaf_start[nu] = n;
             carry[b + 1] = bdd_add_body<D>(cb, tile_sum[b]);
-            local_put<D>(pre, nu, Body{0.0, 0.0, 0.0, 0.0});
+            local_put<D>(pre, n, Body{0.0, 0.0, 0.0, 0.0});
         }
     }
-    uint64_t k[AG_I];
-    uint32_t fl;
-    const Body acc = point_chunk<D>(n, p0, pt, keys, k, fl);
-    Body ex, total;
-    uint32_t exc, tcnt;
-    block_scan_body<D>(acc, (uint32_t)__popc(fl), ex, exc, total, tcnt, s_w, s_c);
-    uint32_t e = cbefore + exc;  // leaves that start before this thread's first point
-    Body run = ex;
+    const uint32_t p0 = b * AG_TILE + threadIdx.x * AG_I;
+    uint32_t v[AG_I];
+#pragma unroll
+    for (int r = 0; r < AG_I; r++) v[r] = p0 + r < n ? uid[p0 + r] : 0u;
 #pragma unroll
     for (int r = 0; r < AG_I; r++) {
         const uint32_t p = p0 + r;
         if (p < n) {
-            if (((fl >> r) & 1u) && e < n) {  // e < n unless a sort pass gave up a wait
-                local_put<D>(pre, e, run);
+            const uint32_t e = cbefore + (v[r] & 0x7fffffffu) - 1u;  // the point's leaf
+            uid[p] = e;
+            if ((v[r] >> 31) && e < n) {  // e < n unless a sort pass gave up a wait
                 leaf_start[e] = p;
-                ukey[e] = k[r];
+                ukey[e] = keys[p];
                 levels[e] = 0;
-                e++;
             }
-            uid[p] = e - 1;
-            run = body_sum<D>(run, point_body<D>(pt[r]));
         }
     }
 }
