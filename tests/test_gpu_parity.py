@@ -93,6 +93,21 @@ def test_large_2d_powerlaw_forces():
     assert abs(info["far_count"] - sc["far"]) <= 1e-3 * sc["far"]
 
 
+def test_ba_100k_linlog_dissuade_weighted_full_size():
+    # the 100k-node BA workload at its own size: lognormal weights, linlog,
+    # dissuade hubs, theta 1.0
+    wl = synth.ba_100k()
+    rel, info, sc = _check(wl.n, wl.src, wl.dst, wl.weight, wl.pos0, wl.params)
+    assert abs(info["far_count"] - sc["far"]) <= 1e-3 * sc["far"]
+
+
+def test_powerlaw_1m_3d_strong_gravity_full_size():
+    # the 1M-node octree workload at its own size: strong gravity, theta 1.2
+    wl = synth.powerlaw_1m(n=1_000_000, dim=3)
+    rel, info, sc = _check(wl.n, wl.src, wl.dst, None, wl.pos0, wl.params)
+    assert abs(info["far_count"] - sc["far"]) <= 1e-3 * sc["far"]
+
+
 def test_large_2d_forces_with_one_block_tile_carries():
     # past 2,048 tiles of 1,024 sorted points the leaf pass's tile carries come
     # from one block (k_leaf_carry) instead of each tile's own fold
