@@ -169,6 +169,30 @@ def test_trajectory_tracks_the_oracle_for_a_few_ticks():
     assert np.abs(g - r).max() / ext < 1e-4
 
 
+@pytest.mark.parametrize("case", ["sbm1500", "ba5k"])
+def test_full_run_matches_the_oracle_on_energy_and_stress(case):
+    """Whole runs diverge chaotically, so the finished layouts are compared on
+    the FA2 energy (each term) and the sampled Kruskal stress, within 1%."""
+    from graph_render_b200 import quality
+
+    wl = synth.sbm_1500() if case == "sbm1500" else synth.ba_100k(n=5000)
+    ticks = 100
+    prm = dict(wl.params, max_iter=ticks)
+    with Fa2(wl.n, wl.src, wl.dst, wl.weight, params=prm, pos0=wl.pos0) as eng:
+        eng.run()
+        g = eng.positions().astype(np.float64)
+    st = oracle_state(wl.n, wl.src, wl.dst, wl.weight, wl.pos0, wl.params)
+    st.run(ticks)
+    r = st.positions()
+    eg = quality.fa2_energy(g, wl.src, wl.dst, wl.weight, prm)
+    er = quality.fa2_energy(r, wl.src, wl.dst, wl.weight, prm)
+    for term in ("attraction", "repulsion", "gravity", "total"):
+        assert abs(eg[term] - er[term]) <= 1e-2 * abs(er[term]), (term, eg[term], er[term])
+    sg = O.stress(g[:, 0], g[:, 1], wl.src, wl.dst, 16)
+    sr = O.stress(r[:, 0], r[:, 1], wl.src, wl.dst, 16)
+    assert abs(sg - sr) <= 1e-2 * sr, (sg, sr)
+
+
 @pytest.mark.parametrize("dim", [2, 3])
 def test_walk_schedules_give_bit_identical_forces_and_tuning_keeps_the_state(dim):
     wl = synth.powerlaw_1m(n=200_000, dim=dim)
