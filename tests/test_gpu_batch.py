@@ -130,3 +130,33 @@ def test_batch_3d():
         with Fa2(g.n, g.src, g.dst, params=g.params, pos0=g.pos0) as eng:
             eng.tick(2)
             assert rel_extent(pos, eng.positions()) < 1e-5
+
+
+def test_batch_full_runs_match_the_oracle_on_energy_and_stress():
+    """Whole 100-tick runs of a dozen mixed graphs (SBM, BA, rewired grids of
+    300-3,000 nodes) against the oracle's FP64 runs: each FA2 energy term and the
+    sampled Kruskal stress within 1%."""
+    from graph_render_b200 import quality
+    from oracle import oracle as O
+
+    gs = [g for g in small_mix(count=24, seed=5) if g.n >= 300][:12]
+    assert len(gs) >= 6
+    ticks = 100
+    with batch.Batch(gs) as b:
+        b.run(ticks)
+        got = b.positions()
+        st = b.stats()
+    assert (st["errors"] == 0).all()
+    for g, pos, done in zip(gs, got, st["ticks"]):
+        o = oracle_state(g.n, g.src, g.dst, g.weight, g.pos0, g.params)
+        assert o.run(ticks) == done, (g.kind, g.n)
+        r = o.positions()
+        prm = dict(g.params)
+        eg = quality.fa2_energy(pos, g.src, g.dst, g.weight, prm)
+        er = quality.fa2_energy(r, g.src, g.dst, g.weight, prm)
+        for term in ("attraction", "repulsion", "gravity", "total"):
+            assert abs(eg[term] - er[term]) <= 1e-2 * abs(er[term]) + 1e-9, (g.kind, g.n, term, eg[term], er[term])
+        if g.params.get("dim", 2) == 2:
+            sg = O.stress(pos[:, 0], pos[:, 1], g.src, g.dst, 16)
+            sr = O.stress(r[:, 0], r[:, 1], g.src, g.dst, 16)
+            assert abs(sg - sr) <= 1e-2 * sr, (g.kind, g.n, sg, sr)
