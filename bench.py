@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-3d", action="store_true")
     ap.add_argument("--no-d3", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other configs and the reference's benchmark")
     ap.add_argument("--batched-graphs", type=int, default=4096, help="graphs per GPU")
     ap.add_argument("--batched-ticks", type=int, default=200)
     ap.add_argument("--batched-sample", type=int, default=48, help="graphs timed one launch sequence each")
@@ -211,6 +212,21 @@ class Dist:
 
 # -------------------------------------------------------------- CPU arms --
 
+def host_cpu() -> dict:
+    """This host's CPU as lscpu names it, and the threads the CPU arms use."""
+    info = {"threads_used": os.cpu_count() or 1}
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        kv = {k.strip(): v.strip() for k, v in (ln.split(":", 1) for ln in out.splitlines() if ":" in ln)}
+        for key, name in (("Model name", "model"), ("CPU(s)", "cpus"), ("Socket(s)", "sockets"),
+                          ("Core(s) per socket", "cores_per_socket"), ("Thread(s) per core", "threads_per_core")):
+            if key in kv:
+                info[name] = kv[key]
+    except (OSError, subprocess.SubprocessError):
+        info["model"] = "lscpu unavailable"
+    return info
+
+
 def cpu_port_rate(wl, threads: int, budget_s: float, min_ticks: int = 1, max_ticks: int = 1000):
     """The oracle (FP64 restatement of graph-core's tick) on the host cores:
     (node-ticks/s, ticks timed, seconds)."""
@@ -240,9 +256,13 @@ def run_reference(args, dist: Dist):
     walk) on this box's host cores, rank 0 only."""
     if dist.rank != 0:
         return
+    from oracle import oracle as O
+    from graph_render_b200 import synth
+
+    O.build()
+    synth.use_library(O.LIB_PATH)  # the same seeded graphs, drawn by the oracle's copy of the generators
     wl = workload(args.workload, args.n)
     threads = os.cpu_count() or 1
-    from oracle import oracle as O
 
     lo, hi, ws = O.simple_graph(wl.n, wl.src, wl.dst, wl.weight)
     p = wl.params
@@ -273,7 +293,8 @@ def run_reference(args, dist: Dist):
         "data": "synthetic",
         "config": {"workload": wl.name, "n": wl.n, "m_raw": wl.m, "theta": p.get("theta"), "dim": p.get("dim")},
         "cpu_baseline": {"value": v, "unit": "node-ticks/s", "cores": threads, "kind": "port",
-                         "sample": f"{steps} full ticks of the {wl.name} workload after {warm} warm-up ticks"},
+                         "sample": f"{steps} full ticks of the {wl.name} workload after {warm} warm-up ticks",
+                         "cpu": host_cpu()},
         "e2e": {"value": v, "unit": "node-ticks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "graph-core is Rust (no cargo here or on the GPU box); the reference arm is the FP64 C "
                 "restatement of its FA2 tick (oracle/), OpenMP over per-node walks",
@@ -446,6 +467,138 @@ def run_d3(args, dist: Dist):
                                                 "source": "docs/measurements/perf-bh-1m.md:36-43, other host"}}
 
 
+# ------------------------------------------------------- the other configs --
+
+REF_GATE_MS = {1_000: (1_541, 43.59, 0.4089), 5_000: (7_721, 263.41, 0.4205), 10_000: (15_474, 583.83, 0.4111),
+               100_000: (154_978, 8_310.29, 0.4539), 1_000_000: (1_549_929, 123_031.69, 0.4486)}
+REF_GATE_SOURCE = "docs/measurements/perf-fa2bh.md:54-60 (graph-cli bench, 100 iterations, 1 thread, other host)"
+
+
+def one_shot(wl, ticks: int, calls: int) -> dict:
+    """The public per-graph call from pinned host buffers: create from host
+    edges, `ticks` ticks, positions back; wall clock, median of `calls`."""
+    import torch
+
+    from graph_render_b200 import Fa2
+
+    dim = int(wl.params.get("dim", 2))
+    src = torch.from_numpy(wl.src).pin_memory().numpy()
+    dst = torch.from_numpy(wl.dst).pin_memory().numpy()
+    pos0 = torch.from_numpy(np.ascontiguousarray(wl.pos0)).pin_memory().numpy()
+    w = None if wl.weight is None else torch.from_numpy(wl.weight).pin_memory().numpy()
+    out = torch.empty((wl.n, dim), dtype=torch.float32).pin_memory().numpy()
+    prm = dict(wl.params, max_iter=ticks)
+    times = []
+    for _ in range(calls):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with Fa2(wl.n, src, dst, w, params=prm, pos0=pos0) as e:
+            e.set_interaction_counting(False)
+            ran = e.run()
+            e.positions(out=out)
+        times.append(time.perf_counter() - t0)
+    el = float(np.median(times))
+    return {"value": wl.n * ran / el, "unit": "node-ticks/s", "seconds": el, "ticks": ran,
+            "h2d_bytes_per_call": wl.m * 8 + wl.n * dim * 4 + (0 if w is None else wl.m * 8),
+            "d2h_bytes_per_call": wl.n * dim * 4, "of": f"median of {calls} calls"}
+
+
+def device_run(wl, ticks: int) -> dict:
+    """`ticks` ticks from the workload's start on a fresh handle (a warm-up
+    handle ran first), each tick timed with CUDA events on the handle's stream,
+    a 256 MiB buffer overwritten before each (outside the events)."""
+    from graph_render_b200 import Fa2
+
+    with Fa2(wl.n, wl.src, wl.dst, wl.weight, params=wl.params, pos0=wl.pos0) as e:
+        e.set_interaction_counting(False)
+        e.tick(3)
+        e.tick_timed(2, l2_flush_bytes=FLUSH_BYTES)
+    with Fa2(wl.n, wl.src, wl.dst, wl.weight, params=wl.params, pos0=wl.pos0) as e:
+        e.set_interaction_counting(False)
+        ms = e.tick_timed(ticks, l2_flush_bytes=FLUSH_BYTES)
+        pos = e.positions()
+    t = float(ms[:, 3].sum())
+    return {"value": wl.n * len(ms) / (t / 1e3), "unit": "node-ticks/s", "ticks": int(len(ms)),
+            "run_ms": t, "ms_per_tick": t / max(len(ms), 1),
+            "phase_ms": {"tree": float(ms[:, 0].mean()), "walk": float(ms[:, 1].mean()),
+                         "finish": float(ms[:, 2].mean())}}, pos
+
+
+def run_config_legs(args, dist: Dist) -> dict:
+    """The 1,500-node SBM for 100 ticks and the 100k-node BA graph (linlog,
+    dissuade hubs, lognormal weights, theta 1.0) for 500 ticks: device time of
+    the whole run, the public call end to end, and the oracle on this host's
+    cores on a bounded sample of the same run."""
+    from graph_render_b200 import synth
+
+    threads = os.cpu_count() or 1
+    legs = {}
+    for key, wl, ticks, calls in (("sbm1500_100_ticks", synth.sbm_1500(), 100, 5),
+                                  ("ba100k_500_ticks", synth.ba_100k(), 500, 3)):
+        dev, _ = device_run(wl, ticks)
+        e2e = one_shot(wl, ticks, calls)
+        v, t, el = cpu_port_rate(wl, threads, min(args.cpu_budget_s, 10.0), max_ticks=ticks)
+        legs[key] = {"workload": wl.name, "n": wl.n, "m_raw": wl.m, "theta": wl.params.get("theta"),
+                     "device": dev, "e2e": e2e,
+                     "cpu_baseline": {"value": v, "unit": "node-ticks/s", "cores": threads, "kind": "port",
+                                      "sample": f"the first {t} FP64 ticks of the same run, {el:.1f} s"}}
+    return legs
+
+
+def run_gate_legs(args, dist: Dist) -> dict:
+    """The reference's own benchmark (graph-cli bench --layout
+    layout.forceatlas2.barnes_hut): its gate-model graph at 1,000 .. 1,000,000
+    nodes, the layout's defaults (theta 0.8, 100 iterations, Mulberry32(0)
+    start), through the drop-in registry call (topology in, geometry out) with
+    no positions given; wall clock of the call (median of 3), and the
+    reference's Kruskal stress-1 of the result, beside its published time and
+    stress for the same n."""
+    import torch
+
+    from graph_render_b200 import FA2_ID, Topology, find, stress as S, synth
+
+    cap = find(FA2_ID)
+    out = {}
+    warm = synth.gate(1000)
+    cap.run_params(Topology(1000, warm[0], warm[1], warm[2]), b"")
+    for n, (m_ref, ms_ref, stress_ref) in REF_GATE_MS.items():
+        src, dst, strength = synth.gate(n)
+        topo = Topology(n, src, dst, strength)
+        times = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            geom = cap.run_params(topo, b"")
+            times.append(time.perf_counter() - t0)
+        el = float(np.median(times))
+        x, y = np.asarray(geom.x, np.float32), np.asarray(geom.y, np.float32)
+        st = S.kruskal_stress(x, y, src, dst, 16)
+        out[str(n)] = {"edges": int(len(src)), "ms": 1e3 * el, "node_ticks_per_s": n * 100 / el,
+                       "kruskal_stress": st,
+                       "reference": {"edges": m_ref, "ms": ms_ref, "kruskal_stress": stress_ref},
+                       "speedup_vs_published": ms_ref / (1e3 * el)}
+    # the oracle (the reference's algorithm, FP64, OpenMP walk) on this host's
+    # cores, a bounded sample of the 1M-node run from the same start
+    from oracle import oracle as O
+
+    n = 1_000_000
+    src, dst, strength = synth.gate(n)
+
+    class Gate:
+        pass
+
+    g = Gate()
+    g.n, g.src, g.dst, g.weight, g.m = n, src, dst, None, len(src)
+    g.pos0 = O.initial_positions(n, 0, 2)
+    g.params = dict(theta=0.8, dim=2, seed=0)
+    threads = os.cpu_count() or 1
+    v, t, el = cpu_port_rate(g, threads, min(args.cpu_budget_s, 12.0))
+    out["cpu_baseline_1000000"] = {"value": v, "unit": "node-ticks/s", "cores": threads, "kind": "port",
+                                   "sample": f"the first {t} FP64 ticks of the 1,000,000-node run, {el:.1f} s"}
+    out["source"] = REF_GATE_SOURCE
+    return out
+
+
 # --------------------------------------------------------------- GPU arm --
 
 def run_gpu(args, dist: Dist):
@@ -550,7 +703,7 @@ def run_gpu(args, dist: Dist):
         v, ticks, el = cpu_port_rate(wl, threads, args.cpu_budget_s)
         cpu = {"value": v, "unit": "node-ticks/s", "cores": threads, "kind": "port",
                "sample": f"{ticks} full FP64 ticks of the same {wl.n}-node graph from the same start, "
-                         f"{el:.1f} s (tree build serial, walks OpenMP)"}
+                         f"{el:.1f} s (tree build serial, walks OpenMP)", "cpu": host_cpu()}
 
     batched = None
     if not args.no_batched:
@@ -564,6 +717,15 @@ def run_gpu(args, dist: Dist):
     d3 = None
     if not args.no_d3 and dist.rank == 0:
         d3 = run_d3(args, dist)
+    legs = gate = None
+    if not args.no_configs and dist.rank == 0:
+        legs = run_config_legs(args, dist)
+        gate = run_gate_legs(args, dist)
+    # vs_baseline: the reference's published 1M-node run against the same
+    # workload here (its gate model, theta 0.8, 100 iterations, its own start)
+    vs = None
+    if gate is not None:
+        vs = gate["1000000"]["node_ticks_per_s"] / REF_1M_NODE_TICKS
 
     if dist.rank == 0:
         line = {
@@ -576,7 +738,7 @@ def run_gpu(args, dist: Dist):
             "ms_per_step": max_ms / max(done, 1),
             "higher_is_better": True,
             "scaling": "weak",
-            "vs_baseline": value / REF_1M_NODE_TICKS if wl.n == 1_000_000 else None,
+            "vs_baseline": vs,
             "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": wl.name, "n": wl.n, "m_raw": wl.m, "m_simple": int(info1["m"]),
@@ -614,8 +776,12 @@ def run_gpu(args, dist: Dist):
             "adjoint": adjoint,
             "powerlaw_1m_3d": three_d,
             "d3_force_1m": d3,
-            "vs_baseline_basis": "reference's own 1M-node FA2-BH run, 1 thread, other host "
-                                 "(perf-fa2bh.md:60-63; theta 0.8, its gate-model graph)",
+            "configs": legs,
+            "reference_benchmark": gate,
+            "vs_baseline_basis": "reference_benchmark['1000000'] (its gate-model graph at 1M nodes, theta 0.8, "
+                                 "100 iterations from its Mulberry32 start, through the registry call) over the "
+                                 "reference's published run of the same workload, 1 thread, other host "
+                                 "(perf-fa2bh.md:60-63)",
         }
         print(json.dumps(line), flush=True)
 

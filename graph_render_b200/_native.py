@@ -113,6 +113,8 @@ SIGNATURES = {
     "gr_fa2_set_interaction_counting": ([P, C.c_int], C.c_int),
     "gr_fa2_launch_mode": ([P, C.POINTER(C.c_int)], C.c_int),
     "gr_fa2_tune": ([P, C.c_uint32, C.POINTER(C.c_int), P], C.c_int),
+    "gr_fa2_set_wait_limit": ([P, C.c_uint32], C.c_int),
+    "gr_fa2_inject_stalled_wait": ([P, C.c_int], C.c_int),
     "gr_fa2_get_controller": ([P, P], C.c_int),
     "gr_fa2_set_controller": ([P, P], C.c_int),
     "gr_fa2_adjoint_forward": ([P, C.c_uint32, C.c_uint32], C.c_int),

@@ -189,6 +189,7 @@ struct gr_fa2 {
     bool unit_w = false;
     void *flush = nullptr;
     size_t flush_bytes = 0;
+    uint32_t *stall_word = nullptr;  // zeroed and never written: the injected wait's flag
 
     std::vector<void *> allocs;
 
@@ -365,7 +366,7 @@ static void keys_sort_fast(gr_fa2 *h, cudaStream_t s) {
         gr_launch(h->pdl, k_keys_hist<D>, std::min<uint32_t>(div_up(n, OS_HIST_THREADS * 4), 4 * 148),
                   OS_HIST_THREADS, 0, s, h->pos, n, h->st, h->keys, h->vals, h->sorter.os_ghist, h->sorter.os_status,
                   (uint64_t)4 * nt * RS_BINS);
-        h->sorter.onesweep_passes(h->keys, h->vals, n, 4, 4, s, &h->st->error, conv, h->pdl);
+        h->sorter.onesweep_passes(h->keys, h->vals, n, 4, 4, s, &h->st->error, conv, h->pdl, &h->st->converged);
     } else {
         k_keys<D><<<div_up(n, 256), 256, 0, s>>>(h->pos, n, h->st, h->keys, h->vals);
         h->sorter.sort_digits(h->keys, h->vals, n, 4, 4, s, conv);
@@ -383,7 +384,10 @@ template <int D, bool COUNT>
 static void launch_walk(gr_fa2 *h, const WalkParams &wp, cudaStream_t s, bool pdl) {
     const uint32_t n = h->n;
     DevState *st = h->st;
-    if (h->walk_schedule == 2)
+    if (h->walk_schedule == 3)  // 64 nodes per warp: two groups of 32, one walk of each per lane
+        gr_launch(pdl, k_walk_s<D, 3, COUNT>, div_up(n, 2 * WALK_THREADS), WALK_THREADS, 0, s, wp, st, h->cells,
+                  h->sp, h->sorig, h->uid, h->leaf_pre, h->rep, st);
+    else if (h->walk_schedule == 2)
         gr_launch(pdl, k_walk_s<D, 2, COUNT>, div_up(div_up(n, 2), WALK_THREADS), WALK_THREADS, 0, s, wp, st,
                   h->cells, h->sp, h->sorig, h->uid, h->leaf_pre, h->rep, st);
     else if (h->walk_schedule == 1)
@@ -1099,7 +1103,7 @@ int gr_fa2_get_info(gr_fa2 *h, gr_fa2_info *out) {
 int gr_fa2_set_walk_schedule(gr_fa2 *h, int schedule) {
     if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
     if (schedule < 0 || schedule >= GR_WALK_SCHEDULES)
-        return set_err(GR_INVALID_ARGUMENT, "walk schedule must be 0, 1 or 2");
+        return set_err(GR_INVALID_ARGUMENT, "walk schedule must be 0, 1, 2 or 3");
     if (schedule != h->walk_schedule) {
         h->walk_schedule = schedule;
         h->drop_graphs();
@@ -1119,6 +1123,33 @@ int gr_fa2_set_interaction_counting(gr_fa2 *h, int on) {
     if (on != 0 && on != 1) return set_err(GR_INVALID_ARGUMENT, "on must be 0 or 1");
     if ((on == 1) != h->count_interactions) {
         h->count_interactions = on == 1;
+        h->drop_graphs();
+    }
+    return ok();
+}
+
+int gr_fa2_set_wait_limit(gr_fa2 *h, uint32_t spins) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    const uint32_t limit = spins ? spins : OS_SPIN_LIMIT;
+    if (limit != h->sorter.wait.limit) {
+        h->sorter.wait.limit = limit;
+        h->drop_graphs();
+    }
+    return ok();
+}
+
+int gr_fa2_inject_stalled_wait(gr_fa2 *h, int on) {
+    if (!h) return set_err(GR_INVALID_HANDLE, "null handle");
+    if (on != 0 && on != 1) return set_err(GR_INVALID_ARGUMENT, "on must be 0 or 1");
+    if (on && !h->stall_word) {
+        cudaError_t e = h->alloc(&h->stall_word, 1);
+        if (e) return set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+        CU(cudaMemsetAsync(h->stall_word, 0, sizeof(uint32_t), h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+    }
+    const uint32_t *want = on ? h->stall_word : nullptr;
+    if (want != h->sorter.wait.stall) {
+        h->sorter.wait.stall = want;
         h->drop_graphs();
     }
     return ok();
@@ -1242,13 +1273,12 @@ int gr_run(const char *layout_id, uint32_t n, uint64_t m, const uint32_t *src, c
 //
 // gr_fa2_forces_static: one force evaluation (the same kernels as
 // gr_fa2_forces) for callers that cannot allocate device memory at all — code
-// running inside another runtime's stream-ordered or pooled allocator, a plugin
-// that is only handed device buffers by its host, or a stream that is being
-// captured into a CUDA graph, where a cudaMalloc would break the capture. Its
-// scratch is the file-scope array below, sized for STATIC_MAX_N nodes; every GPU
-// that loads this library holds that array until the process exits. The caller
-// passes inputs and outputs in device memory; nothing here calls cudaMalloc,
-// cudaFree or any allocating routine.
+// running inside another runtime that owns every device allocation (its own
+// stream-ordered or pooled allocator), or a plugin that is only handed device
+// buffers by its host. Its scratch is the file-scope array below, sized for
+// STATIC_MAX_N nodes; every GPU that loads this library holds that array until
+// the process exits. The caller passes inputs and outputs in device memory;
+// nothing here calls cudaMalloc, cudaFree or any allocating routine.
 
 constexpr uint32_t STATIC_MAX_N = GR_FORCES_STATIC_MAX_N;
 constexpr size_t STATIC_BYTES_PER_NODE = 400;
@@ -1256,20 +1286,52 @@ constexpr size_t STATIC_BYTES = STATIC_BYTES_PER_NODE * STATIC_MAX_N + (1u << 20
 
 static __device__ __align__(256) unsigned char g_static_scratch[STATIC_BYTES];
 
-// Host-side device addresses of g_static_scratch, one per device. In host code
-// the symbol itself is only a stand-in, never a device address.
+// Host-side device addresses of g_static_scratch, one per device, with the id
+// of the context each was looked up in. In host code the symbol itself is only a
+// stand-in, never a device address. A device reset (cudaDeviceReset) ends the
+// context the address belongs to; the next call sees a new context id and looks
+// the address up again.
 static std::mutex g_static_mu;
 static unsigned char *g_static_base[256];
+static unsigned long long g_static_ctx[256];
+
+// The id of the calling thread's current context (driver entry points found at
+// run time, so the library links no driver library); false when there is none.
+static bool current_context_id(unsigned long long *id) {
+    typedef int (*CtxGetCurrent)(void **);
+    typedef int (*CtxGetId)(void *, unsigned long long *);
+    static CtxGetCurrent get_current = nullptr;
+    static CtxGetId get_id = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        void *f = nullptr, *g = nullptr;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q1) == cudaSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &g, cudaEnableDefault, &q2) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+            get_current = (CtxGetCurrent)f;
+            get_id = (CtxGetId)g;
+        }
+        cudaGetLastError();
+        looked = true;
+    }
+    void *ctx = nullptr;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx) return false;
+    return get_id(ctx, id) == 0;
+}
 
 static int static_base(unsigned char **out) {
     int dev = 0;
     CU(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 256) return set_err(GR_INVALID_ARGUMENT, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_base[dev]) {
+    unsigned long long id = 0;
+    const bool known = current_context_id(&id);
+    if (!g_static_base[dev] || !known || id != g_static_ctx[dev]) {
         void *p = nullptr;
-        CU(cudaGetSymbolAddress(&p, g_static_scratch));
+        CU(cudaGetSymbolAddress(&p, g_static_scratch));  // makes the device's context current
         g_static_base[dev] = (unsigned char *)p;
+        g_static_ctx[dev] = current_context_id(&id) ? id : 0ull;
     }
     *out = g_static_base[dev];
     return GR_OK;
@@ -1308,6 +1370,7 @@ static int forces_static(uint32_t n, const float4 *nodes, const uint32_t *rp, co
     memcpy(h.prm, prm, sizeof h.prm);
     h.stream = s;
     h.own_stream = false;
+    h.pdl = pdl_default();  // GR_PDL=0 in the environment: plain stream order
     h.st = cv.take<DevState>(1);
     h.keys = cv.take<uint64_t>(n);
     h.vals = cv.take<uint32_t>(n);
@@ -1384,7 +1447,7 @@ int gr_fa2_forces_static(uint32_t n, const void *nodes, const uint32_t *row_ptr,
         return set_err(GR_INVALID_ARGUMENT, b);
     }
     if (n == 0) return ok();
-    if (!nodes || !row_ptr || !out || !weight) return set_err(GR_INVALID_ARGUMENT, "a device buffer is null");
+    if (!nodes || !row_ptr || !col || !out || !weight) return set_err(GR_INVALID_ARGUMENT, "a device buffer is null");
     const cudaStream_t s = (cudaStream_t)stream;
     int rc = (int)prm[P_DIM] == 3 ? forces_static<3>(n, (const float4 *)nodes, row_ptr, col, weight, prm, tick, out, s)
                                   : forces_static<2>(n, (const float4 *)nodes, row_ptr, col, weight, prm, tick, out, s);

@@ -212,6 +212,17 @@ constexpr int OS_MAX_PASSES = 8;
 constexpr uint32_t OS_FLAG_A = 1u << 30, OS_FLAG_P = 2u << 30, OS_COUNT = (1u << 30) - 1u;
 constexpr uint32_t OS_SPIN_LIMIT = 1u << 22;  // x 32 ns sleeps: ~0.1 s
 
+// The bounds on a pass's look-back waits: `limit` sleeps before a wait gives up
+// (ERR_WAIT in the pass's error word); `halt` (nullable) is set to 1 when one
+// does, the word the caller's later kernels skip on; `stall` (nullable, fault
+// injection for tests) makes tile 1 first wait for that word to become nonzero,
+// which nothing does, so its wait gives up after `limit` sleeps.
+struct OsWait {
+    uint32_t limit = OS_SPIN_LIMIT;
+    uint32_t *halt = nullptr;
+    const uint32_t *stall = nullptr;
+};
+
 // The tile shape the engine uses: T threads x I keys, look-back window L
 // (on B200 at 1M keys: 512 x 8 sorts 4 digits in 78 us, 256 x 8 in 105 us).
 constexpr int OS_T = 512, OS_I = 8, OS_L = 8;
@@ -293,7 +304,7 @@ template <typename V, int T, int I, int L>
 __global__ void __launch_bounds__(T)
 os_pass(const uint64_t *__restrict__ kin, const V *__restrict__ vin, uint64_t *__restrict__ kout, V *__restrict__ vout,
         uint32_t n, int shift, const uint32_t *__restrict__ ghist, uint32_t *status, uint32_t *counter, uint32_t *err,
-        const uint32_t *skip) {
+        const uint32_t *skip, OsWait wt) {
     gr_pdl_enter();
     static_assert(T % RS_BINS == 0, "one thread per digit at least");
     constexpr int W = T / GR_WARP, TILE = T * I, CHUNK = I * GR_WARP;
@@ -355,7 +366,16 @@ os_pass(const uint64_t *__restrict__ kin, const V *__restrict__ vin, uint64_t *_
             // first P (done) or the first tile that has published nothing (wait).
             int64_t j = (int64_t)tile - 1;
             uint32_t spins = 0;
-            bool done = false;
+            bool done = false, gave_up = false;
+            if (wt.stall && tile == 1) {  // injected fault: a word that nothing sets
+                while (*(volatile const uint32_t *)wt.stall == 0u) {
+                    if (++spins > wt.limit) {
+                        gave_up = done = true;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
             while (!done) {
                 uint32_t v[L];
 #pragma unroll
@@ -376,12 +396,16 @@ os_pass(const uint64_t *__restrict__ kin, const V *__restrict__ vin, uint64_t *_
                 }
                 j -= used;
                 if (!done && wait) {
-                    if (++spins > OS_SPIN_LIMIT) {
-                        atomicOr(err, (uint32_t)ERR_WAIT);
+                    if (++spins > wt.limit) {
+                        gave_up = true;
                         break;
                     }
                     __nanosleep(32);
                 }
+            }
+            if (gave_up) {  // the counts are wrong: flag it and stop the caller's later kernels
+                atomicOr(err, (uint32_t)ERR_WAIT);
+                if (wt.halt) atomicExch(wt.halt, 1u);
             }
             vs[(size_t)tile * RS_BINS + t] = OS_FLAG_P | (excl + cnt);
         }
@@ -430,6 +454,7 @@ struct RadixSorter {
     uint32_t os_tiles = 0;
     uint32_t *os_ghist = nullptr;   // OS_MAX_PASSES * RS_BINS digit counts, then OS_MAX_PASSES tile counters
     uint32_t *os_status = nullptr;  // OS_MAX_PASSES * os_tiles * RS_BINS look-back words
+    OsWait wait;                    // the one-sweep passes' wait bounds (halt is per call)
 
     // With a stream, the buffers come from the device's stream-ordered pool on it
     // and go back to it on release (no device-wide synchronisation).
@@ -502,18 +527,21 @@ struct RadixSorter {
     // The one-sweep passes alone, for a caller whose own kernel already filled
     // os_ghist (zeroed first) with the digit counts and zeroed the look-back
     // words (os_hist's work).
+    // A wait that gives up sets ERR_WAIT in *err and, when halt is given, *halt = 1.
     void onesweep_passes(uint64_t *keys, uint32_t *vals, uint32_t n, int first_digit, int passes, cudaStream_t s,
-                         uint32_t *err, const uint32_t *skip = nullptr, bool pdl = false) {
+                         uint32_t *err, const uint32_t *skip = nullptr, bool pdl = false, uint32_t *halt = nullptr) {
         if (n == 0) return;
+        OsWait w = wait;
+        w.halt = halt;
         if (n >= OS_BIG_MIN)
-            passes_shaped<OS_BIG_T, OS_BIG_I>(keys, vals, n, first_digit, passes, s, err, skip, pdl);
+            passes_shaped<OS_BIG_T, OS_BIG_I>(keys, vals, n, first_digit, passes, s, err, skip, pdl, w);
         else
-            passes_shaped<OS_T, OS_I>(keys, vals, n, first_digit, passes, s, err, skip, pdl);
+            passes_shaped<OS_T, OS_I>(keys, vals, n, first_digit, passes, s, err, skip, pdl, w);
     }
 
     template <int T, int I>
     void passes_shaped(uint64_t *keys, uint32_t *vals, uint32_t n, int first_digit, int passes, cudaStream_t s,
-                       uint32_t *err, const uint32_t *skip, bool pdl) {
+                       uint32_t *err, const uint32_t *skip, bool pdl, const OsWait &w) {
         static_assert(T * I >= OS_T * OS_I, "os_tiles counts tiles of the smallest shape");
         const uint32_t nt = div_up(n, T * I);
         constexpr size_t smem = os_smem<uint32_t, T, I>();
@@ -525,7 +553,7 @@ struct RadixSorter {
         for (int p = 0; p < passes; p++) {
             gr_launch(pdl, os_pass<uint32_t, T, I, OS_L>, nt, T, smem, s, ka, (const uint32_t *)va, kb, vb, n,
                       8 * (first_digit + p), (const uint32_t *)(os_ghist + p * RS_BINS),
-                      os_status + (size_t)p * nt * RS_BINS, os_ghist + OS_MAX_PASSES * RS_BINS + p, err, skip);
+                      os_status + (size_t)p * nt * RS_BINS, os_ghist + OS_MAX_PASSES * RS_BINS + p, err, skip, w);
             std::swap(ka, kb);
             std::swap(va, vb);
         }

@@ -183,17 +183,32 @@ __device__ __forceinline__ void lane_init(const WalkView &V, uint32_t p, LaneNod
     X.k = valid ? 0u : V.ncells;
 }
 
-// The visit of cell X.k (X.k < ncells): a body term, a leaf's pairs, or a
-// descent; X.k moves on. COUNT: keep the far / pair interaction counts.
+// One cell's records as the walk reads them (C only in 3D).
+struct CellRec {
+    float4 A, B;
+    int2 C;
+};
+
+template <int D>
+__device__ __forceinline__ CellRec cell_rec(const Cells &cells, uint32_t k) {
+    CellRec r;
+    r.A = cell_a<D>(cells, k);
+    r.B = cell_b<D>(cells, k);
+    r.C = D == 3 ? cell_c3(cells, k) : make_int2(0, 0);
+    return r;
+}
+
+// The visit of cell X.k (X.k < ncells) whose records are R: a body term, a
+// leaf's pairs, or a descent; X.k moves on. COUNT: keep the far / pair
+// interaction counts.
 template <int D, bool COUNT = true>
-__device__ __forceinline__ void lane_step(const WalkView &V, LaneNode &X) {
-    const Cells cells = V.cells;
+__device__ __forceinline__ void lane_visit(const WalkView &V, LaneNode &X, const CellRec &R) {
     const float4 *__restrict__ sp = V.sp;
     const uint32_t n = V.n, iter = V.iter, k = X.k, oi = X.oi;
     const float4 me = X.me;
     const float th2 = V.th2, mk = X.mk;
-    const float4 A = cell_a<D>(cells, k);
-    const float4 B = cell_b<D>(cells, k);
+    const float4 A = R.A;
+    const float4 B = R.B;
     int32_t sk;
     uint32_t start;
     float cx, cy, cz, cm, w2, lx, ly, lz;
@@ -203,7 +218,7 @@ __device__ __forceinline__ void lane_step(const WalkView &V, LaneNode &X) {
         sk = __float_as_int(B.z);
         start = __float_as_uint(B.w);
     } else {
-        const int2 Cc = cell_c3(cells, k);
+        const int2 Cc = R.C;
         cx = A.x; cy = A.y; cz = A.z; cm = A.w;
         lx = B.x; ly = B.y; lz = B.z; w2 = B.w;
         sk = Cc.x;
@@ -274,6 +289,12 @@ __device__ __forceinline__ void lane_step(const WalkView &V, LaneNode &X) {
         }
         X.k = k + 1;
     }
+}
+
+// The visit of cell X.k (X.k < ncells), its records loaded here.
+template <int D, bool COUNT = true>
+__device__ __forceinline__ void lane_step(const WalkView &V, LaneNode &X) {
+    lane_visit<D, COUNT>(V, X, cell_rec<D>(V.cells, X.k));
 }
 
 template <int D, bool COUNT = true>
@@ -413,8 +434,29 @@ __device__ __forceinline__ void walk_pair(const WalkView &V, PairNode &a, PairNo
     }
 }
 
+// Two independent per-lane walks per thread, stepped in turn: the lane's nodes
+// p and p + 32 (a warp holds two groups of 32 consecutive sorted nodes, each
+// group as coherent as walk_lane's warp), each with its own cell index. Both
+// walks' cell records are requested before either is used, so every thread
+// keeps two dependent chains of cell loads in flight where walk_lane keeps
+// one. A walk that has finished re-reads its last cell (a cached load) and
+// does nothing with it. Each node visits its own cells in its own order with
+// lane_visit's arithmetic, so its forces are walk_lane's bit for bit.
+template <int D, bool COUNT = true>
+__device__ __forceinline__ void walk_two(const WalkView &V, LaneNode &a, LaneNode &b) {
+    const uint32_t nc = V.ncells;
+    const uint32_t last = nc - 1u;  // nc >= 1 whenever a node is valid
+    while (a.k < nc || b.k < nc) {
+        const CellRec ra = cell_rec<D>(V.cells, min(a.k, last));
+        const CellRec rb = cell_rec<D>(V.cells, min(b.k, last));
+        if (a.k < nc) lane_visit<D, COUNT>(V, a, ra);
+        if (b.k < nc) lane_visit<D, COUNT>(V, b, rb);
+    }
+}
+
 // Walk schedules: 0 = walk_group (a warp over the union of its 32 nodes),
-// 1 = walk_lane (one node per lane), 2 = walk_pair (two adjacent nodes per lane).
+// 1 = walk_lane (one node per lane), 2 = walk_pair (two adjacent nodes per
+// lane), 3 = walk_two (two independent walks per lane, 32 nodes apart).
 // COUNT: add the far / pair interaction counts to the state (a diagnostic; the
 // forces are the same either way).
 template <int D, int SCHED, bool COUNT>
@@ -425,11 +467,28 @@ k_walk_s(WalkParams P, const DevState *__restrict__ st, Cells cells, const float
     gr_pdl_enter();
     if (st->converged) return;
     const uint32_t g = blockIdx.x * WALK_THREADS + threadIdx.x;
-    const uint32_t p = SCHED == 2 ? 2 * g : g;
+    const uint32_t lane = threadIdx.x % GR_WARP;
+    const uint32_t p = SCHED == 2 ? 2 * g : SCHED == 3 ? 2 * (g - lane) + lane : g;
     if (__all_sync(GR_FULL, p >= P.n)) return;
     WalkView V{cells, sp, sorig, uid, leaf_pre, P.n, st->n_cells, st->iter_no, P.seed, P.kr, P.theta2, &stw->error};
     uint32_t nfar, npair;
-    if (SCHED == 2) {
+    if (SCHED == 3) {
+        LaneNode a, b;
+        lane_init<D>(V, p, a);
+        lane_init<D>(V, p + GR_WARP, b);
+        walk_two<D, COUNT>(V, a, b);
+        const LaneNode *X[2] = {&a, &b};
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+            if (X[j]->p < P.n) {
+                const uint32_t oi = X[j]->oi;
+                rep[(size_t)oi * D + 0] = X[j]->f0;
+                rep[(size_t)oi * D + 1] = X[j]->f1;
+                if (D == 3) rep[(size_t)oi * D + 2] = X[j]->f2;
+            }
+        nfar = a.nfar + b.nfar;
+        npair = a.npair + b.npair;
+    } else if (SCHED == 2) {
         PairNode a, b;
         pair_init<D>(V, p, a);
         pair_init<D>(V, p + 1, b);

@@ -23,9 +23,10 @@ PARAM_NAMES = ("max_iter", "jitter_tolerance", "scaling_ratio", "gravity", "seed
 DEFAULTS = dict(max_iter=100, jitter_tolerance=1.0, scaling_ratio=2.0, gravity=1.0, seed=0, dim=2,
                 theta=0.8, lin_log=0, strong_gravity=0, dissuade_hubs=0, edge_weight_influence=0.0)
 
-# walk schedules (include/graph_cuda.h GR_WALK_SCHEDULES): warp-union, per-lane, two nodes per lane
-WALK_SCHEDULES = 3
-WALK_SCHEDULE_NAMES = ("warp-union", "per-lane", "pair-per-lane")
+# walk schedules (include/graph_cuda.h GR_WALK_SCHEDULES): warp-union, per-lane, two nodes per lane over
+# the union of their walks, two independent walks per lane
+WALK_SCHEDULES = 4
+WALK_SCHEDULE_NAMES = ("warp-union", "per-lane", "pair-per-lane", "two-per-lane")
 
 
 def params_bytes(params: Union[None, bytes, Dict[str, float], Sequence[float]] = None, **kw) -> bytes:
@@ -172,6 +173,16 @@ class Fa2:
         """On (the default): the walk counts far / pair interactions into info();
         off: it keeps no counts (same forces, fewer instructions per cell)."""
         N.check(self._L.gr_fa2_set_interaction_counting(self.h, 1 if on else 0))
+
+    def set_wait_limit(self, spins: int) -> None:
+        """Sleeps (~32 ns each) a bounded wait of the tick's sort takes before it
+        gives up (0: the default)."""
+        N.check(self._L.gr_fa2_set_wait_limit(self.h, int(spins)))
+
+    def inject_stalled_wait(self, on: bool = True) -> None:
+        """Fault injection: a wait of every sort pass that nothing will end, so it
+        runs out and the next tick fails with GR_DEVICE_FAULT (ERR_WAIT)."""
+        N.check(self._L.gr_fa2_inject_stalled_wait(self.h, 1 if on else 0))
 
     def tune(self, sample_ticks: int = 3):
         """Autotunes the walk schedule; returns (chosen, {schedule: mean walk ms})."""

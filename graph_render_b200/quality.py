@@ -20,7 +20,10 @@ centre held fixed at the layout's mean:
 Masses are degree + 1 over the simple graph (self-loops dropped, the first of
 duplicate edges kept, state.rs:83-102). Computed in FP64 on the host over every
 node pair (O(n^2), chunked): a measure for test and evaluation sizes, not a
-step of the tick.
+step of the tick. For large graphs `pair_sample` estimates the repulsion term
+from that many node pairs drawn uniformly from `seed` (the pair sum scaled by
+n(n-1)/2 over the sample size); two layouts compared with the same sample and
+seed are measured on the same pairs.
 """
 
 from __future__ import annotations
@@ -44,10 +47,30 @@ def simple_edges(n: int, src, dst, weight=None):
     return lo[first], hi[first], w[first]
 
 
-def fa2_energy(pos, src, dst, weight=None, params=None, chunk: int = 2048) -> dict:
+def sampled_repulsion(p, mass, kr: float, pairs: int, seed: int, chunk: int = 1 << 22) -> float:
+    """-k_r sum m_i m_j ln d over all pairs i < j, estimated from `pairs` pairs
+    (i, j), i != j, drawn uniformly from `seed`."""
+    n = p.shape[0]
+    rng = np.random.default_rng(seed)
+    total, drawn = 0.0, 0
+    while drawn < pairs:
+        k = min(chunk, pairs - drawn)
+        i = rng.integers(0, n, k)
+        j = rng.integers(0, n - 1, k)
+        j = j + (j >= i)  # uniform over j != i
+        r = np.sqrt(((p[i] - p[j]) ** 2).sum(1))
+        with np.errstate(divide="ignore"):
+            total += float((mass[i] * mass[j] * np.log(r)).sum())
+        drawn += k
+    return -kr * total * (n * (n - 1) / 2.0) / pairs
+
+
+def fa2_energy(pos, src, dst, weight=None, params=None, chunk: int = 2048, pair_sample=None,
+               seed: int = 0) -> dict:
     """Energy terms of the layout `pos` (n x dim) under the FA2 parameters
     `params` (the engine's names and defaults): {"attraction", "repulsion",
-    "gravity", "total"}."""
+    "gravity", "total"}. With `pair_sample` the repulsion term is estimated
+    from that many uniformly drawn pairs (`sampled_repulsion`)."""
     prm = dict(DEFAULTS)
     prm.update(params or {})
     p = np.asarray(pos, np.float64)
@@ -64,7 +87,9 @@ def fa2_energy(pos, src, dst, weight=None, params=None, chunk: int = 2048) -> di
         att = att * 0.5 * (1.0 / mass[lo] + 1.0 / mass[hi])
     kr = float(prm["scaling_ratio"])
     rep = 0.0
-    for a in range(0, n, chunk):
+    if pair_sample is not None and n > 1:
+        rep = sampled_repulsion(p, mass, kr, int(pair_sample), seed)
+    for a in (range(0, n, chunk) if pair_sample is None else ()):
         b = min(n, a + chunk)
         # pairs (i, j) with i in [a, b) and j > i
         dx = p[a:b, None, :] - p[None, a:, :]

@@ -20,6 +20,15 @@ LIB_PATH = os.path.join(HERE, "libgraph_synth.so")
 _lib = None
 
 
+def use_library(path: str) -> None:
+    """Draw from another build of csrc/synth.c (the same generators and seeds),
+    e.g. one linked into a CPU baseline's own library. Call before any draw."""
+    global LIB_PATH, _lib
+    if _lib is not None and path != LIB_PATH:
+        raise RuntimeError("the generators are already loaded from " + LIB_PATH)
+    LIB_PATH = path
+
+
 def lib():
     global _lib
     if _lib is None:

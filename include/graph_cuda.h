@@ -71,7 +71,7 @@ typedef struct gr_fa2_info {
     double moved;            /* last tick's summed |step| */
     uint64_t far_count;      /* far-cell interactions since creation */
     uint64_t pair_count;     /* leaf pair interactions since creation */
-    uint32_t device_error;   /* device error bits (1 non-finite, 2 tree, 4 bounds) */
+    uint32_t device_error;   /* device error bits (1 non-finite, 2 tree, 4 bounds, 8 a bounded wait gave up) */
     uint32_t graph_kernels;  /* kernel launches in one captured tick (0 before the first tick) */
 } gr_fa2_info;
 
@@ -127,11 +127,13 @@ int gr_fa2_tick_timed(gr_fa2 *h, uint32_t ticks, size_t l2_flush_bytes, float *m
 /* Repulsion walk schedule: 0 = warp-cooperative (a warp visits the union of its 32
  * nodes' paths, one broadcast load per cell), 1 = per lane (each lane its own
  * path, gathered loads; the default), 2 = two adjacent nodes per lane over the
- * union of their two paths. All give bit-identical forces.
+ * union of their two paths, 3 = two independent per-lane walks per thread
+ * (nodes 32 apart, stepped in turn, both cells' loads in flight together).
+ * All give bit-identical forces.
  * gr_fa2_tune times sample_ticks ticks with each from the current state (restored
  * afterwards) and keeps the fastest; walk_ms_each (nullable, GR_WALK_SCHEDULES
  * floats) gets the mean walk time of each. */
-#define GR_WALK_SCHEDULES 3
+#define GR_WALK_SCHEDULES 4
 int gr_fa2_set_walk_schedule(gr_fa2 *h, int schedule);
 /* Interaction counting (on = 1, the default): the walk adds every tick's far-cell
  * and exact-pair interaction counts to gr_fa2_info.far_count / pair_count. With
@@ -146,6 +148,21 @@ int gr_fa2_set_interaction_counting(gr_fa2 *h, int on);
  * No counterpart in the reference. */
 int gr_fa2_launch_mode(gr_fa2 *h, int *programmatic);
 int gr_fa2_tune(gr_fa2 *h, uint32_t sample_ticks, int *chosen, float *walk_ms_each);
+
+/* Bounded waits and fault injection, for failure detection. No counterpart in the
+ * reference (graph-core runs on one thread and never waits on another).
+ * A tick's key sort is a one-sweep radix sort whose blocks wait for the digit
+ * counts earlier blocks publish. Every such wait is bounded: after `spins`
+ * sleeps of ~32 ns it gives up, sets device error bit 8 (ERR_WAIT), and the
+ * tick's later kernels do nothing; the call returns GR_DEVICE_FAULT and the
+ * handle stays halted (destroy it; other handles are unaffected).
+ * gr_fa2_set_wait_limit sets `spins` for this handle's later ticks (0 restores
+ * the default, 2^22). gr_fa2_inject_stalled_wait(h, 1) makes the second block
+ * of every sort pass first wait for a device word that nothing ever sets, so
+ * that wait runs out: the way a test drives the failure path without faulting
+ * or hanging the GPU. (h, 0) removes the injection. */
+int gr_fa2_set_wait_limit(gr_fa2 *h, uint32_t spins);
+int gr_fa2_inject_stalled_wait(gr_fa2 *h, int on);
 
 /* Current positions to a host buffer (n x dim), refusing non-finite ones as
  * `settle` does (crates/graph-core/src/layout/forceatlas2.rs:82-91). */
@@ -256,33 +273,42 @@ int gr_fa2_set_stream(gr_fa2 *h, void *cuda_stream);
 
 /* Allocation-free force evaluation. No counterpart in the reference.
  *
- * For callers that cannot call cudaMalloc: code that only receives device
- * buffers from its host (a plugin inside another GPU runtime or memory pool),
- * or a stream being captured into a CUDA graph, where an allocation would break
- * the capture. It computes what gr_fa2_forces computes (u = attraction +
- * repulsion - gravity at the given positions; the same tree build and walk) but
- * takes every input and output as device memory and keeps its scratch in a
- * fixed array compiled into this library, sized for GR_FORCES_STATIC_MAX_N
- * nodes (about 14 MB, held on every GPU that loads the library until the
- * process exits). It calls no cudaMalloc, cudaFree or other allocating routine.
+ * For callers that cannot call cudaMalloc: code that runs inside another GPU
+ * runtime which owns every device allocation (its own pool or stream-ordered
+ * allocator), or a plugin that is only handed device buffers by its host. It
+ * computes what gr_fa2_forces computes (u = attraction + repulsion - gravity at
+ * the given positions; the same tree build and walk) but takes every input and
+ * output as device memory and keeps its scratch in a fixed array compiled into
+ * this library, sized for GR_FORCES_STATIC_MAX_N nodes (about 14 MB, held on
+ * every GPU that loads the library until the process exits). It calls no
+ * cudaMalloc, cudaFree or other allocating routine.
  *
  *   nodes    device, n x float4 {x, y, z (0 in 2D), mass}; FA2's mass is degree + 1
  *   row_ptr  device, n + 1 CSR offsets over both endpoints of every simple edge
- *   col      device, neighbour per CSR entry
- *   weight   device, attraction weight per CSR entry (1.0 for unit weights)
+ *   col      device, neighbour per CSR entry (non-null even for an edgeless graph)
+ *   weight   device, attraction weight per CSR entry, already raised to the
+ *            edge_weight_influence power by the caller (1.0 for unit weights);
+ *            non-null even for an edgeless graph
  *   params   host, the usual parameter buffer (dim, theta, scaling, gravity,
- *            lin_log, strong_gravity, dissuade_hubs are read)
+ *            lin_log, strong_gravity, dissuade_hubs are read; max_iter,
+ *            jitter_tolerance and edge_weight_influence are not)
  *   tick     the tick number the coincident-pair jiggle is keyed on
  *   out      device, n x dim forces
  *   stream   the CUDA stream to enqueue on (NULL = legacy default stream)
  *
  * Enqueued asynchronously; only argument refusals are reported (n beyond
- * GR_FORCES_STATIC_MAX_N is refused with GR_INVALID_ARGUMENT). The first call on
- * each device looks up the array's device address (cudaGetSymbolAddress, with
- * that device current): make that first call before any stream capture. Every
- * call shares the one array, so calls that overlap on the GPU (different streams,
- * or different host threads on the same device) race and corrupt each other's
- * results; serialise them on one stream. */
+ * GR_FORCES_STATIC_MAX_N or a null device buffer is refused with
+ * GR_INVALID_ARGUMENT). Device-side failures are not: with a non-finite position
+ * the evaluation stops early and leaves `out` as it was, so a caller that cannot
+ * rule those out uses gr_fa2_forces. The kernels are programmatic dependent
+ * launches unless GR_PDL=0 is set in the environment. The first call on each
+ * device looks up the array's device address (cudaGetSymbolAddress, with that
+ * device current) and keeps it for that device's context (a new context, after
+ * cudaDeviceReset, is looked up again): make that first call before any stream
+ * capture. Every call shares the one array and it keeps the last call's
+ * contents (each call initialises what it reads), so calls that overlap on the
+ * GPU (different streams, or different host threads on the same device) race
+ * and corrupt each other's results; serialise them on one stream. */
 #define GR_FORCES_STATIC_MAX_N 32768
 int gr_fa2_forces_static(uint32_t n, const void *nodes, const uint32_t *row_ptr, const uint32_t *col,
                          const float *weight, const uint8_t *params, size_t params_len, uint32_t tick,

@@ -17,6 +17,7 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liboracle_fa2.so")
+LIB_PATH = _LIB_PATH  # also carries the workload generators (csrc/synth.c), see Makefile
 _lib = None
 
 

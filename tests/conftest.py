@@ -7,7 +7,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE = "/root/reference"
+# The reference checkout: $GRAPH_RENDER_REFERENCE, else a `reference` directory
+# beside this repository. Tests that read it skip when it is absent.
+REFERENCE = os.environ.get("GRAPH_RENDER_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
 
 
 def pytest_configure(config):

@@ -29,4 +29,9 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) > 1:
+        main(sys.argv[1])
+    elif os.environ.get("GRAPH_RENDER_REFERENCE"):
+        main(os.environ["GRAPH_RENDER_REFERENCE"])
+    else:
+        sys.exit(f"usage: python {sys.argv[0]} <reference checkout> (or set GRAPH_RENDER_REFERENCE)")

@@ -163,3 +163,21 @@ def test_long_run_adjoint_outgrows_fp32_and_stays_exactly_linear():
     assert np.linalg.norm(gp) > 1e10
     assert np.array_equal(np.ldexp(gp, -40), gp2)
     assert np.array_equal(np.ldexp(gw, -40), gw2)
+
+
+@pytest.mark.parametrize("theta,ticks", [(0.0, 1), (0.0, 2), (1.2, 2)])
+def test_backward_seeded_with_the_stress_loss_matches_the_oracle(theta, ticks):
+    """The differentiated workload's own seed: dL/dpT of the sampled stress
+    (pairs and hops from the device BFS) at the GPU's final positions, carried
+    back through the run on the GPU and by the FP64 oracle adjoint."""
+    wl, w, prm = instance(n=2000, theta=theta)
+    a, b, h = stress.sample_pairs(wl.n, wl.src, wl.dst, 200_000, 5, sources=200)
+    with Fa2(wl.n, wl.src, wl.dst, w, params=prm, pos0=wl.pos0) as eng:
+        eng.adjoint_forward(ticks, 1)
+        pT = eng.positions()
+        L, g = stress.stress(pT, a, b, h)
+        gp, gw = eng.adjoint_backward(g)
+    assert 0.0 < L < 1.0 and np.abs(g).max() > 0
+    op, ow = oracle_grad(wl, w, prm, ticks, g, dense=(theta == 0.0))
+    assert rel(gp, op) < TOL, rel(gp, op)
+    assert rel(gw, ow) < TOL, rel(gw, ow)

@@ -196,6 +196,45 @@ def test_full_run_matches_the_oracle_on_energy_and_stress(case):
     assert abs(sg - sr) <= 1e-2 * sr, (sg, sr)
 
 
+@pytest.mark.slow
+@pytest.mark.parametrize("case", ["ba100k_500", "powerlaw1m_3d_300"])
+def test_full_run_at_the_workloads_own_size(case):
+    """Whole runs at the workloads' own sizes and tick counts: the 100k-node BA
+    graph (linlog, dissuade hubs, lognormal weights, theta 1.0) for 500 ticks and
+    the 1M-node 3D octree graph (strong gravity, theta 1.2) for 300 ticks, against
+    the oracle's FP64 runs on each energy term (repulsion estimated from 2^25
+    pairs, the same pairs for both layouts) and, in 2D, the Kruskal stress from
+    16 BFS sources (the reference's measure, graph-cli/src/bench.rs:255-295),
+    within 1%."""
+    import time
+
+    from graph_render_b200 import quality
+
+    if case == "ba100k_500":
+        wl, ticks = synth.ba_100k(), 500
+    else:
+        wl, ticks = synth.powerlaw_1m(n=1_000_000, dim=3), 300
+    prm = dict(wl.params, max_iter=ticks)
+    with Fa2(wl.n, wl.src, wl.dst, wl.weight, params=prm, pos0=wl.pos0) as eng:
+        assert eng.run() == ticks
+        g = eng.positions().astype(np.float64)
+    t0 = time.time()
+    st = oracle_state(wl.n, wl.src, wl.dst, wl.weight, wl.pos0, wl.params)
+    st.run(ticks)
+    r = st.positions()
+    t_oracle = time.time() - t0
+    eg = quality.fa2_energy(g, wl.src, wl.dst, wl.weight, prm, pair_sample=1 << 25, seed=7)
+    er = quality.fa2_energy(r, wl.src, wl.dst, wl.weight, prm, pair_sample=1 << 25, seed=7)
+    gaps = {t: abs(eg[t] - er[t]) / abs(er[t]) for t in ("attraction", "repulsion", "gravity", "total")}
+    if g.shape[1] == 2:
+        sg = O.stress(g[:, 0], g[:, 1], wl.src, wl.dst, 16)
+        sr = O.stress(r[:, 0], r[:, 1], wl.src, wl.dst, 16)
+        gaps["stress"] = abs(sg - sr) / sr
+    print(f"{case}: oracle {t_oracle:.1f} s; relative gaps " + ", ".join(f"{k} {v:.2e}" for k, v in gaps.items()))
+    for k, v in gaps.items():
+        assert v <= 1e-2, (k, v, gaps)
+
+
 @pytest.mark.parametrize("dim", [2, 3])
 def test_walk_schedules_give_bit_identical_forces_and_tuning_keeps_the_state(dim):
     wl = synth.powerlaw_1m(n=200_000, dim=dim)
@@ -203,14 +242,16 @@ def test_walk_schedules_give_bit_identical_forces_and_tuning_keeps_the_state(dim
     with Fa2(wl.n, wl.src, wl.dst, params=wl.params, pos0=wl.pos0) as eng:
         eng.tick(3)
         pos = eng.positions()
-        for sch in (0, 1, 2):
+        for sch in (0, 1, 2, 3):
             eng.set_walk_schedule(sch)
-            outs.append((eng.forces(), eng.info()["far_count"]))
+            f0 = eng.info()["far_count"]
+            outs.append((eng.forces(), eng.info()["far_count"] - f0))
         chosen, ms = eng.tune(2)
-        assert chosen in (0, 1, 2) and all(ms[i] > 0 for i in (0, 1, 2))
+        assert chosen in (0, 1, 2, 3) and all(ms[i] > 0 for i in (0, 1, 2, 3))
         assert np.array_equal(eng.positions(), pos)
-    for sch in (1, 2):
+    for sch in (1, 2, 3):
         assert np.array_equal(outs[0][0], outs[sch][0])
+        assert outs[0][1] == outs[sch][1]
 
 
 @pytest.mark.parametrize("dim", [2, 3])
@@ -222,7 +263,7 @@ def test_walk_without_interaction_counts_gives_the_same_forces_and_run(dim):
         far = eng.info()["far_count"]
         assert far > 0
         eng.set_interaction_counting(False)
-        for sch in (0, 1, 2):
+        for sch in (0, 1, 2, 3):
             eng.set_walk_schedule(sch)
             assert np.array_equal(eng.forces(), ref)
         eng.tick(2)

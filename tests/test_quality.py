@@ -67,3 +67,15 @@ def test_energy_gradient_of_gravity_about_the_moving_mean(strong):
 def test_simple_edges_drop_loops_and_keep_the_first_duplicate():
     lo, hi, w = quality.simple_edges(4, [0, 1, 2, 2, 3], [0, 2, 1, 1, 1], [9.0, 1.0, 2.0, 3.0, 4.0])
     assert lo.tolist() == [1, 1] and hi.tolist() == [2, 3] and w.tolist() == [1.0, 4.0]
+
+
+def test_sampled_repulsion_estimates_the_pair_sum():
+    # the estimator the full-size whole-run comparisons use (n too large for the
+    # O(n^2) sum): 2^24 uniform pairs against every pair of a 5,000-node layout
+    from graph_render_b200 import synth
+
+    wl = synth.ba_100k(n=5000)
+    p = wl.pos0.astype(np.float64)
+    exact = quality.fa2_energy(p, wl.src, wl.dst, wl.weight, wl.params)["repulsion"]
+    est = quality.fa2_energy(p, wl.src, wl.dst, wl.weight, wl.params, pair_sample=1 << 24, seed=3)["repulsion"]
+    assert abs(est - exact) <= 1e-3 * abs(exact), (est, exact)
