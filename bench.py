@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-3d", action="store_true")
     ap.add_argument("--no-d3", action="store_true")
     ap.add_argument("--no-configs", action="store_true", help="skip the other configs and the reference's benchmark")
+    ap.add_argument("--walk-schedule", type=int, default=-1,
+                    help="walk schedule for the main workload (default: the autotuner's choice)")
     ap.add_argument("--batched-graphs", type=int, default=4096, help="graphs per GPU")
     ap.add_argument("--batched-ticks", type=int, default=200)
     ap.add_argument("--batched-sample", type=int, default=48, help="graphs timed one launch sequence each")
@@ -614,7 +616,11 @@ def run_gpu(args, dist: Dist):
     eng = Fa2(wl.n, wl.src, wl.dst, wl.weight, params=wl.params, pos0=wl.pos0)
     eng.set_interaction_counting(False)  # the walk without its diagnostic counters
     eng.tick(1)
-    schedule, schedule_ms = eng.tune(3)  # walk schedule autotuner (state restored)
+    if args.walk_schedule >= 0:  # a fixed schedule (profiling), no autotuning
+        schedule, schedule_ms = args.walk_schedule, {i: None for i in range(len(WALK_SCHEDULE_NAMES))}
+        eng.set_walk_schedule(schedule)
+    else:
+        schedule, schedule_ms = eng.tune(3)  # walk schedule autotuner (state restored)
     eng.tick(max(args.warmup, 3))
     torch.cuda.synchronize()
     start_pos, start_ctl = eng.positions(), eng.controller()
