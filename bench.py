@@ -60,6 +60,7 @@ def parse():
     ap.add_argument("--no-configs", action="store_true", help="skip the other configs and the reference's benchmark")
     ap.add_argument("--walk-schedule", type=int, default=-1,
                     help="walk schedule for the main workload (default: the autotuner's choice)")
+    ap.add_argument("--adjoint-ticks", type=int, default=200, help="ticks of the differentiated workload's run")
     ap.add_argument("--batched-graphs", type=int, default=4096, help="graphs per GPU")
     ap.add_argument("--batched-ticks", type=int, default=200)
     ap.add_argument("--batched-sample", type=int, default=48, help="graphs timed one launch sequence each")
@@ -381,7 +382,7 @@ def run_adjoint(args, dist: Dist):
     with Fa2(wl.n, wl.src, wl.dst, wl.weight, params=wl.params, pos0=wl.pos0) as eng:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        eng.adjoint_forward(200, 20)
+        eng.adjoint_forward(args.adjoint_ticks, 20)
         torch.cuda.synchronize()
         fwd = time.perf_counter() - t0
         pT = eng.positions()
@@ -391,9 +392,9 @@ def run_adjoint(args, dist: Dist):
         gp, gw = eng.adjoint_backward(g)
         torch.cuda.synchronize()
         bwd = time.perf_counter() - t0
-    return {"workload": "sbm50000-16blocks-2d", "ticks": 200, "checkpoint_every": 20, "pairs": int(len(a)),
-            "stress": L, "forward_ms": 1e3 * fwd, "backward_ms": 1e3 * bwd,
-            "backward_node_ticks_per_s": wl.n * 200 / bwd, "pair_sampling_s": pairs_s,
+    return {"workload": "sbm50000-16blocks-2d", "ticks": args.adjoint_ticks, "checkpoint_every": 20,
+            "pairs": int(len(a)), "stress": L, "forward_ms": 1e3 * fwd, "backward_ms": 1e3 * bwd,
+            "backward_node_ticks_per_s": wl.n * args.adjoint_ticks / bwd, "pair_sampling_s": pairs_s,
             "grad_pos_norm": float(np.linalg.norm(gp)), "grad_w_norm": float(np.linalg.norm(gw)),
             "finite": bool(np.isfinite(gp).all() and np.isfinite(gw).all())}
 
