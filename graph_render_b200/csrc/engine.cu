@@ -190,10 +190,6 @@ struct gr_fa2 {
     void *flush = nullptr;
     size_t flush_bytes = 0;
     uint32_t *stall_word = nullptr;  // zeroed and never written: the injected wait's flag
-    // the radix tree bottom up (k_karras_up) unless GR_BOTTOM_UP=0 at create; its
-    // per-node meeting slots, zero between ticks (null: the binary-search build)
-    bool bottom_up = true;
-    uint32_t *up_slot = nullptr;
 
     std::vector<void *> allocs;
 
@@ -264,9 +260,6 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
     A(h->bt.leaf_parent, n);
     A(h->bt.visit, n);
     A(h->bt.rec, n);
-    A(h->up_slot, n);
-    if ((e = cudaMemsetAsync(h->up_slot, 0, (size_t)std::max<uint32_t>(n, 1) * sizeof(uint32_t), h->stream)))
-        return e;
     A(h->leaf_body, n);
     A(h->int_body, n);
     A(h->leaf_coinc, n);
@@ -470,10 +463,7 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
             bt.delta = bt.int_parent = nullptr;
         }
         bt.marks = fold_scan ? h->scanner.bsum : nullptr;
-        if (!adjoint && h->bottom_up && h->up_slot)
-            gr_launch(h->pdl, k_karras_up<D>, gn, 256, 0, s, st, h->ukey, bt, h->up_slot, SC_TILE_LEAVES);
-        else
-            gr_launch(h->pdl, k_karras<D>, gn, 256, 0, s, st, h->ukey, bt);
+        gr_launch(h->pdl, k_karras<D>, gn, 256, 0, s, st, h->ukey, bt);
         if (adjoint) k_leaf_body<D><<<gn, 256, 0, s>>>(st, h->sp, h->leaf_start, h->leaf_body, h->leaf_coinc);
         if (adjoint) k_node_body<D><<<gn, 256, 0, s>>>(st, h->bt, pre, h->int_body);
         if (fold_scan)
@@ -574,13 +564,6 @@ static cudaError_t capture_once(gr_fa2 *h, bool timing, cudaGraph_t *g, cudaGrap
         if ((e = cudaGraphKernelNodeSetAttribute(nd, cudaLaunchAttributePriority, &v)) != cudaSuccess) return e;
     }
     return cudaGraphInstantiate(x, *g, 0);
-}
-
-// The bottom-up radix tree for a new handle's ticks: on unless the
-// environment sets GR_BOTTOM_UP=0 (the binary-search build, k_karras).
-static bool bottom_up_default() {
-    const char *v = getenv("GR_BOTTOM_UP");
-    return !(v && strcmp(v, "0") == 0);
 }
 
 // Programmatic dependent launches for a new handle's ticks: on unless the
@@ -746,7 +729,6 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
         }
         h->own_stream = true;
         h->pdl = pdl_default();
-        h->bottom_up = bottom_up_default();
         keep_pool();
         cudaStream_t s = h->stream;
         cudaError_t e = cudaSuccess;

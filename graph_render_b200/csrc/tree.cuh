@@ -446,81 +446,6 @@ __global__ void k_karras(const DevState *st, const uint64_t *__restrict__ k, Bin
     if (t.levels) mark_cells<D>(valid, i, nu, k, q, t.levels, t.cell_flag, t.marks, SC_TILE_LEAVES);
 }
 
-// The same binary radix tree bottom up (Apetrei 2014, "Fast and simple
-// agglomerative LBVH construction", Eurographics UK): one thread per unique
-// leaf climbs toward the root. A finished node covering leaves [L, R] has its
-// parent at whichever boundary is the more similar one: the split between R
-// and R + 1 when delta(R, R + 1) > delta(L - 1, L) (it is the parent's left
-// child), else the split between L - 1 and L (its right child); unique sorted
-// keys never tie there. Internal nodes are named by their split position (node
-// p lies between leaves p and p + 1); the root is the node whose range is every
-// leaf. The two children of a node meet in its slot: each exchanges in its
-// outer bound; the first to arrive stops, the second learns the node's whole
-// range, empties the slot for the next tick, finishes the node and climbs on.
-// Finishing node c with delta d(c) whose parent has delta d(p) writes
-// rec[c] = {L, R, p, d(c)}, and marks it a cell when its level d(c) / D differs
-// from d(p) / D (the root always): cell_flag[c], bit d(c) / D of levels[L] and
-// one count in marks[L / mark_tile]. Those are mark_cells' outputs for the same
-// tree (only the node names differ), so the cells, their preorder and every
-// force are the same bit for bit. Slots start zeroed (a bound is stored plus
-// one, so never as 0) and every used slot is emptied by its second arrival, so
-// they are zero again after every tick. The per-node arrays (first .. visit) are
-// not written: the adjoint's ticks, which read them, use k_karras.
-template <int D>
-__global__ void __launch_bounds__(256)
-k_karras_up(const DevState *st, const uint64_t *__restrict__ k, BinTree t, uint32_t *__restrict__ slot,
-            uint32_t mark_tile) {
-    gr_pdl_enter();
-    if (st->converged) return;
-    const int32_t nu = (int32_t)st->n_unique;
-    const int32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nu) return;
-    if (nu == 1) {
-        t.leaf_parent[0] = -1;
-        return;
-    }
-    int32_t L = s, R = s;
-    uint32_t code = (uint32_t)s | LEAF_BIT;  // the node just finished: a leaf, or an internal node's name
-    int dcur = 0;                              // its delta (internal nodes)
-    for (int32_t guard = 0; guard < nu; guard++) {  // each step widens [L, R]: at most nu - 1 steps
-        const int dl = L > 0 ? __clzll(k[L - 1] ^ k[L]) : -1;
-        const int dr = R + 1 < nu ? __clzll(k[R] ^ k[R + 1]) : -1;
-        const bool root = dl < 0 && dr < 0;
-        const bool left_child = dr > dl;
-        const int32_t p = root ? -1 : left_child ? R : L - 1;
-        const int dpar = left_child ? dr : dl;
-        if (code & LEAF_BIT) {
-            t.leaf_parent[s] = p;
-        } else {
-            const int lv = dcur / D;
-            const bool cell = root || lv != dpar / D;
-            t.rec[code] = make_int4(L, R, p, dcur);
-            t.cell_flag[code] = cell ? 1 : 0;
-            if (cell) {
-                atomicOr(&t.levels[L], 1u << lv);
-                if (t.marks) {  // one atomic per tile among the lanes here together
-                    const uint32_t tile = (uint32_t)L / mark_tile;
-                    const unsigned am = __activemask();
-                    const unsigned peers = __match_any_sync(am, tile);
-                    if ((int)(threadIdx.x % GR_WARP) == __ffs(peers) - 1)
-                        atomicAdd(&t.marks[tile], (uint32_t)__popc(peers));
-                }
-            }
-        }
-        if (root) return;
-        const uint32_t other = atomicExch(&slot[p], (uint32_t)((left_child ? L : R) + 1));
-        if (other == 0u) return;  // the first child here: the second finishes the node
-        slot[p] = 0u;
-        const int32_t ob = (int32_t)other - 1;
-        if (left_child)
-            R = ob;
-        else
-            L = ob;
-        code = (uint32_t)p;
-        dcur = dpar;
-    }
-}
-
 // ---- bodies without atomics: a prefix of the point terms (m, m x per axis;
 // each an exact FP64 product of two FP32 values) over the sorted points, read
 // at every leaf's first point, and every internal node's body as the

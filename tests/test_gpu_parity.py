@@ -295,40 +295,6 @@ def test_programmatic_launches_give_the_same_run(dim, monkeypatch):
 
 
 @pytest.mark.parametrize("dim", [2, 3])
-@pytest.mark.parametrize("case", ["powerlaw", "clusters", "tiny"])
-def test_bottom_up_tree_equals_the_binary_search_build(dim, case, monkeypatch):
-    # the radix tree built bottom up (one climb per leaf, the default) and by
-    # Karras' binary searches (GR_BOTTOM_UP=0) name their nodes differently but
-    # are the same tree: the same cells, interaction counts and forces bit for
-    # bit, over several ticks
-    if case == "powerlaw":
-        wl = synth.powerlaw_1m(n=300_000, dim=dim)
-        n, src, dst, pos, prm = wl.n, wl.src, wl.dst, wl.pos0, wl.params
-    elif case == "clusters":
-        rng = np.random.default_rng(3)
-        n = 20_000
-        pos = np.round(rng.uniform(0, 30, (n, dim))).astype(np.float32)  # many coincident points
-        src, dst = synth.ba(n, 2, 5)
-        prm = dict(dim=dim, theta=1.0)
-    else:
-        n, src, dst = 3, np.array([0, 1], np.uint32), np.array([1, 2], np.uint32)
-        pos = np.arange(3 * dim, dtype=np.float32).reshape(3, dim)
-        prm = dict(dim=dim)
-    ends = []
-    for flag in ("1", "0"):
-        monkeypatch.setenv("GR_BOTTOM_UP", flag)
-        with Fa2(n, src, dst, params=prm, pos0=pos) as eng:
-            f = eng.forces()
-            eng.tick(4)
-            inf = eng.info()
-            ends.append((f, eng.positions(), inf["n_cells"], inf["far_count"], inf["pair_count"]))
-            assert inf["device_error"] == 0
-    assert np.array_equal(ends[0][0], ends[1][0])
-    assert np.array_equal(ends[0][1], ends[1][1])
-    assert ends[0][2:] == ends[1][2:]
-
-
-@pytest.mark.parametrize("dim", [2, 3])
 def test_update_bounds_equal_the_bounds_pass(dim):
     # a tick's update also computes the next tick's root square and mean; setting
     # the positions again makes the bounds pass recompute them: the runs agree bit
