@@ -45,22 +45,28 @@ def test_the_engines_own_start_is_the_references_mulberry32(n, seed, dim):
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
 
 
-def test_run_params_without_positions_reproduces_the_networkx_fixture():
+@pytest.mark.parametrize("dim", [2, 3])
+def test_run_params_without_positions_reproduces_the_networkx_fixture(dim):
+    # 2D: the reference's own fixture; 3D: the same gate at dim 3 (its 1e-7 gate,
+    # docs/measurements/p12-t4b.md:67-80), from tests/golden/make_golden_3d.py
     cap = find(FA2_ID)
     worst, worst_seed = 0.0, -1
-    lines = [json.loads(x) for x in open(GOLDEN)]
+    path = GOLDEN if dim == 2 else os.path.join(HERE, "golden", "fa2_nx_gate_3d.jsonl")
+    lines = [json.loads(x) for x in open(path)]
     assert len(lines) == 64
+    axes = ("x", "y", "z")[:dim]
     for d in lines:
         n = d["n"]
         src, dst, _ = O.gate_edges(n)
-        geom = cap.run_params(Topology(n, src, dst, None), params_bytes(max_iter=d["max_iter"], theta=0.0))
-        got = np.column_stack([np.asarray(geom.x, np.float64), np.asarray(geom.y, np.float64)])
-        want = np.column_stack([d["x"], d["y"]])
+        geom = cap.run_params(Topology(n, src, dst, None),
+                              params_bytes(max_iter=d["max_iter"], theta=0.0, dim=dim))
+        got = np.column_stack([np.asarray(getattr(geom, a), np.float64) for a in axes])
+        want = np.column_stack([d[a] for a in axes])
         ext = (want.max(0) - want.min(0)).max()
         gap = float(np.abs(got - want).max() / ext)
         if gap > worst:
             worst, worst_seed = gap, d["seed"]
-    print(f"worst gap {worst:.3e} of the extent (gate seed {worst_seed})")
+    print(f"dim {dim}: worst gap {worst:.3e} of the extent (gate seed {worst_seed})")
     assert worst < 1e-5, (worst, worst_seed)
 
 

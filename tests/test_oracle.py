@@ -68,6 +68,18 @@ def test_oracle_matches_networkx_golden_vectors():
     assert worst < 1e-12, worst  # the restatement is exact to rounding, well under the ceiling
 
 
+def test_oracle_matches_the_3d_networkx_gate_fixture():
+    """The 3D gate (docs/measurements/p12-t4b.md:67-80: networkx at dim 3, 2 iterations,
+    ceiling 1e-7) over the committed fixture made by tests/golden/make_golden_3d.py."""
+    worst = 0.0
+    for line_ in open(os.path.join(HERE, "golden", "fa2_nx_gate_3d.jsonl")):
+        d = json.loads(line_)
+        st, _ = gate_state(d["n"], seed=0, dim=3, theta=-1.0)
+        st.run(d["max_iter"])
+        worst = max(worst, rel_gap(st.positions(), np.column_stack([d["x"], d["y"], d["z"]])))
+    assert worst < 1e-12, worst
+
+
 def nx_run(n, lo, hi, w, start, iters, **opts):
     g = nx.Graph()
     g.add_nodes_from(range(n))
