@@ -92,6 +92,7 @@ SIGNATURES = {
     "gr_force_session_create": ([P, C.c_uint32, C.c_uint64, P, P, P, P, P], C.c_int),
     "gr_force_session_destroy": ([P], None),
     "gr_force_session_tick": ([P, C.c_uint32], C.c_int),
+    "gr_force_session_tick_timed": ([P, C.c_uint32, C.POINTER(C.c_float)], C.c_int),
     "gr_force_session_positions": ([P, P], C.c_int),
     "gr_force_session_velocities": ([P, P], C.c_int),
     "gr_force_session_alpha": ([P, C.POINTER(C.c_double), C.POINTER(C.c_uint32)], C.c_int),

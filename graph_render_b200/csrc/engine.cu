@@ -2481,6 +2481,33 @@ int gr_force_session_tick(gr_force_session *S, uint32_t ticks) {
     return ok();
 }
 
+int gr_force_session_tick_timed(gr_force_session *S, uint32_t ticks, float *ms) {
+    if (!S) return set_err(GR_INVALID_HANDLE, "null session");
+    if (!ms) return set_err(GR_INVALID_ARGUMENT, "ms is null");
+    *ms = 0.f;
+    if (S->n == 0 || ticks == 0) return ok();
+    if (int c = d3_build_graph(S)) return c;
+    cudaStream_t s = S->t->stream;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CU(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return set_err(GR_CUDA_ERROR, "event creation failed");
+    }
+    cudaError_t e = cudaEventRecord(e0, s);
+    for (uint32_t k = 0; k < ticks && e == cudaSuccess; k++) e = cudaGraphLaunch(S->exec, s);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return set_err(GR_CUDA_ERROR, cudaGetErrorString(e));
+    DevState st;
+    if (int c = read_state(S->t, &st)) return c;
+    if (int c = check_device(S->t, st)) return c;
+    return ok();
+}
+
 int gr_force_session_positions(gr_force_session *S, float *out) {
     if (!S) return set_err(GR_INVALID_HANDLE, "null session");
     if (!out && S->n) return set_err(GR_INVALID_ARGUMENT, "out is null");

@@ -71,6 +71,13 @@ class ForceSession:
     def tick(self, ticks: int = 1) -> None:
         N.check(self._L.gr_force_session_tick(self.h, int(ticks)))
 
+    def tick_timed(self, ticks: int = 1) -> float:
+        """Runs `ticks` ticks; returns their device time in ms (CUDA events on the
+        session's stream)."""
+        ms = C.c_float()
+        N.check(self._L.gr_force_session_tick_timed(self.h, int(ticks), C.byref(ms)))
+        return ms.value
+
     def positions(self) -> np.ndarray:
         out = np.zeros((self.n, 2), np.float32)
         N.check(self._L.gr_force_session_positions(self.h, _ptr(out)))

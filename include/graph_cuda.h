@@ -241,6 +241,10 @@ int gr_force_session_create(gr_force_session **out, uint32_t n, uint64_t m, cons
                             const double *strength, const gr_force_params *params, const float *pos0);
 void gr_force_session_destroy(gr_force_session *s);
 int gr_force_session_tick(gr_force_session *s, uint32_t ticks);
+/* The same ticks with their device time: *ms receives the milliseconds between
+ * CUDA events recorded on the session's stream before the first tick and after
+ * the last. No counterpart in the reference (which has no clock). */
+int gr_force_session_tick_timed(gr_force_session *s, uint32_t ticks, float *ms);
 int gr_force_session_positions(gr_force_session *s, float *out);
 int gr_force_session_velocities(gr_force_session *s, float *out);
 /* alpha after the ticks so far, and how many ticks have run. */

@@ -162,3 +162,15 @@ def test_empty_and_single_node():
     with ForceSession(1, [], []) as s:
         s.tick(112)
         assert np.isfinite(s.positions()).all()
+
+
+def test_timed_ticks_are_the_same_ticks():
+    # gr_force_session_tick_timed runs the same captured ticks between two CUDA
+    # events on the session's stream
+    n, src, dst, st = _gate(2000)
+    with ForceSession(n, src, dst, st) as a, ForceSession(n, src, dst, st) as b:
+        a.tick(7)
+        ms = b.tick_timed(7)
+        assert ms > 0.0
+        assert np.array_equal(a.positions(), b.positions())
+        assert a.ticks_done() == b.ticks_done() == 7
