@@ -353,14 +353,62 @@ k_keys_hist(const float4 *__restrict__ pos, uint32_t n, const DevState *st, uint
     for (uint64_t i = (uint64_t)blockIdx.x * OS_HIST_THREADS + t; i < status_words; i += stride) status[i] = 0u;
 }
 
+// Small graphs: the keys and their whole sort in one CTA, in shared memory. A
+// tick's sort otherwise takes seven dependent kernels (keys with histograms,
+// four one-sweep passes, two run fix-ups), each a few microseconds of launch
+// and drain at any size, which dominate a small graph's tick. Here the keys go
+// to shared memory and block_sort_keys sorts them: four stable passes on the
+// high 32 bits, then runs of equal high words in full-key order (the batched
+// kernel's sort), the same permutation as the stable 64-bit sort.
+constexpr uint32_t SMALL_SORT_MAX = 4096;
+constexpr int SMALL_SORT_T = 1024;
+constexpr size_t SMALL_SORT_SMEM = (size_t)SMALL_SORT_MAX * (2 * sizeof(uint64_t) + 2 * sizeof(uint32_t)) +
+                                   (size_t)(SMALL_SORT_T / GR_WARP) * 256 * 4 + 256 * 4 +
+                                   2 * (SMALL_SORT_MAX / 65 + 1) * 4;
+
+template <int D>
+__global__ void __launch_bounds__(SMALL_SORT_T)
+k_sort_small(const float4 *__restrict__ pos, uint32_t n, const DevState *st, uint64_t *__restrict__ keys_out,
+             uint32_t *__restrict__ vals_out) {
+    gr_pdl_enter();
+    if (st->converged || n > SMALL_SORT_MAX) return;
+    extern __shared__ __align__(16) unsigned char ss_sm[];
+    uint64_t *k = (uint64_t *)ss_sm;
+    uint64_t *ka = k + SMALL_SORT_MAX;
+    uint32_t *v = (uint32_t *)(ka + SMALL_SORT_MAX);
+    uint32_t *va = v + SMALL_SORT_MAX;
+    uint32_t(*s_cnt)[256] = (uint32_t(*)[256])(va + SMALL_SORT_MAX);
+    uint32_t *s_tot = (uint32_t *)(s_cnt + SMALL_SORT_T / GR_WARP);
+    uint32_t *runs = s_tot + 256;  // (start, length) of the runs longer than 64
+    __shared__ uint32_t s_nlong;
+    const double r0[3] = {st->root0[0], st->root0[1], D == 3 ? st->root0[2] : 0.0};
+    const double rw = st->root_w;
+    for (uint32_t i = threadIdx.x; i < n; i += SMALL_SORT_T) {
+        k[i] = morton_key<D>(pos[i], r0, rw);
+        v[i] = i;
+    }
+    __syncthreads();
+    block_sort_keys<SMALL_SORT_T>(k, v, ka, va, n, s_cnt, s_tot, runs, &s_nlong);
+    for (uint32_t i = threadIdx.x; i < n; i += SMALL_SORT_T) {
+        keys_out[i] = k[i];
+        vals_out[i] = v[i];
+    }
+}
+
 // Keys, then a sort on the high 32 key bits (4 passes, stable), then every run
 // of equal high words put in full-key order: runs of up to 64 in place by one
 // thread, longer ones by one CTA each. The order is exactly the full stable
-// 64-bit sort's. The bounds pass zeroed os_ghist and too_long.
+// 64-bit sort's. The bounds pass zeroed os_ghist and too_long. Up to
+// SMALL_SORT_MAX nodes all of it is one kernel (k_sort_small).
 template <int D>
 static void keys_sort_fast(gr_fa2 *h, cudaStream_t s) {
     const uint32_t n = h->n;
     const uint32_t *conv = &h->st->converged;
+    if (n <= SMALL_SORT_MAX) {
+        cudaFuncSetAttribute(k_sort_small<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_SORT_SMEM);
+        gr_launch(h->pdl, k_sort_small<D>, 1, SMALL_SORT_T, SMALL_SORT_SMEM, s, h->pos, n, h->st, h->keys, h->vals);
+        return;
+    }
     if (n < (1u << 30)) {
         const uint32_t nt = div_up(n, os_tile_keys(n));
         gr_launch(h->pdl, k_keys_hist<D>, std::min<uint32_t>(div_up(n, OS_HIST_THREADS * 4), 4 * 148),

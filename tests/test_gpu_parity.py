@@ -322,13 +322,15 @@ def _full_sort_forces(n, src, dst, pos, prm):
     from graph_render_b200 import _native as N, params_bytes
     from tests.test_zz_no_alloc import csr
 
+    dim = int(prm.get("dim", 2))
     rp, col, wts, mass = csr(n, src, dst, None)
     nodes = np.zeros((n, 4), np.float32)
-    nodes[:, :2] = pos
+    nodes[:, :dim] = pos
     nodes[:, 3] = mass
     dev = torch.device("cuda", 0)
+    col = col if len(col) else np.zeros(1, np.int32)
     t = [torch.from_numpy(a).to(dev) for a in (nodes, rp, col, np.ones(len(col), np.float32))]
-    out = torch.zeros((n, 2), dtype=torch.float32, device=dev)
+    out = torch.zeros((n, dim), dtype=torch.float32, device=dev)
     pb = params_bytes(prm)
     N.check(N.lib().gr_fa2_forces_static(n, *[C.c_void_p(x.data_ptr()) for x in t], C.c_char_p(pb), len(pb), 0,
                                          C.c_void_p(out.data_ptr()),
@@ -351,6 +353,29 @@ def test_high_word_sort_with_run_fixup_equals_the_full_sort(cluster):
     with Fa2(wl.n, wl.src, wl.dst, params=prm, pos0=pos) as eng:
         fast = eng.forces()
     full = _full_sort_forces(wl.n, wl.src, wl.dst, pos, prm)
+    assert np.array_equal(fast, full)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("n,cluster", [(4096, 0), (4096, 500), (3000, 70), (2, 0), (1, 0)])
+def test_small_graph_sort_equals_the_full_sort(dim, n, cluster):
+    """Up to 4,096 nodes a tick's keys and sort run as one CTA in shared memory
+    (high words, then runs of equal high words, up to the 500-point cluster here
+    by the block's own sort); the order must be the full 64-bit stable sort's
+    (the allocation-free path sorts all 8 digits), so the forces are identical."""
+    rng = np.random.default_rng(n + cluster + dim)
+    pos = rng.uniform(0, 1000, (n, dim)).astype(np.float32)
+    if cluster:
+        pos[:cluster] = pos[0]
+    # uniform random edges (degrees far below the 64 at which a row's attraction
+    # is split into segments, which only the handle does)
+    src = rng.integers(0, n, 2 * n).astype(np.uint32)
+    dst = rng.integers(0, n, 2 * n).astype(np.uint32)
+    prm = dict(dim=dim, theta=1.0, seed=3)
+    with Fa2(n, src, dst, params=prm, pos0=pos) as eng:
+        fast = eng.forces()
+        assert eng.info()["device_error"] == 0
+    full = _full_sort_forces(n, src, dst, pos, prm)
     assert np.array_equal(fast, full)
 
 
