@@ -77,6 +77,21 @@ def walk_traffic_per_node():
         return None
 
 
+def measure_fp32_tflops(iters: int = 200_000):
+    """This GPU's FP32 FMA rate (TFLOP/s, an FMA as two) from the engine's own
+    FMA-chain kernel, timed with CUDA events; None if the call fails."""
+    import ctypes as C
+
+    from graph_render_b200 import _native as N
+
+    v = C.c_double()
+    try:
+        N.check(N.lib().gr_measure_fp32_rate(iters, C.byref(v)))
+    except N.EngineError:
+        return None
+    return v.value
+
+
 def walk_hbm_view(n: int, n_cells: int, dim: int, walk_ms: float) -> dict:
     """The walk against the measured HBM copy bandwidth: its algorithmic bytes per
     launch (every cell record and sorted node read once, the per-node indices read,
@@ -623,6 +638,7 @@ def run_gpu(args, dist: Dist):
     torch.cuda.synchronize()
     start_pos, start_ctl = eng.positions(), eng.controller()
     programmatic = eng.programmatic_launches()
+    fp32_measured = measure_fp32_tflops()  # the walk roofline's denominator, at the clocks of the timed run
     uuid = str(torch.cuda.get_device_properties(dev).uuid)
     sampler = ClockSampler(uuid if uuid.startswith("GPU-") else f"GPU-{uuid}")
     sampler.start()
@@ -656,7 +672,8 @@ def run_gpu(args, dist: Dist):
     pair = (info1["pair_count"] - info0["pair_count"]) / max(done, 1)
     flops = (far + pair) * FLOPS_PER_INTERACTION[dim]
     sm_max = clocks.get("sm_max_mhz") or 1965.0
-    fp32_peak = 148 * 128 * 2 * sm_max * 1e6
+    fp32_nominal = 148 * 128 * 2 * sm_max * 1e6
+    fp32_peak = fp32_measured * 1e12 if fp32_measured else fp32_nominal
     achieved = flops / (walk_ms / 1e3)
 
     # e2e: the public one-shot path from pinned host buffers, create -> ticks -> positions
@@ -764,8 +781,12 @@ def run_gpu(args, dist: Dist):
                          "traffic": (walk_traffic_per_node() * wl.n if walk_traffic_per_node() and dim == 2
                                      else None),
                          "traffic_source": "ncu dram__bytes_read+write of k_walk_s at 2M nodes, scaled by nodes",
-                         "peak_source": "nominal FP32 FMA rate, 148 SM x 128 lanes x 2 x sm_max_mhz "
-                                        "(MEASURED_PEAKS.json has no non-tensor FP32 figure)",
+                         "peak_source": ("measured: gr_measure_fp32_rate, 8 independent FMA chains a thread, "
+                                         "64 warps a SM, CUDA events, just before the timed ticks "
+                                         "(MEASURED_PEAKS.json has no non-tensor FP32 figure)")
+                                        if fp32_measured else "nominal FP32 FMA rate, 148 SM x 128 lanes x 2 x "
+                                                              "sm_max_mhz",
+                         "peak_nominal": fp32_nominal / 1e12,
                          "interactions_per_tick": {"far": far, "pair": pair},
                          "interactions_from": "the timed ticks replayed from their start state on a second handle "
                                               "whose walk counts them (the timed walk keeps no counters)",

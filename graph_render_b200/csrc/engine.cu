@@ -2229,6 +2229,58 @@ int gr_bfs_hops(uint32_t n, uint64_t m, const uint32_t *source, const uint32_t *
     return ok();
 }
 
+}  // extern "C"
+
+// Eight independent FMA chains per thread, so the FMA pipe, not a chain's
+// latency, sets the rate. `sink` is written only if the sum is exactly -1,
+// which these positive values never reach: it keeps the chains live.
+__global__ void __launch_bounds__(256) k_fma_rate(uint32_t iters, float *sink) {
+    float a[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) a[j] = 1.0f + 1e-7f * (float)(threadIdx.x + j);
+    const float b = 0.9999999f, c = 1e-7f;
+    for (uint32_t i = 0; i < iters; i++) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) a[j] = fmaf(a[j], b, c);
+    }
+    float t = 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; j++) t += a[j];
+    if (t == -1.0f) sink[0] = t;
+}
+
+extern "C" {
+
+int gr_measure_fp32_rate(uint32_t iters, double *tflops) {
+    if (!tflops) return set_err(GR_INVALID_ARGUMENT, "tflops is null");
+    if (iters == 0) return set_err(GR_INVALID_ARGUMENT, "iters must be > 0");
+    int dev = 0, sms = 0;
+    CU(cudaGetDevice(&dev));
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const uint32_t blocks = (uint32_t)sms * 8;  // 64 resident warps a SM
+    float *sink = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMalloc((void **)&sink, sizeof(float));
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) {
+        k_fma_rate<<<blocks, 256>>>(iters, sink);  // warm-up
+        cudaEventRecord(e0);
+        k_fma_rate<<<blocks, 256>>>(iters, sink);
+        cudaEventRecord(e1);
+        e = cudaEventSynchronize(e1);
+    }
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (sink) cudaFree(sink);
+    if (e != cudaSuccess) return set_err(GR_CUDA_ERROR, cudaGetErrorString(e));
+    const double flops = (double)blocks * 256.0 * (double)iters * 8.0 * 2.0;  // an FMA counted as 2
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return ok();
+}
+
 int gr_stress(uint32_t n, uint64_t m, const uint32_t *source, const uint32_t *target, const float *x, const float *y,
               uint32_t sources, double *out) {
     if (!out || (m && (!source || !target)) || (n && (!x || !y))) return set_err(GR_INVALID_ARGUMENT, "null buffer");

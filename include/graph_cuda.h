@@ -205,6 +205,13 @@ int gr_fa2_set_controller(gr_fa2 *h, const gr_fa2_controller *in);
 int gr_fa2_adjoint_forward(gr_fa2 *h, uint32_t ticks, uint32_t checkpoint_every);
 int gr_fa2_adjoint_backward(gr_fa2 *h, const float *dL_dpT, double *dL_dp0, double *dL_dw);
 
+/* The FP32 FMA rate of the current device at its present clocks, in TFLOP/s (an
+ * FMA counted as two operations): a kernel of 8 independent FMA chains per thread,
+ * 64 resident warps per SM, `iters` steps each, timed with CUDA events after one
+ * warm-up launch. The denominator of the repulsion walk's roofline. No
+ * counterpart in the reference. */
+int gr_measure_fp32_rate(uint32_t iters, double *tflops);
+
 /* Multi-source BFS on the device: hop counts from k source nodes to every node
  * (host out, k x n, UINT32_MAX when unreachable) over the raw edges (source,
  * target), undirected, self-loops ignored. No counterpart in the reference, whose

@@ -399,3 +399,16 @@ def test_engine_result_flows_through_the_snapshot_encoder(dim):
     assert np.array_equal(back.y.view(np.uint32), np.asarray(geom.y, np.float32).view(np.uint32))
     assert np.array_equal(back.source, src) and np.array_equal(back.target, dst)
     assert b[8:12] == (b"\x04\0\0\0" if dim == 3 else b"\x03\0\0\0")
+
+
+def test_the_fp32_rate_is_measured():
+    # the repulsion walk's roofline denominator: eight FMA chains a thread, timed
+    # on the device; B200's nominal FP32 FMA rate is 74.4 TFLOP/s at 1,965 MHz
+    import ctypes as C
+
+    from graph_render_b200 import _native as N
+
+    v = C.c_double()
+    N.check(N.lib().gr_measure_fp32_rate(50_000, C.byref(v)))
+    assert 20.0 < v.value < 100.0, v.value
+    assert N.lib().gr_measure_fp32_rate(0, C.byref(v)) == N.GR_INVALID_ARGUMENT
