@@ -197,27 +197,49 @@ def test_full_run_matches_the_oracle_on_energy_and_stress(case):
 
 
 @pytest.mark.slow
-@pytest.mark.parametrize("case", ["ba100k_500", "powerlaw1m_3d_300"])
+@pytest.mark.parametrize("case", ["ba100k_500", "powerlaw1m_3d_300", "powerlaw1m_2d_100", "gate1m_defaults_100"])
 def test_full_run_at_the_workloads_own_size(case):
     """Whole runs at the workloads' own sizes and tick counts: the 100k-node BA
-    graph (linlog, dissuade hubs, lognormal weights, theta 1.0) for 500 ticks and
-    the 1M-node 3D octree graph (strong gravity, theta 1.2) for 300 ticks, against
-    the oracle's FP64 runs on each energy term (repulsion estimated from 2^25
-    pairs, the same pairs for both layouts) and, in 2D, the Kruskal stress from
-    16 BFS sources (the reference's measure, graph-cli/src/bench.rs:255-295),
-    within 1%."""
+    graph (linlog, dissuade hubs, lognormal weights, theta 1.0) for 500 ticks,
+    the 1M-node 3D octree graph (strong gravity, theta 1.2) for 300 ticks, the
+    bench's 1M-node 2D graph (theta 1.2) for 100 ticks, and the reference's own
+    benchmark (its 1M-node gate model through the registry call with an empty
+    parameter buffer: theta 0.8, 100 iterations, the Mulberry32(0) start the
+    engine draws itself), against the oracle's FP64 runs on each energy term
+    (repulsion estimated from 2^25 pairs, the same pairs for both layouts) and, in
+    2D, the Kruskal stress from 16 BFS sources (the reference's measure,
+    graph-cli/src/bench.rs:255-295), within 1%."""
     import time
 
-    from graph_render_b200 import quality
+    from graph_render_b200 import FA2_ID, Topology, find, quality
 
     if case == "ba100k_500":
         wl, ticks = synth.ba_100k(), 500
-    else:
+    elif case == "powerlaw1m_3d_300":
         wl, ticks = synth.powerlaw_1m(n=1_000_000, dim=3), 300
+    elif case == "powerlaw1m_2d_100":
+        wl, ticks = synth.powerlaw_1m(n=1_000_000, dim=2), 100
+    else:
+        wl, ticks = None, 100
+    if wl is None:  # the drop-in call: no positions, default parameters
+        n = 1_000_000
+        src, dst, strength = synth.gate(n)
+        geom = find(FA2_ID).run_params(Topology(n, src, dst, strength), b"")
+        g = np.column_stack([np.asarray(geom.x, np.float64), np.asarray(geom.y, np.float64)])
+
+        class W:
+            pass
+
+        wl = W()
+        wl.n, wl.src, wl.dst, wl.weight = n, src, dst, None
+        wl.pos0 = O.initial_positions(n, 0, 2).astype(np.float32)
+        wl.params = dict(theta=0.8, dim=2, seed=0)
+    else:
+        prm = dict(wl.params, max_iter=ticks)
+        with Fa2(wl.n, wl.src, wl.dst, wl.weight, params=prm, pos0=wl.pos0) as eng:
+            assert eng.run() == ticks
+            g = eng.positions().astype(np.float64)
     prm = dict(wl.params, max_iter=ticks)
-    with Fa2(wl.n, wl.src, wl.dst, wl.weight, params=prm, pos0=wl.pos0) as eng:
-        assert eng.run() == ticks
-        g = eng.positions().astype(np.float64)
     t0 = time.time()
     st = oracle_state(wl.n, wl.src, wl.dst, wl.weight, wl.pos0, wl.params)
     st.run(ticks)
