@@ -540,16 +540,18 @@ def device_run(wl, ticks: int) -> dict:
 
 
 def run_config_legs(args, dist: Dist) -> dict:
-    """The 1,500-node SBM for 100 ticks and the 100k-node BA graph (linlog,
-    dissuade hubs, lognormal weights, theta 1.0) for 500 ticks: device time of
-    the whole run, the public call end to end, and the oracle on this host's
-    cores on a bounded sample of the same run."""
+    """The 1,500-node SBM for 100 ticks, the 100k-node BA graph (linlog,
+    dissuade hubs, lognormal weights, theta 1.0) for 500 ticks and the 1M-node 3D
+    octree graph (strong gravity, theta 1.2) for 300 ticks: device time of the
+    whole run, the public call end to end, and the oracle on this host's cores on
+    a bounded sample of the same run."""
     from graph_render_b200 import synth
 
     threads = os.cpu_count() or 1
     legs = {}
     for key, wl, ticks, calls in (("sbm1500_100_ticks", synth.sbm_1500(), 100, 5),
-                                  ("ba100k_500_ticks", synth.ba_100k(), 500, 3)):
+                                  ("ba100k_500_ticks", synth.ba_100k(), 500, 3),
+                                  ("powerlaw1m_3d_300_ticks", synth.powerlaw_1m(n=1_000_000, dim=3), 300, 3)):
         dev, _ = device_run(wl, ticks)
         e2e = one_shot(wl, ticks, calls)
         v, t, el = cpu_port_rate(wl, threads, min(args.cpu_budget_s, 10.0), max_ticks=ticks)

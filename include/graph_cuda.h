@@ -126,8 +126,8 @@ int gr_fa2_tick_timed(gr_fa2 *h, uint32_t ticks, size_t l2_flush_bytes, float *m
 
 /* Repulsion walk schedule: 0 = warp-cooperative (a warp visits the union of its 32
  * nodes' paths, one broadcast load per cell), 1 = per lane (each lane its own
- * path, gathered loads; the default), 2 = two adjacent nodes per lane over the
- * union of their two paths, 3 = two independent per-lane walks per thread
+ * path, gathered loads; the default in 2D), 2 = two adjacent nodes per lane over the
+ * union of their two paths (the default in 3D), 3 = two independent per-lane walks per thread
  * (nodes 32 apart, stepped in turn, both cells' loads in flight together).
  * All give bit-identical forces.
  * gr_fa2_tune times sample_ticks ticks with each from the current state (restored
