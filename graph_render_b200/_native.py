@@ -87,6 +87,7 @@ SIGNATURES = {
     "gr_fa2_set_stream": ([P, P], C.c_int),
     "gr_run": ([C.c_char_p, C.c_uint32, C.c_uint64, u32p, u32p, f64p, u8p, C.c_size_t, f32p], C.c_int),
     "gr_fa2_forces_static": ([C.c_uint32, P, P, P, P, u8p, C.c_size_t, C.c_uint32, P, P], C.c_int),
+    "gr_fa2_forces_static_status": ([C.POINTER(C.c_uint32)], C.c_int),
     "gr_bfs_hops": ([C.c_uint32, C.c_uint64, P, P, C.c_uint32, P, P], C.c_int),
     "gr_measure_fp32_rate": ([C.c_uint32, C.POINTER(C.c_double)], C.c_int),
     "gr_force_default_params": ([P], None),

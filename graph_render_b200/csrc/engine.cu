@@ -587,9 +587,9 @@ static cudaError_t capture_once(gr_fa2 *h, bool timing, cudaGraph_t *g, cudaGrap
     h->branch = false;
     h->timing_events = false;
     if ((e = cudaStreamEndCapture(h->stream, g)) != cudaSuccess) return e;
-    // The attraction branch fills what the tree build leaves idle: its kernels
-    // run at the lowest priority, the tick's own path at the highest, so a free
-    // SM slot goes to the tree's next block first.
+    // The attraction branch runs beside the walk and fills what the walk leaves
+    // idle: its kernels run at the lowest priority, the tick's own path at the
+    // highest, so a free SM slot goes to the walk's next block first.
     int least = 0, greatest = 0;
     if ((e = cudaDeviceGetStreamPriorityRange(&least, &greatest)) != cudaSuccess) return e;
     size_t nn = 0;
@@ -1422,7 +1422,7 @@ static int forces_static(uint32_t n, const float4 *nodes, const uint32_t *rp, co
     h.stream = s;
     h.own_stream = false;
     h.pdl = pdl_default();  // GR_PDL=0 in the environment: plain stream order
-    h.st = cv.take<DevState>(1);
+    h.st = cv.take<DevState>(1);  // first, at offset 0: gr_fa2_forces_static_status reads it there
     h.keys = cv.take<uint64_t>(n);
     h.vals = cv.take<uint32_t>(n);
     h.ukey = cv.take<uint64_t>(n);
@@ -1503,6 +1503,18 @@ int gr_fa2_forces_static(uint32_t n, const void *nodes, const uint32_t *row_ptr,
     int rc = (int)prm[P_DIM] == 3 ? forces_static<3>(n, (const float4 *)nodes, row_ptr, col, weight, prm, tick, out, s)
                                   : forces_static<2>(n, (const float4 *)nodes, row_ptr, col, weight, prm, tick, out, s);
     if (rc) return rc;
+    return ok();
+}
+
+int gr_fa2_forces_static_status(uint32_t *device_error) {
+    unsigned char *base = nullptr;
+    if (int c = static_base(&base)) return c;
+    // forces_static carves its DevState first, at the array's offset 0
+    DevState s;
+    memset(&s, 0, sizeof s);
+    CU(cudaMemcpy(&s.error, base + offsetof(DevState, error), sizeof s.error, cudaMemcpyDeviceToHost));
+    if (device_error) *device_error = s.error;
+    if (int c = check_device(nullptr, s)) return c;
     return ok();
 }
 

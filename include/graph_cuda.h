@@ -307,11 +307,11 @@ int gr_fa2_set_stream(gr_fa2 *h, void *cuda_stream);
  *   out      device, n x dim forces
  *   stream   the CUDA stream to enqueue on (NULL = legacy default stream)
  *
- * Enqueued asynchronously; only argument refusals are reported (n beyond
- * GR_FORCES_STATIC_MAX_N or a null device buffer is refused with
- * GR_INVALID_ARGUMENT). Device-side failures are not: with a non-finite position
- * the evaluation stops early and leaves `out` as it was, so a caller that cannot
- * rule those out uses gr_fa2_forces. The kernels are programmatic dependent
+ * Enqueued asynchronously; the return value reports argument refusals only (n
+ * beyond GR_FORCES_STATIC_MAX_N or a null device buffer is refused with
+ * GR_INVALID_ARGUMENT). Device-side failures are read afterwards with
+ * gr_fa2_forces_static_status: with a non-finite position the evaluation stops
+ * early and leaves `out` as it was. The kernels are programmatic dependent
  * launches unless GR_PDL=0 is set in the environment. The first call on each
  * device looks up the array's device address (cudaGetSymbolAddress, with that
  * device current) and keeps it for that device's context (a new context, after
@@ -324,6 +324,15 @@ int gr_fa2_set_stream(gr_fa2 *h, void *cuda_stream);
 int gr_fa2_forces_static(uint32_t n, const void *nodes, const uint32_t *row_ptr, const uint32_t *col,
                          const float *weight, const uint8_t *params, size_t params_len, uint32_t tick,
                          float *out, void *stream);
+
+/* The outcome of the last gr_fa2_forces_static evaluation on the current
+ * device, read from the static array (a 4-byte device-to-host copy; nothing is
+ * allocated). Call it once the stream that evaluation ran on has been
+ * synchronised. *device_error (nullable) receives the device error bits (those
+ * of gr_fa2_info's device_error; 0 before any evaluation). Returns GR_OK when
+ * the bits are 0, GR_LAYOUT_FAILED when a position was non-finite, and
+ * GR_DEVICE_FAULT for any other bit. */
+int gr_fa2_forces_static_status(uint32_t *device_error);
 
 /* Batched layouts: many independent graphs in one persistent launch (one CTA per
  * graph at a time, largest first; every tick of a graph inside its CTA). No

@@ -11,7 +11,9 @@ graph first, so a dependence on what a larger earlier call left in the array
 would show), checks that the device's free memory does not change across those
 calls, and checks each result against gr_fa2_forces on the same graph and
 positions within the parity tolerance (1e-5 relative L2). It also checks that
-a graph above the array's stated maximum, and a null device buffer, are refused.
+a graph above the array's stated maximum, and a null device buffer, are refused,
+and that gr_fa2_forces_static_status reports a non-finite position of the last
+evaluation (GR_LAYOUT_FAILED) and a clean one after it.
 
 This file sorts last so a run that stops at the first failure has run every
 other test before it.
@@ -147,3 +149,34 @@ def test_static_forces_refuse_a_null_device_buffer():
                                           C.c_void_p(call.d_out.data_ptr()), None)
         assert rc == N.GR_INVALID_ARGUMENT, i
     torch.cuda.synchronize()
+
+
+def test_static_status_reports_a_non_finite_position_and_clears_on_the_next_call():
+    import torch
+
+    wl = synth.sbm_1500()
+    call = StaticCall(wl.n, wl.src, wl.dst, None, wl.pos0, wl.params)
+    want = call()
+    bits = C.c_uint32(99)
+    assert N.lib().gr_fa2_forces_static_status(C.byref(bits)) == N.GR_OK and bits.value == 0
+    # a NaN coordinate: the bounds pass flags it and every later kernel returns
+    # early, so the output buffer keeps what it held
+    good = call.d_nodes[700, 1].item()
+    call.d_nodes[700, 1] = float("nan")
+    sentinel = torch.full_like(call.d_out, 7.0)
+    call.d_out.copy_(sentinel)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(call.dev)
+    rc = N.lib().gr_fa2_forces_static(call.n, C.c_void_p(call.d_nodes.data_ptr()), C.c_void_p(call.d_rp.data_ptr()),
+                                      C.c_void_p(call.d_col.data_ptr()), C.c_void_p(call.d_w.data_ptr()),
+                                      C.c_char_p(call.pb), len(call.pb), 0, C.c_void_p(call.d_out.data_ptr()),
+                                      C.c_void_p(stream.cuda_stream))
+    assert rc == N.GR_OK  # enqueued: the failure is on the device
+    torch.cuda.synchronize()
+    rc = N.lib().gr_fa2_forces_static_status(C.byref(bits))
+    assert rc == N.GR_LAYOUT_FAILED and bits.value & 1
+    assert torch.equal(call.d_out, sentinel)
+    # the next evaluation starts from a fresh state
+    call.d_nodes[700, 1] = good
+    assert np.array_equal(call(), want)
+    assert N.lib().gr_fa2_forces_static_status(C.byref(bits)) == N.GR_OK and bits.value == 0
