@@ -142,8 +142,9 @@ struct gr_fa2 {
 
     // per-tick buffers
     uint64_t *keys = nullptr, *ukey = nullptr;
-    uint32_t *too_long = nullptr;  // count of runs of equal high key words longer than 64
+    uint32_t *too_long = nullptr;  // count of runs of equal sorted key bits longer than 64
     uint2 *long_runs = nullptr;    // those runs (start, length)
+    int sort_passes = 4;           // one-sweep passes of the tick's key sort (sort_passes_for)
     uint32_t *vals = nullptr, *sorig = nullptr, *uid = nullptr;
     uint32_t *leaf_start = nullptr, *levels = nullptr, *P = nullptr, *leaf_pre = nullptr;
     uint8_t *cell_flag = nullptr;  // internal node -> 1 when it is a cell
@@ -285,13 +286,14 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
 
 enum Phase { PH_TREE = 1, PH_WALK = 2, PH_FINISH = 4, PH_ALL = 7 };
 
-// Runs of equal high key words longer than the in-place fix-up takes: one CTA
-// each, a stable block radix sort of the run in place (scratch: the sorter's
+// Runs of equal sorted key bits longer than the in-place fix-up takes: one CTA
+// each, a stable block radix sort of the run in place by its low `low_passes`
+// digits (even, covering every digit the passes left out; scratch: the sorter's
 // ping-pong buffers at the run's own offsets, free after an even pass count).
 __global__ void __launch_bounds__(256) k_fix_long_runs(uint64_t *__restrict__ keys, uint32_t *__restrict__ vals,
                                                        uint64_t *__restrict__ kalt, uint32_t *__restrict__ valt,
                                                        const uint32_t *long_count, const uint2 *__restrict__ runs,
-                                                       const uint32_t *skip) {
+                                                       int low_passes, const uint32_t *skip) {
     gr_pdl_enter();
     if (skip && *skip) return;
     __shared__ uint32_t s_cnt[8][256];
@@ -299,25 +301,26 @@ __global__ void __launch_bounds__(256) k_fix_long_runs(uint64_t *__restrict__ ke
     const uint32_t count = *long_count;
     for (uint32_t q = blockIdx.x; q < count; q += gridDim.x) {
         const uint2 r = runs[q];
-        // the run's high words are equal: a stable sort of its low words (digits 0-3)
-        block_sort<256>(keys + r.x, vals + r.x, kalt + r.x, valt + r.x, r.y, s_cnt, s_tot, 0, 4);
+        // the run's sorted top digits are equal: a stable sort of the others
+        block_sort<256>(keys + r.x, vals + r.x, kalt + r.x, valt + r.x, r.y, s_cnt, s_tot, 0, low_passes);
     }
 }
 
 // Morton keys of every node (k_keys' work) fused with the one-sweep digit
-// histograms of the keys' high 32 bits (os_hist's work for 4 digits from digit
-// 4) and the zeroing of those passes' look-back words. ghist (digit counts and
-// tile counters) was zeroed by the bounds pass. Grid-stride over the nodes in
-// order, 4 positions in flight per thread; counts are integers, so the
-// histogram does not depend on the order the atomics land in.
-template <int D>
+// histograms of the keys' top PASSES digits (os_hist's work for digits
+// 8 - PASSES .. 7) and the zeroing of those passes' look-back words. ghist
+// (digit counts and tile counters) was zeroed by the bounds pass. Grid-stride
+// over the nodes in order, 4 positions in flight per thread; counts are
+// integers, so the histogram does not depend on the order the atomics land in.
+template <int D, int PASSES>
 __global__ void __launch_bounds__(OS_HIST_THREADS)
 k_keys_hist(const float4 *__restrict__ pos, uint32_t n, const DevState *st, uint64_t *__restrict__ keys,
             uint32_t *__restrict__ vals, uint32_t *__restrict__ ghist, uint32_t *__restrict__ status,
             uint64_t status_words) {
     gr_pdl_enter();
     static_assert(OS_HIST_THREADS == RS_BINS, "one thread per digit");
-    constexpr int PASSES = 4, FIRST = 4, U = 4;
+    static_assert(PASSES >= 2 && PASSES <= 4, "the top two to four digits");
+    constexpr int FIRST = 8 - PASSES, U = 4;
     if (st->converged) return;
     __shared__ uint32_t s_h[PASSES][RS_BINS];
     const int t = threadIdx.x;
@@ -354,9 +357,10 @@ k_keys_hist(const float4 *__restrict__ pos, uint32_t n, const DevState *st, uint
 }
 
 // Small graphs: the keys and their whole sort in one CTA, in shared memory. A
-// tick's sort otherwise takes seven dependent kernels (keys with histograms,
-// four one-sweep passes, two run fix-ups), each a few microseconds of launch
-// and drain at any size, which dominate a small graph's tick. Here the keys go
+// tick's sort otherwise takes five to seven dependent kernels (keys with
+// histograms, two to four one-sweep passes, two run fix-ups), each a few
+// microseconds of launch and drain at any size, which dominate a small graph's
+// tick. Here the keys go
 // to shared memory and block_sort_keys sorts them: four stable passes on the
 // high 32 bits, then runs of equal high words in full-key order (the batched
 // kernel's sort), the same permutation as the stable 64-bit sort.
@@ -395,10 +399,20 @@ k_sort_small(const float4 *__restrict__ pos, uint32_t n, const DevState *st, uin
     }
 }
 
-// Keys, then a sort on the high 32 key bits (4 passes, stable), then every run
-// of equal high words put in full-key order: runs of up to 64 in place by one
-// thread, longer ones by one CTA each. The order is exactly the full stable
-// 64-bit sort's. The bounds pass zeroed os_ghist and too_long. Up to
+// One-sweep passes of a tick's key sort for n nodes: the top 16 key bits up to
+// 2^14 nodes, 24 up to 2^22, else the high 32. The fewer the passes, the more
+// keys share their sorted bits and the longer the runs the fix-up puts in
+// full-key order; while n / 2^(8 passes) stays at or below 1/4 (uniform points:
+// a run of one in most cells; a cluster 30 times as dense: runs of about 8) a
+// pass costs more than the longer runs.
+static int sort_passes_for(uint32_t n) { return n <= (1u << 14) ? 2 : n <= (1u << 22) ? 3 : 4; }
+
+// Keys, then a stable sort on the keys' top digits (h->sort_passes one-sweep
+// passes), then every run of equal sorted bits put in full-key order: runs of
+// up to 64 in place by one thread, longer ones by one CTA each. The order is
+// exactly the full stable 64-bit sort's. With an odd pass count the keys are
+// written to the sorter's scratch pair first, so the last pass lands in
+// keys/vals. The bounds pass zeroed os_ghist and too_long. Up to
 // SMALL_SORT_MAX nodes all of it is one kernel (k_sort_small).
 template <int D>
 static void keys_sort_fast(gr_fa2 *h, cudaStream_t s) {
@@ -409,20 +423,33 @@ static void keys_sort_fast(gr_fa2 *h, cudaStream_t s) {
         gr_launch(h->pdl, k_sort_small<D>, 1, SMALL_SORT_T, SMALL_SORT_SMEM, s, h->pos, n, h->st, h->keys, h->vals);
         return;
     }
+    int passes = 4;
     if (n < (1u << 30)) {
+        passes = h->sort_passes;
         const uint32_t nt = div_up(n, os_tile_keys(n));
-        gr_launch(h->pdl, k_keys_hist<D>, std::min<uint32_t>(div_up(n, OS_HIST_THREADS * 4), 4 * 148),
-                  OS_HIST_THREADS, 0, s, h->pos, n, h->st, h->keys, h->vals, h->sorter.os_ghist, h->sorter.os_status,
-                  (uint64_t)4 * nt * RS_BINS);
-        h->sorter.onesweep_passes(h->keys, h->vals, n, 4, 4, s, &h->st->error, conv, h->pdl, &h->st->converged);
+        const uint32_t hb = std::min<uint32_t>(div_up(n, OS_HIST_THREADS * 4), 4 * 148);
+        const bool odd = passes & 1;
+        uint64_t *k0 = odd ? h->sorter.k_alt : h->keys;
+        uint32_t *v0 = odd ? h->sorter.v_alt : h->vals;
+        uint32_t *gh = h->sorter.os_ghist, *ss = h->sorter.os_status;
+        const uint64_t words = (uint64_t)passes * nt * RS_BINS;
+        if (passes == 2)
+            gr_launch(h->pdl, k_keys_hist<D, 2>, hb, OS_HIST_THREADS, 0, s, h->pos, n, h->st, k0, v0, gh, ss, words);
+        else if (passes == 3)
+            gr_launch(h->pdl, k_keys_hist<D, 3>, hb, OS_HIST_THREADS, 0, s, h->pos, n, h->st, k0, v0, gh, ss, words);
+        else
+            gr_launch(h->pdl, k_keys_hist<D, 4>, hb, OS_HIST_THREADS, 0, s, h->pos, n, h->st, k0, v0, gh, ss, words);
+        h->sorter.onesweep_passes(h->keys, h->vals, n, 8 - passes, passes, s, &h->st->error, conv, h->pdl,
+                                  &h->st->converged);
     } else {
         k_keys<D><<<div_up(n, 256), 256, 0, s>>>(h->pos, n, h->st, h->keys, h->vals);
         h->sorter.sort_digits(h->keys, h->vals, n, 4, 4, s, conv);
     }
-    gr_launch(h->pdl, rs_fix_runs, div_up(n, 256), 256, 0, s, h->keys, h->vals, n, 64u, h->too_long, h->long_runs,
-              conv);
+    const int low = 8 - passes;  // the digits the passes left out, sorted within runs
+    gr_launch(h->pdl, rs_fix_runs, div_up(n, 256), 256, 0, s, h->keys, h->vals, n, 64u, 8 * low, h->too_long,
+              h->long_runs, conv);
     gr_launch(h->pdl, k_fix_long_runs, 148, 256, 0, s, h->keys, h->vals, h->sorter.k_alt, h->sorter.v_alt,
-              h->too_long, h->long_runs, conv);
+              h->too_long, h->long_runs, low + (low & 1), conv);
 }
 
 static_assert(SC_TILE == (int)SC_TILE_LEAVES, "k_karras counts level bits per cell-level scan block");
@@ -771,6 +798,7 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
     // the autotuner's choice on both 1M-node graphs: per lane in 2D, two nodes per
     // lane over the union of their walks in 3D (0.43 against 0.46 ms)
     h->walk_schedule = D == 3 ? 2 : 1;
+    h->sort_passes = sort_passes_for(n);
     memcpy(h->prm, prm, sizeof prm);
     int rc = GR_OK;
     do {

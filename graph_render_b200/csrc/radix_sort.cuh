@@ -161,21 +161,22 @@ rs_downsweep(const uint64_t *__restrict__ kin, const V *__restrict__ vin, uint64
 
 __global__ void rs_zero(uint32_t *__restrict__ totals) { totals[blockIdx.x * RS_BINS + threadIdx.x] = 0; }
 
-// After a stable sort on the high 32 key bits: every run of equal high words
-// is put in full-key order by a stable insertion sort in place, which makes the
-// result identical to a stable sort of the whole key. A run longer than
-// max_run is left alone and raises *too_long instead.
+// After a stable sort on the key bits from `shift` up: every run of equal
+// sorted bits is put in full-key order by a stable insertion sort in place,
+// which makes the result identical to a stable sort of the whole key. A run
+// longer than max_run is left alone and listed in long_runs (*long_count)
+// instead.
 __global__ void rs_fix_runs(uint64_t *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t n, uint32_t max_run,
-                            uint32_t *long_count, uint2 *__restrict__ long_runs, const uint32_t *skip) {
+                            int shift, uint32_t *long_count, uint2 *__restrict__ long_runs, const uint32_t *skip) {
     gr_pdl_enter();
     if (skip && *skip) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i + 1 >= n) return;
-    const uint32_t hi = (uint32_t)(keys[i] >> 32);
-    if ((uint32_t)(keys[i + 1] >> 32) != hi) return;  // not a run of two or more
-    if (i > 0 && (uint32_t)(keys[i - 1] >> 32) == hi) return;  // not the run's first element
+    const uint64_t hi = keys[i] >> shift;
+    if ((keys[i + 1] >> shift) != hi) return;  // not a run of two or more
+    if (i > 0 && (keys[i - 1] >> shift) == hi) return;  // not the run's first element
     uint32_t len = 2;
-    while (i + len < n && (uint32_t)(keys[i + len] >> 32) == hi) len++;
+    while (i + len < n && (keys[i + len] >> shift) == hi) len++;
     if (len > max_run) {  // one CTA sorts it (rs_fix_long_runs)
         const uint32_t q = atomicAdd(long_count, 1u);
         long_runs[q] = make_uint2(i, len);
@@ -526,7 +527,9 @@ struct RadixSorter {
 
     // The one-sweep passes alone, for a caller whose own kernel already filled
     // os_ghist (zeroed first) with the digit counts and zeroed the look-back
-    // words (os_hist's work).
+    // words (os_hist's work). The result lands in keys/vals: with an even pass
+    // count the input is read from there, with an odd one from the scratch pair
+    // (k_alt, v_alt), where the caller's kernel wrote it.
     // A wait that gives up sets ERR_WAIT in *err and, when halt is given, *halt = 1.
     void onesweep_passes(uint64_t *keys, uint32_t *vals, uint32_t n, int first_digit, int passes, cudaStream_t s,
                          uint32_t *err, const uint32_t *skip = nullptr, bool pdl = false, uint32_t *halt = nullptr) {
@@ -548,8 +551,9 @@ struct RadixSorter {
         if (smem > 48 * 1024)
             cudaFuncSetAttribute(os_pass<uint32_t, T, I, OS_L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
-        uint64_t *ka = keys, *kb = k_alt;
-        uint32_t *va = vals, *vb = v_alt;
+        const bool odd = passes & 1;
+        uint64_t *ka = odd ? k_alt : keys, *kb = odd ? keys : k_alt;
+        uint32_t *va = odd ? v_alt : vals, *vb = odd ? vals : v_alt;
         for (int p = 0; p < passes; p++) {
             gr_launch(pdl, os_pass<uint32_t, T, I, OS_L>, nt, T, smem, s, ka, (const uint32_t *)va, kb, vb, n,
                       8 * (first_digit + p), (const uint32_t *)(os_ghist + p * RS_BINS),

@@ -361,44 +361,57 @@ def _full_sort_forces(n, src, dst, pos, prm):
     return out.cpu().numpy()
 
 
-@pytest.mark.parametrize("cluster", [0, 300])
-def test_high_word_sort_with_run_fixup_equals_the_full_sort(cluster):
-    """A handle sorts the keys' high 32 bits and then orders each run of equal
-    high words in place (runs > 64, here a cluster of 300 coincident nodes, by
-    one CTA each); the result must be the full 64-bit sort's, so forces on a
-    graph whose rows all take the same attraction path are bit-identical."""
-    wl = synth.sbm_1500()
-    pos = wl.pos0.copy()
-    if cluster:
-        pos[:cluster] = pos[0]
-    prm = dict(wl.params)
-    with Fa2(wl.n, wl.src, wl.dst, params=prm, pos0=pos) as eng:
-        fast = eng.forces()
-    full = _full_sort_forces(wl.n, wl.src, wl.dst, pos, prm)
-    assert np.array_equal(fast, full)
-
-
-@pytest.mark.parametrize("dim", [2, 3])
-@pytest.mark.parametrize("n,cluster", [(4096, 0), (4096, 500), (3000, 70), (2, 0), (1, 0)])
-def test_small_graph_sort_equals_the_full_sort(dim, n, cluster):
-    """Up to 4,096 nodes a tick's keys and sort run as one CTA in shared memory
-    (high words, then runs of equal high words, up to the 500-point cluster here
-    by the block's own sort); the order must be the full 64-bit stable sort's
-    (the allocation-free path sorts all 8 digits), so the forces are identical."""
-    rng = np.random.default_rng(n + cluster + dim)
+def _uniform_graph(n, dim, seed, cluster=0, spread=0.0):
+    """n points uniform in [0, 1000)^dim, the first `cluster` of them moved onto
+    one point (spread 0) or into a cube of side `spread` around it, and 2n
+    uniform random edges (degrees far below the 64 at which a handle splits a
+    row's attraction into segments, which the allocation-free path does not)."""
+    rng = np.random.default_rng(seed)
     pos = rng.uniform(0, 1000, (n, dim)).astype(np.float32)
     if cluster:
         pos[:cluster] = pos[0]
-    # uniform random edges (degrees far below the 64 at which a row's attraction
-    # is split into segments, which only the handle does)
+        if spread:
+            pos[1:cluster] += rng.uniform(0, spread, (cluster - 1, dim)).astype(np.float32)
     src = rng.integers(0, n, 2 * n).astype(np.uint32)
     dst = rng.integers(0, n, 2 * n).astype(np.uint32)
+    return pos, src, dst
+
+
+def _fast_equals_full(n, dim, pos, src, dst):
     prm = dict(dim=dim, theta=1.0, seed=3)
     with Fa2(n, src, dst, params=prm, pos0=pos) as eng:
         fast = eng.forces()
         assert eng.info()["device_error"] == 0
     full = _full_sort_forces(n, src, dst, pos, prm)
     assert np.array_equal(fast, full)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("n", [12_000, 32_768])
+@pytest.mark.parametrize("cluster,spread", [(0, 0.0), (300, 0.0), (40, 1e-3), (3000, 1e-3)])
+def test_one_sweep_sort_with_run_fixup_equals_the_full_sort(dim, n, cluster, spread):
+    """Above 4,096 nodes a handle sorts the keys' top digits with one-sweep
+    passes and then puts each run of equal sorted bits in full-key order in
+    place: one thread's insertion sort up to 64 keys (the 40-point cluster), one
+    CTA's block sort above (300 coincident points: equal keys, kept in index
+    order; 3,000 distinct points in a cube of side 1e-3, which share the sorted
+    bits). The order must be the full 64-bit stable sort's, which the
+    allocation-free path computes with all 8 digits, so the forces are
+    bit-identical."""
+    pos, src, dst = _uniform_graph(n, dim, 11 + cluster + dim + n, cluster, spread)
+    _fast_equals_full(n, dim, pos, src, dst)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("n,cluster,spread", [(4096, 0, 0.0), (4096, 500, 0.0), (4096, 500, 1e-3), (3000, 70, 0.0),
+                                              (2, 0, 0.0), (1, 0, 0.0)])
+def test_small_graph_sort_equals_the_full_sort(dim, n, cluster, spread):
+    """Up to 4,096 nodes a tick's keys and sort run as one CTA in shared memory
+    (high words, then runs of equal high words, up to the 500-point clusters here
+    by the block's own sort); the order must be the full 64-bit stable sort's
+    (the allocation-free path sorts all 8 digits), so the forces are identical."""
+    pos, src, dst = _uniform_graph(n, dim, n + cluster + dim, cluster, spread)
+    _fast_equals_full(n, dim, pos, src, dst)
 
 
 @pytest.mark.parametrize("dim", [2, 3])
