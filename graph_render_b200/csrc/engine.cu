@@ -142,8 +142,7 @@ struct gr_fa2 {
 
     // per-tick buffers
     uint64_t *keys = nullptr, *ukey = nullptr;
-    uint32_t *too_long = nullptr;  // count of runs of equal sorted key bits longer than 64
-    uint2 *long_runs = nullptr;    // those runs (start, length)
+    bool fast_sort = false;        // the tick sorts the keys' top digits and fixes the runs (keys_sort_fast)
     int sort_passes = 4;           // one-sweep passes of the tick's key sort (sort_passes_for)
     uint32_t *vals = nullptr, *sorig = nullptr, *uid = nullptr;
     uint32_t *leaf_start = nullptr, *levels = nullptr, *P = nullptr, *leaf_pre = nullptr;
@@ -240,8 +239,7 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
     cudaError_t e;
 #define A(p, c) if ((e = h->alloc(&(p), (c)))) return e
     A(h->keys, n);
-    A(h->too_long, 1);
-    A(h->long_runs, (size_t)n / 64 + 2);
+    h->fast_sort = true;
     A(h->vals, n);
     A(h->ukey, n);
     A(h->sorig, n);
@@ -286,23 +284,57 @@ static cudaError_t alloc_tick_buffers(gr_fa2 *h) {
 
 enum Phase { PH_TREE = 1, PH_WALK = 2, PH_FINISH = 4, PH_ALL = 7 };
 
-// Runs of equal sorted key bits longer than the in-place fix-up takes: one CTA
-// each, a stable block radix sort of the run in place by its low `low_passes`
-// digits (even, covering every digit the passes left out; scratch: the sorter's
-// ping-pong buffers at the run's own offsets, free after an even pass count).
-__global__ void __launch_bounds__(256) k_fix_long_runs(uint64_t *__restrict__ keys, uint32_t *__restrict__ vals,
-                                                       uint64_t *__restrict__ kalt, uint32_t *__restrict__ valt,
-                                                       const uint32_t *long_count, const uint2 *__restrict__ runs,
-                                                       int low_passes, const uint32_t *skip) {
+// After a stable sort on the key bits from `shift` up, every run of equal
+// sorted bits put in full-key order in place, which makes the result identical
+// to a stable sort of the whole key: a run of up to 64 keys by the thread at
+// its first key (a stable insertion sort), a longer one by the whole block that
+// holds its first key (a stable block radix sort of its low `low_passes`
+// digits, an even count covering every digit the passes left out; scratch: the
+// sorter's ping-pong pair at the run's own offsets, free after an even pass
+// count). Runs are disjoint, so the result does not depend on which finishes
+// first.
+constexpr uint32_t FIX_T = 256, FIX_SHORT = 64;
+__global__ void __launch_bounds__(FIX_T) k_fix_runs(uint64_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                                                    uint64_t *__restrict__ kalt, uint32_t *__restrict__ valt,
+                                                    uint32_t n, int shift, int low_passes, const uint32_t *skip) {
     gr_pdl_enter();
     if (skip && *skip) return;
-    __shared__ uint32_t s_cnt[8][256];
+    __shared__ uint32_t s_cnt[FIX_T / GR_WARP][256];
     __shared__ uint32_t s_tot[256];
-    const uint32_t count = *long_count;
-    for (uint32_t q = blockIdx.x; q < count; q += gridDim.x) {
-        const uint2 r = runs[q];
-        // the run's sorted top digits are equal: a stable sort of the others
-        block_sort<256>(keys + r.x, vals + r.x, kalt + r.x, valt + r.x, r.y, s_cnt, s_tot, 0, low_passes);
+    __shared__ uint2 s_long[FIX_T];  // at most one run starts at each thread's key
+    __shared__ uint32_t s_nlong;
+    if (threadIdx.x == 0) s_nlong = 0;
+    __syncthreads();
+    const uint32_t i = blockIdx.x * FIX_T + threadIdx.x;
+    if (i + 1 < n) {
+        const uint64_t hi = keys[i] >> shift;
+        // the first key of a run of two or more
+        if ((keys[i + 1] >> shift) == hi && !(i > 0 && (keys[i - 1] >> shift) == hi)) {
+            uint32_t len = 2;
+            while (i + len < n && (keys[i + len] >> shift) == hi) len++;
+            if (len > FIX_SHORT) {
+                s_long[atomicAdd(&s_nlong, 1u)] = make_uint2(i, len);
+            } else {
+                for (uint32_t a = i + 1; a < i + len; a++) {
+                    const uint64_t k = keys[a];
+                    const uint32_t v = vals[a];
+                    uint32_t b = a;
+                    while (b > i && keys[b - 1] > k) {  // strictly greater: equal keys keep their order
+                        keys[b] = keys[b - 1];
+                        vals[b] = vals[b - 1];
+                        b--;
+                    }
+                    keys[b] = k;
+                    vals[b] = v;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    const uint32_t nlong = s_nlong;
+    for (uint32_t q = 0; q < nlong; q++) {
+        const uint2 r = s_long[q];
+        block_sort<FIX_T>(keys + r.x, vals + r.x, kalt + r.x, valt + r.x, r.y, s_cnt, s_tot, 0, low_passes);
     }
 }
 
@@ -408,11 +440,10 @@ k_sort_small(const float4 *__restrict__ pos, uint32_t n, const DevState *st, uin
 static int sort_passes_for(uint32_t n) { return n <= (1u << 14) ? 2 : n <= (1u << 22) ? 3 : 4; }
 
 // Keys, then a stable sort on the keys' top digits (h->sort_passes one-sweep
-// passes), then every run of equal sorted bits put in full-key order: runs of
-// up to 64 in place by one thread, longer ones by one CTA each. The order is
-// exactly the full stable 64-bit sort's. With an odd pass count the keys are
-// written to the sorter's scratch pair first, so the last pass lands in
-// keys/vals. The bounds pass zeroed os_ghist and too_long. Up to
+// passes), then every run of equal sorted bits put in full-key order
+// (k_fix_runs). The order is exactly the full stable 64-bit sort's. With an odd
+// pass count the keys are written to the sorter's scratch pair first, so the
+// last pass lands in keys/vals. The bounds pass zeroed os_ghist. Up to
 // SMALL_SORT_MAX nodes all of it is one kernel (k_sort_small).
 template <int D>
 static void keys_sort_fast(gr_fa2 *h, cudaStream_t s) {
@@ -446,10 +477,8 @@ static void keys_sort_fast(gr_fa2 *h, cudaStream_t s) {
         h->sorter.sort_digits(h->keys, h->vals, n, 4, 4, s, conv);
     }
     const int low = 8 - passes;  // the digits the passes left out, sorted within runs
-    gr_launch(h->pdl, rs_fix_runs, div_up(n, 256), 256, 0, s, h->keys, h->vals, n, 64u, 8 * low, h->too_long,
-              h->long_runs, conv);
-    gr_launch(h->pdl, k_fix_long_runs, 148, 256, 0, s, h->keys, h->vals, h->sorter.k_alt, h->sorter.v_alt,
-              h->too_long, h->long_runs, low + (low & 1), conv);
+    gr_launch(h->pdl, k_fix_runs, div_up(n, FIX_T), FIX_T, 0, s, h->keys, h->vals, h->sorter.k_alt,
+              h->sorter.v_alt, n, 8 * low, low + (low & 1), conv);
 }
 
 static_assert(SC_TILE == (int)SC_TILE_LEAVES, "k_karras counts level bits per cell-level scan block");
@@ -502,17 +531,14 @@ static void enqueue_tick(gr_fa2 *h, bool forces_only, int phases) {
     if (h->timing_events) cudaEventRecordWithFlags(h->ev[0], s, cudaEventRecordExternal);
     if (phases & PH_TREE) {
         // counters later kernels of the tree build accumulate into: the fast
-        // sort's digit counts and long-run count, the cell-level scan's marks
+        // sort's digit counts and tile counters, the cell-level scan's marks
         ZeroWords zw;
-        if (h->long_runs) {
-            zw.add(h->sorter.os_ghist, RadixSorter::ghist_words());
-            zw.add(h->too_long, 1);
-        }
+        if (h->fast_sort) zw.add(h->sorter.os_ghist, RadixSorter::ghist_words());
         const bool fold_scan = h->scanner.folds(n);
         if (fold_scan) zw.add(h->scanner.bsum, div_up(n, SC_TILE));
         k_bounds<D><<<h->bnd_blocks(), BND_THREADS, 0, s>>>(h->pos, n, st, h->part, zw);
         const uint32_t ab = div_up(n, AG_TILE);
-        if (h->long_runs) {
+        if (h->fast_sort) {
             keys_sort_fast<D>(h, s);
         } else {
             k_keys<D><<<gn, 256, 0, s>>>(h->pos, n, st, h->keys, h->vals);

@@ -161,41 +161,6 @@ rs_downsweep(const uint64_t *__restrict__ kin, const V *__restrict__ vin, uint64
 
 __global__ void rs_zero(uint32_t *__restrict__ totals) { totals[blockIdx.x * RS_BINS + threadIdx.x] = 0; }
 
-// After a stable sort on the key bits from `shift` up: every run of equal
-// sorted bits is put in full-key order by a stable insertion sort in place,
-// which makes the result identical to a stable sort of the whole key. A run
-// longer than max_run is left alone and listed in long_runs (*long_count)
-// instead.
-__global__ void rs_fix_runs(uint64_t *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t n, uint32_t max_run,
-                            int shift, uint32_t *long_count, uint2 *__restrict__ long_runs, const uint32_t *skip) {
-    gr_pdl_enter();
-    if (skip && *skip) return;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i + 1 >= n) return;
-    const uint64_t hi = keys[i] >> shift;
-    if ((keys[i + 1] >> shift) != hi) return;  // not a run of two or more
-    if (i > 0 && (keys[i - 1] >> shift) == hi) return;  // not the run's first element
-    uint32_t len = 2;
-    while (i + len < n && (keys[i + len] >> shift) == hi) len++;
-    if (len > max_run) {  // one CTA sorts it (rs_fix_long_runs)
-        const uint32_t q = atomicAdd(long_count, 1u);
-        long_runs[q] = make_uint2(i, len);
-        return;
-    }
-    for (uint32_t a = i + 1; a < i + len; a++) {
-        const uint64_t k = keys[a];
-        const uint32_t v = vals[a];
-        uint32_t b = a;
-        while (b > i && keys[b - 1] > k) {  // strictly greater: equal keys keep their order
-            keys[b] = keys[b - 1];
-            vals[b] = vals[b - 1];
-            b--;
-        }
-        keys[b] = k;
-        vals[b] = v;
-    }
-}
-
 // ---- one-sweep passes (Adinets & Merrill 2022, "Onesweep: a faster least
 // significant digit radix sort for GPUs"): one histogram kernel for every digit
 // of the sort, then one kernel per digit. A block takes the next tile id from a
