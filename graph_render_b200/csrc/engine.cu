@@ -396,7 +396,7 @@ k_keys_hist(const float4 *__restrict__ pos, uint32_t n, const DevState *st, uint
 // to shared memory and block_sort_keys sorts them: four stable passes on the
 // high 32 bits, then runs of equal high words in full-key order (the batched
 // kernel's sort), the same permutation as the stable 64-bit sort.
-constexpr uint32_t SMALL_SORT_MAX = 4096;
+constexpr uint32_t SMALL_SORT_MAX = 1536;
 constexpr int SMALL_SORT_T = 1024;
 constexpr size_t SMALL_SORT_SMEM = (size_t)SMALL_SORT_MAX * (2 * sizeof(uint64_t) + 2 * sizeof(uint32_t)) +
                                    (size_t)(SMALL_SORT_T / GR_WARP) * 256 * 4 + 256 * 4 +
