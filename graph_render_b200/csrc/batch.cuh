@@ -262,23 +262,29 @@ __device__ void block_sort(uint64_t *keys, uint32_t *vals, uint64_t *kalt, uint3
 }
 
 // The same order as an 8-pass block_sort of the full keys, in fewer passes: a
-// stable sort on the high 32 key bits (4 passes), then every run of equal high
-// words in full-key order, by one thread's in-place stable insertion sort (runs
-// of up to 64) or, one after another, by the whole block's 4-pass sort of the
-// run's low words (longer runs; their starts and lengths kept in runs[], at most
-// n / 65 pairs). The one-graph engine's tick sort, at block level.
+// stable sort on the keys' top `top` digits (2 or 4 passes), then every run of
+// equal sorted bits in full-key order, by one thread's in-place stable
+// insertion sort (runs of up to 64) or, one after another, by the whole block's
+// sort of the run's other digits (longer runs; their starts and lengths kept in
+// runs[], at most n / 65 pairs). The one-graph engine's tick sort, at block
+// level. block_sort_top(n) picks the passes: the top 16 bits up to 2^14 keys
+// (runs stay short while n / 2^16 <= 1/4), else the high 32.
+__host__ __device__ inline int block_sort_top(uint32_t n) { return n <= (1u << 14) ? 2 : 4; }
+
 template <int BT>
 __device__ void block_sort_keys(uint64_t *keys, uint32_t *vals, uint64_t *kalt, uint32_t *valt, uint32_t n,
-                                uint32_t (*s_cnt)[256], uint32_t *s_tot, uint32_t *runs, uint32_t *s_nlong) {
-    block_sort<BT>(keys, vals, kalt, valt, n, s_cnt, s_tot, 4, 4);
+                                uint32_t (*s_cnt)[256], uint32_t *s_tot, uint32_t *runs, uint32_t *s_nlong,
+                                int top = 4) {
+    const int shift = 64 - 8 * top;  // the sorted bits: key >> shift
+    block_sort<BT>(keys, vals, kalt, valt, n, s_cnt, s_tot, 8 - top, top);
     if (threadIdx.x == 0) *s_nlong = 0;
     __syncthreads();
     for (uint32_t p = threadIdx.x; p < n; p += BT) {
-        const uint32_t hi = (uint32_t)(keys[p] >> 32);
-        if (p > 0 && (uint32_t)(keys[p - 1] >> 32) == hi) continue;        // not the start of a run
-        if (p + 1 >= n || (uint32_t)(keys[p + 1] >> 32) != hi) continue;  // a run of one
+        const uint64_t hi = keys[p] >> shift;
+        if (p > 0 && (keys[p - 1] >> shift) == hi) continue;        // not the start of a run
+        if (p + 1 >= n || (keys[p + 1] >> shift) != hi) continue;  // a run of one
         uint32_t r = 2;
-        while (p + r < n && (uint32_t)(keys[p + r] >> 32) == hi) r++;
+        while (p + r < n && (keys[p + r] >> shift) == hi) r++;
         if (r <= 64) {
             for (uint32_t a = p + 1; a < p + r; a++) {
                 const uint64_t k = keys[a];
@@ -301,7 +307,7 @@ __device__ void block_sort_keys(uint64_t *keys, uint32_t *vals, uint64_t *kalt, 
     const uint32_t nlong = *s_nlong;
     for (uint32_t q = 0; q < nlong; q++) {
         const uint32_t p = runs[2 * q], r = runs[2 * q + 1];
-        block_sort<BT>(keys + p, vals + p, kalt + p, valt + p, r, s_cnt, s_tot, 0, 4);
+        block_sort<BT>(keys + p, vals + p, kalt + p, valt + p, r, s_cnt, s_tot, 0, 8 - top);
     }
 }
 
@@ -449,7 +455,8 @@ __global__ void __launch_bounds__(BT, BatchOcc<BT>::MIN_BLOCKS) k_batch(BatchArg
                 S.vals[i] = i;
             }
             __syncthreads();
-            block_sort_keys<BT>(S.keys, S.vals, S.kalt, S.valt, n, s_cnt, s_tot, S.flag, &s_nlong);
+            block_sort_keys<BT>(S.keys, S.vals, S.kalt, S.valt, n, s_cnt, s_tot, S.flag, &s_nlong,
+                                block_sort_top(n));
             // ---- sorted nodes, unique keys
             for (uint32_t p = t; p < n; p += BT) {
                 const uint32_t i = S.vals[p];

@@ -389,14 +389,14 @@ k_keys_hist(const float4 *__restrict__ pos, uint32_t n, const DevState *st, uint
 }
 
 // Small graphs: the keys and their whole sort in one CTA, in shared memory. A
-// tick's sort otherwise takes five to seven dependent kernels (keys with
-// histograms, two to four one-sweep passes, two run fix-ups), each a few
+// tick's sort otherwise takes four to six dependent kernels (keys with
+// histograms, two to four one-sweep passes, the run fix-up), each a few
 // microseconds of launch and drain at any size, which dominate a small graph's
-// tick. Here the keys go
-// to shared memory and block_sort_keys sorts them: four stable passes on the
-// high 32 bits, then runs of equal high words in full-key order (the batched
-// kernel's sort), the same permutation as the stable 64-bit sort.
-constexpr uint32_t SMALL_SORT_MAX = 1536;
+// tick. Here the keys go to shared memory and block_sort_keys sorts them: two
+// stable passes on the top 16 bits, then runs of equal sorted bits in full-key
+// order (the batched kernel's sort), the same permutation as the stable 64-bit
+// sort.
+constexpr uint32_t SMALL_SORT_MAX = 3072;
 constexpr int SMALL_SORT_T = 1024;
 constexpr size_t SMALL_SORT_SMEM = (size_t)SMALL_SORT_MAX * (2 * sizeof(uint64_t) + 2 * sizeof(uint32_t)) +
                                    (size_t)(SMALL_SORT_T / GR_WARP) * 256 * 4 + 256 * 4 +
@@ -424,7 +424,7 @@ k_sort_small(const float4 *__restrict__ pos, uint32_t n, const DevState *st, uin
         v[i] = i;
     }
     __syncthreads();
-    block_sort_keys<SMALL_SORT_T>(k, v, ka, va, n, s_cnt, s_tot, runs, &s_nlong);
+    block_sort_keys<SMALL_SORT_T>(k, v, ka, va, n, s_cnt, s_tot, runs, &s_nlong, block_sort_top(n));
     for (uint32_t i = threadIdx.x; i < n; i += SMALL_SORT_T) {
         keys_out[i] = k[i];
         vals_out[i] = v[i];

@@ -390,7 +390,7 @@ def _fast_equals_full(n, dim, pos, src, dst):
 @pytest.mark.parametrize("n", [4_096, 12_000, 32_768])
 @pytest.mark.parametrize("cluster,spread", [(0, 0.0), (300, 0.0), (40, 1e-3), (3000, 1e-3)])
 def test_one_sweep_sort_with_run_fixup_equals_the_full_sort(dim, n, cluster, spread):
-    """Above 1,536 nodes a handle sorts the keys' top digits with one-sweep
+    """Above 3,072 nodes a handle sorts the keys' top digits with one-sweep
     passes and then puts each run of equal sorted bits in full-key order in
     place: one thread's insertion sort up to 64 keys (the 40-point cluster), one
     CTA's block sort above (300 coincident points: equal keys, kept in index
@@ -403,11 +403,11 @@ def test_one_sweep_sort_with_run_fixup_equals_the_full_sort(dim, n, cluster, spr
 
 
 @pytest.mark.parametrize("dim", [2, 3])
-@pytest.mark.parametrize("n,cluster,spread", [(1536, 0, 0.0), (1536, 500, 0.0), (1536, 500, 1e-3), (1200, 70, 0.0),
+@pytest.mark.parametrize("n,cluster,spread", [(3072, 0, 0.0), (3072, 500, 0.0), (3072, 500, 1e-3), (1200, 70, 0.0),
                                               (2, 0, 0.0), (1, 0, 0.0)])
 def test_small_graph_sort_equals_the_full_sort(dim, n, cluster, spread):
-    """Up to 1,536 nodes a tick's keys and sort run as one CTA in shared memory
-    (high words, then runs of equal high words, up to the 500-point clusters here
+    """Up to 3,072 nodes a tick's keys and sort run as one CTA in shared memory
+    (two passes on the top 16 bits, then runs of equal sorted bits, up to the 500-point clusters here
     by the block's own sort); the order must be the full 64-bit stable sort's
     (the allocation-free path sorts all 8 digits), so the forces are identical."""
     pos, src, dst = _uniform_graph(n, dim, n + cluster + dim, cluster, spread)
