@@ -67,6 +67,33 @@ def test_coincident_clusters_take_the_long_run_sort(dim):
         assert (int(st["far"][i]), int(st["pair"][i])) == (inf["far_count"], inf["pair_count"]), g.n
 
 
+def test_graphs_either_side_of_the_block_sort_limit_match_the_engine():
+    # up to 2^14 nodes a graph's block sort takes two passes on the top 16 key
+    # bits, above it four on the high 32 (block_sort_top); a clustered graph on
+    # each side makes long runs of equal sorted bits
+    gs = []
+    rng = np.random.default_rng(21)
+    for i, (n, cl) in enumerate([(16384, 0), (16385, 0), (16000, 500), (19000, 500)]):
+        src = rng.integers(0, n, 3 * n).astype(np.uint32)
+        dst = rng.integers(0, n, 3 * n).astype(np.uint32)
+        pos = rng.uniform(0, 1000, (n, 2)).astype(np.float32)
+        if cl:
+            pos[:cl] = pos[0] + rng.uniform(0, 1e-3, (cl, 2)).astype(np.float32)
+        gs.append(batch.GraphSpec(n, src, dst, dict(theta=1.0, seed=i), None, pos, "sized"))
+    with batch.Batch(gs) as b:
+        b.run(1)
+        got = b.positions()
+        st = b.stats()
+    assert (st["errors"] == 0).all()
+    for i, (g, pos) in enumerate(zip(gs, got)):
+        with Fa2(g.n, g.src, g.dst, params=g.params, pos0=g.pos0) as eng:
+            eng.tick(1)
+            want = eng.positions()
+            inf = eng.info()
+        assert rel_extent(pos, want) < 1e-5, g.n
+        assert (int(st["far"][i]), int(st["pair"][i])) == (inf["far_count"], inf["pair_count"]), g.n
+
+
 def test_first_tick_interactions_equal_the_one_graph_engine():
     gs = small_mix(16, seed=3)
     with batch.Batch(gs) as b:
