@@ -297,7 +297,7 @@ struct BinTree {
     int32_t *leaf_parent; // leaf -> parent (-1 when the tree is one leaf)
     uint32_t *visit;      // bottom-up arrival tickets
     uint32_t *cell_of;    // internal node -> its cell's preorder index, when it is a cell (nullable)
-    int4 *rec;            // internal node -> {first, last, parent, delta} in one load (nullable)
+    int4 *rec;            // internal node -> {first, last, 0, delta} in one load (nullable)
     uint32_t *levels;     // unique leaf s -> bit l set when a cell of level l begins at s (nullable)
     uint8_t *cell_flag;   // internal node -> 1 when it is a cell (written with levels)
     uint32_t *marks;      // nullable: per SC_TILE-leaf block, the count of level bits set in it (zeroed before)
@@ -342,12 +342,7 @@ __device__ __forceinline__ KarrasNode karras_node(int32_t i, int32_t nu, const u
         t.delta[i] = dnode;
         t.visit[i] = 0;
     }
-    if (t.rec) {  // z (parent) is written by the parent
-        int *r = (int *)&t.rec[i];
-        r[0] = first;
-        r[1] = last;
-        r[3] = dnode;
-    }
+    if (t.rec) t.rec[i] = make_int4(first, last, 0, dnode);  // one 16-byte store
     if (first == gamma) {
         if (arrays) t.left[i] = (uint32_t)gamma | LEAF_BIT;
         t.leaf_parent[gamma] = i;
@@ -356,7 +351,6 @@ __device__ __forceinline__ KarrasNode karras_node(int32_t i, int32_t nu, const u
             t.left[i] = (uint32_t)gamma;
             t.int_parent[gamma] = i;
         }
-        if (t.rec) ((int *)&t.rec[gamma])[2] = i;
     }
     if (last == gamma + 1) {
         if (arrays) t.right[i] = (uint32_t)(gamma + 1) | LEAF_BIT;
@@ -366,12 +360,8 @@ __device__ __forceinline__ KarrasNode karras_node(int32_t i, int32_t nu, const u
             t.right[i] = (uint32_t)(gamma + 1);
             t.int_parent[gamma + 1] = i;
         }
-        if (t.rec) ((int *)&t.rec[gamma + 1])[2] = i;
     }
-    if (i == 0) {
-        if (arrays) t.int_parent[0] = -1;
-        if (t.rec) ((int *)&t.rec[0])[2] = -1;
-    }
+    if (i == 0 && arrays) t.int_parent[0] = -1;
     return KarrasNode{first, last, gamma, dnode};
 }
 
