@@ -447,3 +447,19 @@ def test_the_fp32_rate_is_measured():
     N.check(N.lib().gr_measure_fp32_rate(50_000, C.byref(v)))
     assert 20.0 < v.value < 100.0, v.value
     assert N.lib().gr_measure_fp32_rate(0, C.byref(v)) == N.GR_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_recorded_run_builds_the_same_cells_as_a_plain_run(dim):
+    """A run recorded for the adjoint builds its trees with the radix tree's
+    full arrays and the leaf and node body kernels; a plain run keeps only the
+    packed records. Clusters of coincident points make leaves whose level comes
+    from their parent: both runs must give the same positions bit for bit."""
+    n = 6000
+    pos, src, dst = _uniform_graph(n, dim, 77 + dim, cluster=400)
+    pos[1000:1100] = pos[1000]
+    prm = dict(dim=dim, theta=1.0, seed=5)
+    with Fa2(n, src, dst, params=prm, pos0=pos) as a, Fa2(n, src, dst, params=prm, pos0=pos) as b:
+        a.adjoint_forward(6, every=3)
+        b.tick(6)
+        assert np.array_equal(a.positions(), b.positions())
