@@ -804,19 +804,8 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
     if (m && (!src || !dst)) return set_err(GR_INVALID_ARGUMENT, "edge arrays are null");
     if (m > 0x7fffffffull) return set_err(GR_INVALID_ARGUMENT, "more than 2^31 edges");
     const int D = (int)prm[P_DIM];
-    std::vector<float> xyz;  // the seeded start when none is given (a given one is checked on the device)
-    if (!pos0) {
-        xyz.resize((size_t)n * D);
-        // state.rs:272-283 / synthetic.rs:37-50: Mulberry32(seed), dim draws per node.
-        uint32_t s = (uint32_t)prm[P_SEED];
-        for (size_t i = 0; i < xyz.size(); i++) {
-            s += 0x6D2B79F5u;
-            uint32_t a = s;
-            uint32_t t = (a ^ (a >> 15)) * (1u | a);
-            t = (t + ((t ^ (t >> 7)) * (61u | t))) ^ t;
-            xyz[i] = (float)((double)(t ^ (t >> 14)) / 4294967296.0);
-        }
-    }
+    // without pos0 the start is Mulberry32(seed), dim draws per node, drawn on
+    // the device (k_init_nodes); a given one is checked there
     gr_fa2 *h = new (std::nothrow) gr_fa2();
     if (!h) return set_err(GR_ALLOC_FAILED, "host allocation failed");
     h->dim = D;
@@ -926,17 +915,18 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
         }
         float *d_xyz = nullptr;
         const size_t nxyz = (size_t)n * D;
-        if ((e = tmp(&d_xyz, std::max<size_t>(nxyz, 1) * 4))) {
+        if (pos0 && (e = tmp(&d_xyz, std::max<size_t>(nxyz, 1) * 4))) {
             cleanup();
             rc = set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
             break;
         }
         if (n) {
-            cudaMemcpyAsync(d_xyz, pos0 ? pos0 : xyz.data(), nxyz * 4, cudaMemcpyHostToDevice, s);
+            if (pos0) cudaMemcpyAsync(d_xyz, pos0, nxyz * 4, cudaMemcpyHostToDevice, s);
+            const uint32_t seed = (uint32_t)prm[P_SEED];
             if (D == 3)
-                k_init_nodes<3><<<div_up(n, 256), 256, 0, s>>>(n, d_xyz, h->rp, h->pos, d_err);
+                k_init_nodes<3><<<div_up(n, 256), 256, 0, s>>>(n, d_xyz, h->rp, h->pos, d_err, seed);
             else
-                k_init_nodes<2><<<div_up(n, 256), 256, 0, s>>>(n, d_xyz, h->rp, h->pos, d_err);
+                k_init_nodes<2><<<div_up(n, 256), 256, 0, s>>>(n, d_xyz, h->rp, h->pos, d_err, seed);
         }
         DevState init;
         memset(&init, 0, sizeof init);
@@ -944,7 +934,7 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
         init.converged = n == 0 ? 1u : 0u;
         cudaMemcpyAsync(h->st, &init, sizeof init, cudaMemcpyHostToDevice, s);
         cudaMemcpyAsync(hdr, d_err, sizeof hdr, cudaMemcpyDeviceToHost, s);
-        cudaFreeAsync(d_xyz, s);
+        if (d_xyz) cudaFreeAsync(d_xyz, s);
         cleanup();
         e = cudaStreamSynchronize(s);
         if (e) {

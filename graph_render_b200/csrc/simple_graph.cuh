@@ -98,14 +98,34 @@ __global__ void k_csr(uint32_t n, uint32_t ne, EdgeKey ek, const uint64_t *__res
         for (uint32_t r = row + 1; r <= n; r++) rp[r] = ne;
 }
 
+// Draw k (from 0) of Mulberry32 seeded with `seed` as a float in [0, 1)
+// (state.rs:272-283, synthetic.rs:37-50): the generator's state after k + 1
+// steps is seed + (k + 1) * 0x6D2B79F5 (mod 2^32), so any draw is computed
+// directly; u / 2^32 is exact in FP64 and then rounded to FP32 like the
+// reference's f32 start.
+__device__ __forceinline__ float mulberry32_draw(uint32_t seed, uint64_t k) {
+    const uint32_t a = seed + (uint32_t)(k + 1u) * 0x6D2B79F5u;
+    uint32_t t = (a ^ (a >> 15)) * (1u | a);
+    t = (t + ((t ^ (t >> 7)) * (61u | t))) ^ t;
+    return (float)((double)(t ^ (t >> 14)) * 0x1p-32);
+}
+
 // float4 node records: the start coordinates with mass = simple degree + 1
-// (state.rs:86) in .w; a non-finite start coordinate sets bit 4 of *err.
+// (state.rs:86) in .w; a non-finite start coordinate sets bit 4 of *err. A
+// null xyz means the seeded start: node i's axes are Mulberry32(seed) draws
+// D i .. D i + D - 1.
 template <int D>
 __global__ void k_init_nodes(uint32_t n, const float *__restrict__ xyz, const uint32_t *__restrict__ rp,
-                             float4 *__restrict__ pos, uint32_t *err) {
+                             float4 *__restrict__ pos, uint32_t *err, uint32_t seed = 0) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float m = (float)(rp[i + 1] - rp[i]) + 1.0f;
+    if (!xyz) {
+        const uint64_t k = (uint64_t)i * D;
+        pos[i] = make_float4(mulberry32_draw(seed, k), mulberry32_draw(seed, k + 1),
+                             D == 3 ? mulberry32_draw(seed, k + 2) : 0.f, m);
+        return;
+    }
     const float x = xyz[(size_t)i * D], y = xyz[(size_t)i * D + 1], z = D == 3 ? xyz[(size_t)i * D + 2] : 0.f;
     if (!(isfinite(x) && isfinite(y) && isfinite(z))) atomicOr(err, 4u);
     pos[i] = make_float4(x, y, z, m);
