@@ -794,9 +794,16 @@ static void keep_pool() {
     done.push_back(dev);
 }
 
+// Per-graph seeded starts of a concatenation of graphs (host arrays): graph g
+// begins at node off[g] and draws from Mulberry32(seed[g]). Empty: one seed.
+struct SeededStarts {
+    uint32_t graphs = 0;
+    const uint32_t *off = nullptr, *seed = nullptr;
+};
+
 static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
                        const double *weight, const uint8_t *params, size_t params_len, const float *pos0,
-                       bool tick_buffers = true) {
+                       bool tick_buffers = true, SeededStarts starts = SeededStarts()) {
     if (!out) return set_err(GR_INVALID_ARGUMENT, "out is null");
     *out = nullptr;
     double prm[16];
@@ -920,7 +927,24 @@ static int create_impl(gr_fa2 **out, uint32_t n, uint64_t m, const uint32_t *src
             rc = set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
             break;
         }
-        if (n) {
+        uint32_t *d_goff = nullptr;  // per-graph seeded starts: offsets, then seeds
+        if (n && !pos0 && starts.graphs) {
+            if ((e = tmp(&d_goff, (size_t)starts.graphs * 8))) {
+                cleanup();
+                rc = set_err(GR_ALLOC_FAILED, cudaGetErrorString(e));
+                break;
+            }
+            cudaMemcpyAsync(d_goff, starts.off, (size_t)starts.graphs * 4, cudaMemcpyHostToDevice, s);
+            cudaMemcpyAsync(d_goff + starts.graphs, starts.seed, (size_t)starts.graphs * 4, cudaMemcpyHostToDevice,
+                            s);
+            if (D == 3)
+                k_init_nodes_seeded<3><<<div_up(n, 256), 256, 0, s>>>(n, d_goff, d_goff + starts.graphs,
+                                                                      starts.graphs, h->rp, h->pos);
+            else
+                k_init_nodes_seeded<2><<<div_up(n, 256), 256, 0, s>>>(n, d_goff, d_goff + starts.graphs,
+                                                                      starts.graphs, h->rp, h->pos);
+            cudaFreeAsync(d_goff, s);
+        } else if (n) {
             if (pos0) cudaMemcpyAsync(d_xyz, pos0, nxyz * 4, cudaMemcpyHostToDevice, s);
             const uint32_t seed = (uint32_t)prm[P_SEED];
             if (D == 3)
@@ -1751,23 +1775,15 @@ int gr_fa2_batch_create(gr_fa2_batch **out, uint32_t ngraphs, const uint32_t *no
             }
         }
     }
-    // start positions: given, or Mulberry32(seed of the graph) per graph
-    std::vector<float> xyz;
-    const float *p0 = pos0;
+    // start positions: given, or Mulberry32(seed of the graph) per graph, drawn
+    // on the device
+    std::vector<uint32_t> seeds(ngraphs);
+    for (uint32_t g = 0; g < ngraphs; g++) seeds[g] = (uint32_t)prm[(size_t)g * 16 + P_SEED];
+    SeededStarts starts;
     if (!pos0) {
-        xyz.resize(total_n * dim);
-        for (uint32_t g = 0; g < ngraphs; g++) {
-            uint32_t s = (uint32_t)prm[(size_t)g * 16 + P_SEED];
-            float *o = xyz.data() + (size_t)off[g] * dim;
-            for (size_t i = 0; i < (size_t)node_counts[g] * dim; i++) {
-                s += 0x6D2B79F5u;
-                uint32_t a = s;
-                uint32_t t = (a ^ (a >> 15)) * (1u | a);
-                t = (t + ((t ^ (t >> 7)) * (61u | t))) ^ t;
-                o[i] = (float)((double)(t ^ (t >> 14)) / 4294967296.0);
-            }
-        }
-        p0 = xyz.data();
+        starts.graphs = ngraphs;
+        starts.off = off.data();
+        starts.seed = seeds.data();
     }
     double base[11];
     for (uint32_t i = 0; i < kNParams; i++) base[i] = kSpecs[i].def;
@@ -1777,7 +1793,7 @@ int gr_fa2_batch_create(gr_fa2_batch **out, uint32_t ngraphs, const uint32_t *no
     memcpy(bb, base, sizeof bb);
     gr_fa2 *G = nullptr;
     if (int c = create_impl(&G, (uint32_t)total_n, total_m, gs.data(), gd.data(), gw.empty() ? nullptr : gw.data(),
-                            bb, sizeof bb, p0, false))
+                            bb, sizeof bb, pos0, false, starts))
         return c;
     gr_fa2_batch *b = new (std::nothrow) gr_fa2_batch();
     if (!b) {

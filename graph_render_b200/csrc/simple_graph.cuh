@@ -131,6 +131,27 @@ __global__ void k_init_nodes(uint32_t n, const float *__restrict__ xyz, const ui
     pos[i] = make_float4(x, y, z, m);
 }
 
+// The seeded start of a concatenation of graphs: node i of the concatenation
+// belongs to graph g with off[g] <= i < off[g + 1] (off has graphs entries,
+// ascending), and its axes are draws D (i - off[g]) .. + D - 1 of
+// Mulberry32(seed[g]), each graph's own start.
+template <int D>
+__global__ void k_init_nodes_seeded(uint32_t n, const uint32_t *__restrict__ off, const uint32_t *__restrict__ seed,
+                                    uint32_t graphs, const uint32_t *__restrict__ rp, float4 *__restrict__ pos) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || graphs == 0) return;
+    uint32_t lo = 0, hi = graphs;  // the last g with off[g] <= i
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (off[mid] <= i) lo = mid;
+        else hi = mid;
+    }
+    const uint64_t k = (uint64_t)(i - off[lo]) * D;
+    const float m = (float)(rp[i + 1] - rp[i]) + 1.0f;
+    pos[i] = make_float4(mulberry32_draw(seed[lo], k), mulberry32_draw(seed[lo], k + 1),
+                         D == 3 ? mulberry32_draw(seed[lo], k + 2) : 0.f, m);
+}
+
 // Heavy rows (degree > light_max) take ceil(degree / seg) segments: the count
 // per row, then (after an exclusive scan into first) each heavy row's segments.
 __global__ void k_seg_count(uint32_t n, const uint32_t *__restrict__ rp, uint32_t light_max, uint32_t seg,

@@ -187,3 +187,23 @@ def test_batch_full_runs_match_the_oracle_on_energy_and_stress():
             sg = O.stress(pos[:, 0], pos[:, 1], g.src, g.dst, 16)
             sr = O.stress(r[:, 0], r[:, 1], g.src, g.dst, 16)
             assert abs(sg - sr) <= 1e-2 * sr, (g.kind, g.n, sg, sr)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_graphs_without_positions_start_from_their_own_seeded_draws(dim):
+    # no pos0 anywhere: each graph starts from Mulberry32(its own seed), drawn on
+    # the device from its first node, bit for bit the one-graph engine's start
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(40 + dim)
+    gs = []
+    for i, n in enumerate([1, 37, 2500, 700, 64]):
+        src = rng.integers(0, max(n, 1), 2 * n).astype(np.uint32)
+        dst = rng.integers(0, max(n, 1), 2 * n).astype(np.uint32)
+        gs.append(batch.GraphSpec(n, src, dst, dict(dim=dim, seed=[3, 0, 5, 4294967295, 11][i]), None, None, "seeded"))
+    with batch.Batch(gs) as b:
+        got = b.positions()
+    for g, pos in zip(gs, got):
+        want = O.initial_positions(g.n, g.params["seed"], dim).astype(np.float32)
+        assert pos.shape == (g.n, dim)
+        assert np.array_equal(np.asarray(pos, np.float32).view(np.uint32), want.view(np.uint32)), g.n
